@@ -1,0 +1,490 @@
+#!/usr/bin/env python
+"""Benchmark: Mvis/s of ms2dirty + dirty2ms (improved W-stacking) on B200.
+
+One step = ms2dirty of the workload's visibilities followed by dirty2ms of an
+image onto the same rows (Mvis/s = nrow / (t_ms2dirty + t_dirty2ms) / 1e6).
+Default workload: 4096x4096 image, fov 5 deg, 20M rows at 1.5e8 Hz,
+u,v ~ N(0, 6000 m) clipped to +-20 km, w ~ U(-2 km, 2 km), complex64
+visibilities, float32 weights, FP64 uvw, epsilon 1e-5 -- the precision-split
+FP32 form; the plain FP64 form of the same workload is measured beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 runs under torchrun, one process per GPU, each on its own synthetic
+dataset (weak scaling, no collective on the data path); the time is the max
+over ranks.  --impl reference times the reference algorithm on the host cores
+(the CPU restatement in oracle/, all threads), on a bounded sample of the same
+workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "wstack_4096_20M"
+METRIC = "Mvis/s ms2dirty+dirty2ms at eps 1e-5, learned-FP32 vs plain ES-FP64, 1 B200"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default=WORKLOAD)
+    ap.add_argument("--nrow", type=int, default=None, help="override the number of rows")
+    ap.add_argument("--eps", type=float, default=1e-5)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------- ranks
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if (torch.cuda.is_available() and dist.get_backend() == "nccl") else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if (torch.cuda.is_available() and dist.get_backend() == "nccl") else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# --------------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+
+        sm = [num(s[1]) for s in self.samples if num(s[1]) is not None]
+        mx = [num(s[2]) for s in self.samples if num(s[2]) is not None]
+        power = [num(s[3]) for s in self.samples if num(s[3]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i] == "Active"})
+        loaded = [x for x, p in zip(sm, power) if p is not None and p > 250] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "power_w_max": max(power) if power else None, "samples": len(self.samples)}
+
+
+# --------------------------------------------------------------------------- peaks
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel, workload):
+    """Per-launch DRAM traffic recorded from an ncu capture (profiles/*.json)."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    return d.get(workload, {}).get(kernel)
+
+
+# --------------------------------------------------------------------------- workload
+def make_data(cfg_name, seed, nrow, torch):
+    from cugridder_b200 import synth
+
+    d = synth.make(cfg_name, seed=seed, nrow=nrow)
+    img = synth.random_image(d["nx"], d["ny"], seed=seed + 1000, dtype=np.complex64)
+    return d, img
+
+
+def algorithmic_bytes(stage, d, info, prec):
+    """Minimum HBM bytes of one launch of each stage (reads of its inputs plus
+    writes of its outputs, each once)."""
+    M = d["uvw"].shape[0]
+    s_c = 8 if prec == "fp32" else 16
+    rec = 32 if prec == "fp32" else 48
+    G = info["nf1"] * info["nf2"] * info["nw"]
+    npix = d["nx"] * d["ny"]
+    nq = (d["nx"] // 2 + 1) * (d["ny"] // 2 + 1)
+    return {
+        "gridding": M * rec + G * s_c,
+        "degridding": G * s_c + M * rec + M * 4 + M * s_c,
+        "plane_fill": G * s_c + npix * s_c + nq * 16,
+        "wdft_deconv": info["nw"] * npix * s_c + npix * s_c + nq * 16,
+        "fft": 4 * G * s_c,
+        "sorted_stream": M * (4 + 24 + s_c + s_c // 2) + M * rec,
+        "binning": M * 24 + 4 * 3 * M * 8,
+    }.get(stage)
+
+
+def run_b200(args, rank, world, local):
+    import torch
+
+    from cugridder_b200 import Plan, _lib, dirty2ms_mixed, ms2dirty_mixed, synth  # noqa: F401
+
+    torch.cuda.set_device(local)
+    cfg = synth.CONFIGS[args.config]
+    d, img = make_data(args.config, rank, args.nrow, torch)
+    M = d["uvw"].shape[0]
+    nx, ny, fov, freq = d["nx"], d["ny"], d["fov"], d["freq"]
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+
+    uvw = torch.from_numpy(d["uvw"]).to(dev)
+    res = {}
+    lib = _lib.load()
+    clocks = ClockSampler(local)
+
+    def timed_run(prec, steps, warmup, sample_clocks=False, timing=False):
+        cdt = torch.complex64 if prec == "fp32" else torch.complex128
+        rdt = torch.float32 if prec == "fp32" else torch.float64
+        vis = torch.from_numpy(d["vis"]).to(device=dev, dtype=cdt)
+        wgt = torch.from_numpy(d["wgt"]).to(device=dev, dtype=rdt)
+        dimg = torch.from_numpy(img).to(device=dev, dtype=cdt)
+        dirty = torch.empty((nx, ny), dtype=cdt, device=dev)
+        vout = torch.empty(M, dtype=cdt, device=dev)
+        plan = Plan(nx, ny, fov, args.eps, precision=prec, stream=stream.cuda_stream)
+
+        def step():
+            plan.ms2dirty(uvw, freq, vis, wgt, dirty)
+            plan.dirty2ms(uvw, freq, dimg, wgt, vout)
+
+        for _ in range(warmup):
+            step()
+        torch.cuda.synchronize()
+        if timing:
+            plan.set_timing(True)
+        if sample_clocks:
+            clocks.start()
+            time.sleep(0.3)
+        barrier(world)
+        torch.cuda.synchronize()
+        l0 = lib.cg_kernel_launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+        launches = lib.cg_kernel_launches() - l0
+        if sample_clocks:
+            clocks.stop()
+        ms = e0.elapsed_time(e1)
+        out = {"ms": ms, "launches": launches, "info": plan.info()}
+        if timing:
+            out["timing"] = plan.timing()
+        plan.close()
+        del vis, wgt, dimg, dirty, vout
+        torch.cuda.empty_cache()
+        return out
+
+    main = timed_run("fp32", args.steps, args.warmup, sample_clocks=True, timing=True)
+    t_max = max_over_ranks(main["ms"], world)
+    total_rows = sum_over_ranks(M, world)
+    res["value"] = total_rows * args.steps / (t_max / 1e3) / 1e6
+    res["ms_per_step"] = t_max / args.steps
+    res["gpu_launches"] = int(main["launches"])
+    res["info"] = main["info"]
+
+    # per-stage timing and roofline of the dominant kernel of this library
+    tm = main["timing"]
+    ncalls = max(tm["calls"][0], 1)
+    stages = {}
+    peak, peak_kind = measured_peaks()
+    for direction in ("ms2dirty", "dirty2ms"):
+        for name, total in tm[direction].items():
+            per = total / ncalls
+            b = algorithmic_bytes(name, d, main["info"], "fp32")
+            stages[direction + "." + name] = {
+                "ms": round(per, 4),
+                "algorithmic_GB": None if b is None else round(b / 1e9, 4),
+                "GBps": None if (b is None or per <= 0) else round(b / 1e9 / (per / 1e3), 1),
+            }
+    own = {k: v for k, v in stages.items() if not k.endswith(".fft") and not k.endswith("w_range")}
+    dom = max(own, key=lambda k: own[k]["ms"])
+    dom_name = dom.split(".")[1]
+    ach = stages[dom]["GBps"]
+    res["roofline"] = {
+        "kernel": dom, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s",
+        "frac": None if ach is None else round(ach / peak, 4),
+        "traffic": ncu_traffic(dom_name, args.config), "peak_source": peak_kind,
+    }
+    res["stages"] = stages
+    res["clocks"] = clocks.summary()
+
+    if not args.no_fp64:
+        fp = timed_run("fp64", max(2, args.steps // 3), 1)
+        t64 = max_over_ranks(fp["ms"], world)
+        v64 = total_rows * max(2, args.steps // 3) / (t64 / 1e3) / 1e6
+        res["fp64_plain"] = {"value": round(v64, 2), "ms_per_step": round(t64 / max(2, args.steps // 3), 3),
+                             "eps": args.eps, "kw": fp["info"]["kw"], "nw": fp["info"]["nw"]}
+        res["fp32_over_fp64"] = round(res["value"] / v64, 3)
+
+    if not args.no_e2e:
+        res["e2e"] = run_e2e(args, d, img, world)
+    return res
+
+
+def run_e2e(args, d, img, world):
+    """Same metric through the public host API (cg_ms2dirty_mixed /
+    cg_dirty2ms_mixed) from pinned host buffers: every step copies its inputs
+    host->device and its outputs device->host."""
+    import torch
+
+    from cugridder_b200 import _lib
+
+    lib = _lib.load()
+    M = d["uvw"].shape[0]
+    nx, ny = d["nx"], d["ny"]
+
+    def pinned(a):
+        t = torch.empty(a.shape, dtype=getattr(torch, str(a.dtype)), pin_memory=True)
+        t.numpy()[...] = a
+        return t.numpy()
+
+    uvw = pinned(d["uvw"])
+    vis = pinned(d["vis"].astype(np.complex64))
+    wgt = pinned(d["wgt"].astype(np.float32))
+    dimg = pinned(img.astype(np.complex64))
+    dirty = pinned(np.zeros((nx, ny), np.complex64))
+    vout = pinned(np.zeros(M, np.complex64))
+
+    def step():
+        r1 = lib.cg_ms2dirty_mixed(M, nx, ny, d["fov"], d["freq"], uvw.ctypes.data, vis.ctypes.data,
+                                   wgt.ctypes.data, dirty.ctypes.data, args.eps, 2.0, -1)
+        r2 = lib.cg_dirty2ms_mixed(M, nx, ny, d["fov"], d["freq"], uvw.ctypes.data, vout.ctypes.data,
+                                   wgt.ctypes.data, dimg.ctypes.data, args.eps, 2.0, -1)
+        _lib.check(r1)
+        _lib.check(r2)
+
+    step()
+    torch.cuda.synchronize()
+    barrier(world)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(torch.cuda.default_stream())
+    for _ in range(args.e2e_steps):
+        step()
+    e1.record(torch.cuda.default_stream())
+    torch.cuda.synchronize()
+    barrier(world)
+    t = max_over_ranks(e0.elapsed_time(e1), world)
+    total_rows = sum_over_ranks(M, world)
+    lib.cg_release_cache()
+    h2d = 2 * uvw.nbytes + vis.nbytes + 2 * wgt.nbytes + dimg.nbytes
+    d2h = dirty.nbytes + vout.nbytes
+    return {"value": round(total_rows * args.e2e_steps / (t / 1e3) / 1e6, 2), "unit": "Mvis/s",
+            "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+            "ms_per_step": round(t / args.e2e_steps, 3), "api": "cg_ms2dirty_mixed+cg_dirty2ms_mixed"}
+
+
+# --------------------------------------------------------------------------- CPU (oracle port)
+def cpu_reference_rate(cfg_name, nsample=200_000, seed=0):
+    """Mvis/s of the reference algorithm restated on the host cores, for the
+    full workload, assembled from measured parts: per-row gridding and
+    degridding cost (nsample rows, same kernel width), one full-size 2-D FFT
+    plane per direction (times nw), and the per-pixel w stage / corrections
+    (measured on a 256x256 image, scaled to the workload's pixels)."""
+    from cugridder_b200 import synth
+    from oracle import oracle as O
+
+    full = synth.CONFIGS[cfg_name]
+    d = synth.make(cfg_name, seed=seed, nrow=nsample)
+    p = O.setup(np.array([[0, 0, -full["w_max"]], [0, 0, full["w_max"]]], float), full["nx"],
+                full["ny"], full["fov"], full["freq"], 1e-5)
+    # gridding / degridding per row, on a small grid with the same W
+    ps = O.setup(d["uvw"], 256, 256, 2.0, full["freq"], 1e-5)
+    X = O.grid_coords(ps, d["uvw"])
+    c = d["vis"].astype(np.complex128)
+    t0 = time.perf_counter()
+    fw = O.grid(ps, X, c)
+    t1 = time.perf_counter()
+    O.degrid(ps, X, fw)
+    t2 = time.perf_counter()
+    t_grid, t_degrid = (t1 - t0) / nsample, (t2 - t1) / nsample
+    # one full-size plane FFT per direction
+    pf = O.Params()
+    ctypes_fields = O.setup(np.zeros((1, 3)), full["nx"], full["ny"], full["fov"], full["freq"], 1e-5)
+    for name, _ in O.Params._fields_:
+        setattr(pf, name, getattr(ctypes_fields, name))
+    pf.nf3 = 1
+    plane = np.zeros((1, pf.nf2, pf.nf1), np.complex128)
+    plane[0, :64, :64] = 1.0
+    t0 = time.perf_counter()
+    O.fft2_planes(pf, plane, +1)
+    t1 = time.perf_counter()
+    t_fft_plane = (t1 - t0)
+    # w stage + corrections per pixel: a 256^2 run minus its gridding and FFT
+    small = synth.make("ms2dirty_256_fp64", seed=seed, nrow=2000)
+    t0 = time.perf_counter()
+    O.ms2dirty(small["uvw"], small["vis"], small["wgt"], 256, 256, 2.0, 1e8, 1e-5)
+    t1 = time.perf_counter()
+    psm = O.setup(small["uvw"], 256, 256, 2.0, 1e8, 1e-5)
+    t_small_fft = t_fft_plane * (psm.nf1 * psm.nf2) / (pf.nf1 * pf.nf2) * psm.nf3
+    t_pix = max((t1 - t0) - t_small_fft - 2000 * t_grid, 0.0) / (256 * 256)
+    M = full["nrow"]
+    npix = full["nx"] * full["ny"]
+    t_total = M * (t_grid + t_degrid) + 2 * p.nf3 * t_fft_plane + 2 * npix * t_pix
+    return {
+        "value": round(M / t_total / 1e6, 6), "unit": "Mvis/s", "cores": O.num_threads(),
+        "kind": "port",
+        "sample": ("oracle (C/OpenMP restatement of the reference pipeline): gridding+degridding "
+                   "timed on %d rows (W=%d), one %dx%d FFT plane per direction x nw=%d, w stage "
+                   "per pixel from a 256^2 run; assembled for %d rows on %dx%d"
+                   % (nsample, p.kw, pf.nf1, pf.nf2, p.nf3, M, full["nx"], full["ny"])),
+        "seconds_for_full_workload": round(t_total, 1),
+    }
+
+
+def run_reference(args, rank, world):
+    """--impl reference: rank 0 times the reference algorithm on the host."""
+    if rank != 0:
+        return None
+    vals = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference_rate(args.config, nsample=100_000, seed=i)
+        if i >= args.warmup:
+            vals.append(r)
+    v = statistics.median(x["value"] for x in vals)
+    r = dict(vals[-1])
+    r["value"] = v
+    return r
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_setup()
+    if args.impl == "reference":
+        r = run_reference(args, rank, world)
+        if rank == 0:
+            line = {"impl": "reference", "metric": METRIC, "value": r["value"], "unit": "Mvis/s",
+                    "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                    "dtype": "f64", "data": "synthetic",
+                    "config": {"workload": args.config, "eps": args.eps},
+                    "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                    "e2e": {"value": r["value"], "unit": "Mvis/s", "h2d_bytes_per_step": 0,
+                            "d2h_bytes_per_step": 0}}
+            print(json.dumps(line), flush=True)
+        return
+    res = run_b200(args, rank, world, local)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_rate(args.config)
+    if rank == 0:
+        from cugridder_b200 import synth
+
+        cfg = synth.CONFIGS[args.config]
+        info = res.pop("info")
+        line = {
+            "metric": METRIC, "value": round(res["value"], 2), "unit": "Mvis/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(res["ms_per_step"], 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (fp64 uvw/coordinates)", "data": "synthetic",
+            "config": {"workload": args.config, "nx": cfg["nx"], "ny": cfg["ny"], "fov_deg": cfg["fov"],
+                       "nrow_per_gpu": args.nrow or cfg["nrow"], "freq_hz": cfg["freq"], "eps": args.eps,
+                       "kernel": "ES", "W": info["kw"], "nw": info["nw"], "grid": [info["nf1"], info["nf2"]],
+                       "parallelism": "independent datasets per GPU" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (uvw 480 MB, grid 7.5 GB)"},
+            "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res.get("e2e"),
+            "gpu_launches": res["gpu_launches"], "clocks": res["clocks"],
+            "fp64_plain": res.get("fp64_plain"), "fp32_over_fp64": res.get("fp32_over_fp64"),
+            "stages": res["stages"],
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

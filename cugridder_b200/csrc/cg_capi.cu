@@ -1,0 +1,367 @@
+// extern "C" entry points of libcugridder.so.
+//
+// The eight reference-compatible functions (reference include/cugridder.h:37-47,
+// src/astro/cugridder.cu:541-571) take HOST pointers and are synchronous, as in
+// the reference.  Unlike the reference, which mallocs, copies and frees every
+// device buffer and cuFFT plan inside each call (cugridder.cu:309-388), they
+// share one cached plan per precision so repeated calls reuse HBM workspace;
+// cg_release_cache() frees it.  Errors are returned, never exit()ed.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "cg_plan.cuh"
+
+#include <atomic>
+
+namespace cg {
+static thread_local std::string g_last_error;
+void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+static std::atomic<long long> g_launches{0};
+void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+}  // namespace cg
+
+using cg::ensure;
+
+namespace {
+
+std::mutex g_cache_mu;
+cg_plan_s* g_cache[2] = {nullptr, nullptr};
+
+int ensure_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    cg::set_last_error("no CUDA device");
+    return CG_ERR_NOGPU;
+  }
+  return CG_OK;
+}
+
+void destroy_plan(cg_plan_s* P) {
+  if (!P) return;
+  cudaSetDevice(P->device);
+  if (P->fft_valid) cufftDestroy(P->fft);
+  cg_dev_buf* bs[] = {&P->mm,   &P->K1,    &P->K2,     &P->K3q,    &P->zq,     &P->grid,
+                      &P->recs, &P->perm,  &P->skeys,  &P->hive_start, &P->binws, &P->fftwork,
+                      &P->io_uvw, &P->io_vis, &P->io_wgt, &P->io_dirty};
+  for (auto b : bs) cg::release(*b);
+  if (P->h_mm) cudaFreeHost(P->h_mm);
+  if (P->timer.created)
+    for (int s = 0; s < 2; s++)
+      for (int i = 0; i <= kMaxStages; i++) cudaEventDestroy(P->timer.ev[s][i]);
+  delete P;
+}
+
+cg_plan_s* cached_plan(int precision, int& status) {
+  status = ensure_device();
+  if (status) return nullptr;
+  cg_plan_s*& P = g_cache[precision];
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (P && P->device != dev) {
+    destroy_plan(P);
+    P = nullptr;
+  }
+  if (!P) {
+    P = new cg_plan_s();
+    P->device = dev;
+    P->stream = nullptr;
+  }
+  return P;
+}
+
+__global__ void k_widen_uvw(const float* __restrict__ in, double* __restrict__ out, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (double)in[i];
+}
+
+// Host-pointer driver shared by every host entry point.
+// uvw_is_float: uvw given in float (reference -DSINGLE API), widened on device.
+int host_call(bool to_dirty, int precision, int64_t nrow, int nx, int ny, double fov,
+              double freq, const void* uvw, bool uvw_is_float, void* vis, const void* wgt,
+              void* dirty, double eps, double sigma, int sign) {
+  if (nrow < 0 || (nrow > 0 && (!uvw || !vis)) || !dirty) {
+    cg::set_last_error("invalid argument");
+    return CG_ERR_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_cache_mu);
+  int st;
+  cg_plan_s* P = cached_plan(precision, st);
+  if (!P) return st;
+  CG_CUDA(cudaSetDevice(P->device));
+  CG_TRY(cg::plan_configure(P, nx, ny, fov, eps, sigma, sign, precision));
+  size_t tsz = precision == CG_PREC_FP64 ? 8 : 4;
+  size_t n_uvw = (size_t)nrow * 3;
+  CG_TRY(ensure(P->io_uvw, n_uvw * 8 + (uvw_is_float ? n_uvw * 4 : 0)));
+  CG_TRY(ensure(P->io_vis, (size_t)nrow * 2 * tsz));
+  CG_TRY(ensure(P->io_wgt, (size_t)nrow * tsz));
+  CG_TRY(ensure(P->io_dirty, (size_t)nx * ny * 2 * tsz));
+  cudaStream_t s = P->stream;
+  double* d_uvw = (double*)P->io_uvw.p;
+  if (nrow > 0) {
+    if (uvw_is_float) {
+      float* d_f = (float*)(d_uvw + n_uvw);
+      CG_CUDA(cudaMemcpyAsync(d_f, uvw, n_uvw * 4, cudaMemcpyHostToDevice, s));
+      k_widen_uvw<<<592, 256, 0, s>>>(d_f, d_uvw, (int64_t)n_uvw);
+      cg::count_launches(1);
+      CG_CUDA(cudaGetLastError());
+    } else {
+      CG_CUDA(cudaMemcpyAsync(d_uvw, uvw, n_uvw * 8, cudaMemcpyHostToDevice, s));
+    }
+    if (wgt) CG_CUDA(cudaMemcpyAsync(P->io_wgt.p, wgt, (size_t)nrow * tsz, cudaMemcpyHostToDevice, s));
+  }
+  int rs;
+  if (to_dirty) {
+    if (nrow > 0) CG_CUDA(cudaMemcpyAsync(P->io_vis.p, vis, (size_t)nrow * 2 * tsz, cudaMemcpyHostToDevice, s));
+    rs = cg::ms2dirty_device(P, nrow, freq, d_uvw, P->io_vis.p, wgt ? P->io_wgt.p : nullptr,
+                             P->io_dirty.p);
+    if (rs > 1) return rs;
+    CG_CUDA(cudaMemcpyAsync(dirty, P->io_dirty.p, (size_t)nx * ny * 2 * tsz, cudaMemcpyDeviceToHost, s));
+  } else {
+    CG_CUDA(cudaMemcpyAsync(P->io_dirty.p, dirty, (size_t)nx * ny * 2 * tsz, cudaMemcpyHostToDevice, s));
+    rs = cg::dirty2ms_device(P, nrow, freq, d_uvw, P->io_dirty.p, wgt ? P->io_wgt.p : nullptr,
+                             P->io_vis.p);
+    if (rs > 1) return rs;
+    if (nrow > 0) CG_CUDA(cudaMemcpyAsync(vis, P->io_vis.p, (size_t)nrow * 2 * tsz, cudaMemcpyDeviceToHost, s));
+  }
+  CG_CUDA(cudaStreamSynchronize(s));
+  return rs;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---------------- reference-compatible FP64 (cugridder.cu:541-571) ----------------
+int ms2dirty_2(int nrow, int nxdirty, int nydirty, double fov, double freq, double* uvw,
+               cg_c128* vis, double* wgt, cg_c128* dirty, double epsilon, double sigma, int sign) {
+  return host_call(true, CG_PREC_FP64, nrow, nxdirty, nydirty, fov, freq, uvw, false, vis, wgt,
+                   dirty, epsilon, sigma, sign);
+}
+int ms2dirty_1(int nrow, int nxdirty, int nydirty, double fov, double freq, double* uvw,
+               cg_c128* vis, cg_c128* dirty, double epsilon, double sigma, int sign) {
+  return host_call(true, CG_PREC_FP64, nrow, nxdirty, nydirty, fov, freq, uvw, false, vis,
+                   nullptr, dirty, epsilon, sigma, sign);
+}
+int dirty2ms_1(int nrow, int nxdirty, int nydirty, double fov, double freq, double* uvw,
+               cg_c128* vis, cg_c128* dirty, double epsilon, double sigma, int sign) {
+  return host_call(false, CG_PREC_FP64, nrow, nxdirty, nydirty, fov, freq, uvw, false, vis,
+                   nullptr, dirty, epsilon, sigma, sign);
+}
+int dirty2ms_2(int nrow, int nxdirty, int nydirty, double fov, double freq, double* uvw,
+               cg_c128* vis, double* wgt, cg_c128* dirty, double epsilon, double sigma, int sign) {
+  return host_call(false, CG_PREC_FP64, nrow, nxdirty, nydirty, fov, freq, uvw, false, vis, wgt,
+                   dirty, epsilon, sigma, sign);
+}
+
+// ---------------- reference-compatible FP32 (-DSINGLE twins) ----------------
+int ms2dirtyf_2(int nrow, int nxdirty, int nydirty, float fov, float freq, float* uvw,
+                cg_c64* vis, float* wgt, cg_c64* dirty, float epsilon, float sigma, int sign) {
+  return host_call(true, CG_PREC_FP32, nrow, nxdirty, nydirty, fov, freq, uvw, true, vis, wgt,
+                   dirty, epsilon, sigma, sign);
+}
+int ms2dirtyf_1(int nrow, int nxdirty, int nydirty, float fov, float freq, float* uvw,
+                cg_c64* vis, cg_c64* dirty, float epsilon, float sigma, int sign) {
+  return host_call(true, CG_PREC_FP32, nrow, nxdirty, nydirty, fov, freq, uvw, true, vis,
+                   nullptr, dirty, epsilon, sigma, sign);
+}
+int dirty2msf_1(int nrow, int nxdirty, int nydirty, float fov, float freq, float* uvw,
+                cg_c64* vis, cg_c64* dirty, float epsilon, float sigma, int sign) {
+  return host_call(false, CG_PREC_FP32, nrow, nxdirty, nydirty, fov, freq, uvw, true, vis,
+                   nullptr, dirty, epsilon, sigma, sign);
+}
+int dirty2msf_2(int nrow, int nxdirty, int nydirty, float fov, float freq, float* uvw,
+                cg_c64* vis, float* wgt, cg_c64* dirty, float epsilon, float sigma, int sign) {
+  return host_call(false, CG_PREC_FP32, nrow, nxdirty, nydirty, fov, freq, uvw, true, vis, wgt,
+                   dirty, epsilon, sigma, sign);
+}
+
+// ---------------- precision split, host pointers ----------------
+int cg_ms2dirty_mixed(int64_t nrow, int nxdirty, int nydirty, double fov, double freq,
+                      const double* uvw, const cg_c64* vis, const float* wgt, cg_c64* dirty,
+                      double epsilon, double sigma, int sign) {
+  return host_call(true, CG_PREC_FP32, nrow, nxdirty, nydirty, fov, freq, uvw, false,
+                   (void*)vis, wgt, dirty, epsilon, sigma, sign);
+}
+int cg_dirty2ms_mixed(int64_t nrow, int nxdirty, int nydirty, double fov, double freq,
+                      const double* uvw, cg_c64* vis, const float* wgt, const cg_c64* dirty,
+                      double epsilon, double sigma, int sign) {
+  return host_call(false, CG_PREC_FP32, nrow, nxdirty, nydirty, fov, freq, uvw, false, vis, wgt,
+                   (void*)dirty, epsilon, sigma, sign);
+}
+
+// ---------------- plan API ----------------
+int cg_plan_create(cg_plan** plan, int nxdirty, int nydirty, double fov, double epsilon,
+                   double sigma, int sign, int precision, void* stream) {
+  if (!plan) return CG_ERR_ARG;
+  *plan = nullptr;
+  int st = ensure_device();
+  if (st) return st;
+  cg_plan_s* P = new cg_plan_s();
+  cudaGetDevice(&P->device);
+  P->stream = (cudaStream_t)stream;
+  st = cg::plan_configure(P, nxdirty, nydirty, fov, epsilon, sigma, sign, precision);
+  if (st > 1) {
+    destroy_plan(P);
+    return st;
+  }
+  *plan = P;
+  return st;
+}
+
+int cg_plan_set_stream(cg_plan* plan, void* stream) {
+  if (!plan) return CG_ERR_ARG;
+  plan->stream = (cudaStream_t)stream;
+  return CG_OK;
+}
+
+int cg_plan_ms2dirty(cg_plan* plan, int64_t nrow, double freq, const double* d_uvw,
+                     const void* d_vis, const void* d_wgt, void* d_dirty) {
+  if (!plan) return CG_ERR_ARG;
+  std::lock_guard<std::mutex> lock(plan->mu);
+  return cg::ms2dirty_device(plan, nrow, freq, d_uvw, d_vis, d_wgt, d_dirty);
+}
+
+int cg_plan_dirty2ms(cg_plan* plan, int64_t nrow, double freq, const double* d_uvw,
+                     const void* d_dirty, const void* d_wgt, void* d_vis) {
+  if (!plan) return CG_ERR_ARG;
+  std::lock_guard<std::mutex> lock(plan->mu);
+  return cg::dirty2ms_device(plan, nrow, freq, d_uvw, d_dirty, d_wgt, d_vis);
+}
+
+int cg_plan_get_info(const cg_plan* plan, cg_plan_info* info) {
+  if (!plan || !info) return CG_ERR_ARG;
+  const cg::Geom& g = plan->geom;
+  info->kw = plan->kw;
+  info->beta = plan->beta;
+  info->nf1 = plan->nf1;
+  info->nf2 = plan->nf2;
+  info->nw = g.nw;
+  info->i_center = g.i_center;
+  info->i_half_width = g.i_half_width;
+  info->o_center = g.o_center;
+  info->o_half_width = g.o_half_width;
+  info->gamma = g.gamma;
+  info->h = g.h;
+  info->pixelsize_x = plan->fov / 180.0 * cg::kPi / (double)plan->nx;
+  info->pixelsize_y = plan->fov / 180.0 * cg::kPi / (double)plan->ny;
+  info->nhive[0] = g.nhx;
+  info->nhive[1] = g.nhy;
+  info->nhive[2] = g.nhz;
+  info->nrow = plan->nrow;
+  info->workspace_bytes = cg::workspace_bytes(plan);
+  return CG_OK;
+}
+
+int cg_plan_destroy(cg_plan* plan) {
+  destroy_plan(plan);
+  return CG_OK;
+}
+
+int cg_plan_set_stop_stage(cg_plan* plan, int stage) {
+  if (!plan || stage < 0 || stage > 3) return CG_ERR_ARG;
+  plan->stop_stage = stage;
+  return CG_OK;
+}
+
+int cg_plan_copy_buffer(cg_plan* plan, int which, void* host_dst, size_t bytes,
+                        size_t* bytes_needed) {
+  if (!plan) return CG_ERR_ARG;
+  const cg::Geom& g = plan->geom;
+  size_t tsz = plan->precision == CG_PREC_FP64 ? 8 : 4;
+  const void* src = nullptr;
+  size_t need = 0;
+  switch (which) {
+    case CG_BUF_HIVE_START:
+      src = plan->hive_start.p;
+      need = ((size_t)g.nhx * g.nhy * g.nhz + 1) * 4;
+      break;
+    case CG_BUF_PERM:
+      src = plan->perm.p;
+      need = (size_t)plan->nrow * 4;
+      break;
+    case CG_BUF_SORTED_KEYS:
+      src = plan->skeys.p;
+      need = (size_t)plan->nrow * 8;
+      break;
+    case CG_BUF_GRID:
+      src = plan->grid.p;
+      need = (size_t)g.nf1 * g.nf2 * g.nw * 2 * tsz;
+      break;
+    case CG_BUF_FSERIES_1:
+      src = plan->K1.p;
+      need = (size_t)(plan->nf1 / 2 + 1) * 8;
+      break;
+    case CG_BUF_FSERIES_2:
+      src = plan->K2.p;
+      need = (size_t)(plan->nf2 / 2 + 1) * 8;
+      break;
+    case CG_BUF_FSERIES_W:
+      src = plan->K3q.p;
+      need = (size_t)(plan->ny / 2 + 1) * (plan->nx / 2 + 1) * 8;
+      break;
+    default:
+      return CG_ERR_ARG;
+  }
+  if (bytes_needed) *bytes_needed = need;
+  if (!host_dst) return CG_OK;
+  if (bytes < need || !src) return CG_ERR_ARG;
+  CG_CUDA(cudaStreamSynchronize(plan->stream));
+  if (which == CG_BUF_SORTED_KEYS && plan->key_bytes == 4) {
+    // widen 32-bit keys to int64 on the host
+    std::vector<uint32_t> tmp(plan->nrow);
+    if (plan->nrow) CG_CUDA(cudaMemcpy(tmp.data(), src, (size_t)plan->nrow * 4, cudaMemcpyDeviceToHost));
+    int64_t* dst = (int64_t*)host_dst;
+    for (int64_t i = 0; i < plan->nrow; i++) dst[i] = (int64_t)tmp[i];
+    return CG_OK;
+  }
+  if (need) CG_CUDA(cudaMemcpy(host_dst, src, need, cudaMemcpyDeviceToHost));
+  return CG_OK;
+}
+
+int cg_plan_set_timing(cg_plan* plan, int on) {
+  if (!plan) return CG_ERR_ARG;
+  std::lock_guard<std::mutex> lock(plan->mu);
+  plan->timer.on = on != 0;
+  for (int d = 0; d < 2; d++) {
+    plan->timer.calls[d] = 0;
+    for (int i = 0; i < kMaxStages; i++) plan->timer.acc[d][i] = 0;
+  }
+  plan->timer.pending[0] = plan->timer.pending[1] = false;
+  return CG_OK;
+}
+
+int cg_plan_get_timing(cg_plan* plan, int direction, double* stage_ms, int cap, int* nstages,
+                       long long* ncalls) {
+  if (!plan || direction < 0 || direction > 1) return CG_ERR_ARG;
+  std::lock_guard<std::mutex> lock(plan->mu);
+  CG_CUDA(cudaStreamSynchronize(plan->stream));
+  cg::timer_flush(plan, 0);
+  cg::timer_flush(plan, 1);
+  int n = kMaxStages < cap ? kMaxStages : cap;
+  for (int i = 0; i < n; i++) stage_ms[i] = plan->timer.acc[direction][i];
+  if (nstages) *nstages = 7;
+  if (ncalls) *ncalls = plan->timer.calls[direction];
+  return CG_OK;
+}
+
+int cg_release_cache(void) {
+  std::lock_guard<std::mutex> lock(g_cache_mu);
+  for (int i = 0; i < 2; i++) {
+    destroy_plan(g_cache[i]);
+    g_cache[i] = nullptr;
+  }
+  return CG_OK;
+}
+
+const char* cg_last_error(void) { return cg::g_last_error.c_str(); }
+
+long long cg_kernel_launches(void) { return cg::g_launches.load(); }
+
+int cg_version(void) { return 100; }
+
+}  // extern "C"

@@ -1,0 +1,98 @@
+// Internal declarations of the B200 gridder (libcugridder.so).
+//
+// Naming follows the reference (RapidsAtHKUST/cuGridder): N1 = nydirty is the
+// fast image axis and grid dim 0 (size nf1, fed by v), N2 = nxdirty is the
+// slow image axis and grid dim 1 (size nf2, fed by u); nw = nf3 is the number
+// of w planes (cugridder.cu:191,347).  The grid is stored plane-major,
+// fw[p][g1][g0] with g0 fastest, as in the reference (conv.cu:596-598).
+#pragma once
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <cstddef>
+#include <cstdint>
+
+#include "../../include/cugridder.h"
+
+namespace cg {
+
+constexpr double kPi = 3.14159265358979323846;
+// constants exactly as the reference's include/utils.h:29-30
+constexpr double kM_1_2PI = 0.159154943091895336;
+constexpr double kM_2PI = 6.28318530717958648;
+constexpr double kSpeedOfLight = 299792458.0;
+constexpr int kMaxW = 16;
+constexpr int kMaxQuad = 32;  // GL nodes used by the kernel Fourier series (p <= 26)
+
+// Per-call geometry, passed by value to every kernel.
+struct Geom {
+  int N1, N2;        // image sizes (N1 = ny fast, N2 = nx)
+  int nf1, nf2, nw;  // grid sizes
+  int kw;            // kernel width W
+  double beta, es_c; // ES kernel exp(beta*sqrt(1 - c d^2)), |d| < W/2
+  double pixx, pixy; // pixel sizes (radians): pixx with u / image x, pixy with v / image y
+  double foc;        // freq / c
+  int sign;
+  double i_center, i_half_width, o_center, o_half_width, gamma, h;
+  int nhx, nhy, nhz; // 8 x 8 x 1 hives
+};
+
+// Kernel Fourier-series quadrature: phi_hat(k) = sum_i g[i] * 2 cos(x[i] k)
+struct Quad {
+  int p;
+  double x[kMaxQuad];
+  double g[kMaxQuad];
+};
+
+// Sorted visibility record: cell index (bx,by,bz) and the fractional offset
+// inside the cell in the working precision, plus a complex payload
+// (the weighted, phase-shifted visibility for gridding; the output factor
+// wgt*exp(-i o_c w) for degridding).
+template <typename T>
+struct alignas(16) Rec {
+  T f[3];
+  uint32_t bxy;  // bx | by << 16
+  uint32_t bz;
+  T c[2];
+};
+
+// ---- pipeline entry points (cg_pipeline.cu) ----
+}  // namespace cg
+
+struct cg_plan_s;
+
+namespace cg {
+int ms2dirty_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw,
+                    const void* d_vis, const void* d_wgt, void* d_dirty);
+int dirty2ms_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw,
+                    const void* d_dirty, const void* d_wgt, void* d_vis);
+}  // namespace cg
+
+#define CG_CUDA(call)                                  \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) {                           \
+      cg::set_last_error(cudaGetErrorString(e_));      \
+      return (e_ == cudaErrorMemoryAllocation) ? CG_ERR_NOMEM : CG_ERR_CUDA; \
+    }                                                  \
+  } while (0)
+
+#define CG_CUFFT(call)                                 \
+  do {                                                 \
+    cufftResult r_ = (call);                           \
+    if (r_ != CUFFT_SUCCESS) {                         \
+      cg::set_last_error("cuFFT error");               \
+      return (r_ == CUFFT_ALLOC_FAILED) ? CG_ERR_NOMEM : CG_ERR_CUFFT; \
+    }                                                  \
+  } while (0)
+
+#define CG_TRY(expr)            \
+  do {                          \
+    int s_ = (expr);            \
+    if (s_ > 1) return s_;      \
+  } while (0)
+
+namespace cg {
+void set_last_error(const char* msg);
+// number of kernels this library has launched (process-wide)
+void count_launches(long long n);
+}

@@ -1,0 +1,42 @@
+// Launchers of the device kernels (one per pipeline stage).  All take the
+// stream explicitly and return a status code; none synchronizes.
+#pragma once
+#include "cg_internal.cuh"
+
+namespace cg {
+
+// ---- binning (cg_bin.cu) ----
+int launch_wminmax(const double* d_uvw, int64_t M, unsigned long long* d_mm, int* d_bad,
+                   cudaStream_t st);
+double decode_ordered(unsigned long long k);
+
+// Stable LSD radix sort of the reference's hive-major cell keys.
+// Workspace sizes in bytes for M rows and a key of key_bytes (4 or 8).
+size_t bin_workspace_bytes(int64_t M, int key_bytes);
+int launch_bin(const double* d_uvw, int64_t M, const Geom& g, int key_bytes, void* d_ws,
+               size_t ws_bytes, int* d_perm, void* d_sorted_keys, int* d_hive_start,
+               cudaStream_t st);
+
+template <typename T>
+int launch_build_stream(const int* d_perm, int64_t M, const double* d_uvw, const T* d_vis,
+                        const T* d_wgt, const Geom& g, bool grid_dir, Rec<T>* d_recs,
+                        cudaStream_t st);
+
+// ---- spreading / interpolation (cg_spread.cu) ----
+template <typename T>
+int launch_grid(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, const Geom& g, T* d_fw,
+                int method, cudaStream_t st);
+template <typename T>
+int launch_degrid(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_start, int64_t M,
+                  const Geom& g, const T* d_fw, T* d_vis, int method, cudaStream_t st);
+
+// ---- w stage (cg_wstage.cu) ----
+int launch_quarter(const Geom& g, const Quad& q, double* d_K3q, double* d_zq, cudaStream_t st);
+template <typename T>
+int launch_wdft_deconv(const T* d_fw, const Geom& g, const double* d_K1, const double* d_K2,
+                       const double* d_K3q, const double* d_zq, T* d_dirty, cudaStream_t st);
+template <typename T>
+int launch_plane_fill(const T* d_dirty, const Geom& g, const double* d_K1, const double* d_K2,
+                      const double* d_K3q, const double* d_zq, T* d_fw, cudaStream_t st);
+
+}  // namespace cg

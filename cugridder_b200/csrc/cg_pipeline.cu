@@ -1,0 +1,471 @@
+// Host orchestration of ms2dirty / dirty2ms (improved W-stacking).
+//
+// Reference flow: ms2dirty_exec -> gridder_setting -> exec_vis2dirty
+// (cugridder.cu:276-404, :90-210; ra_exec.cu:184-468) and dirty2ms_exec ->
+// exec_dirty2vis (cugridder.cu:406-538; ra_exec.cu:470-680).  The scalar plan
+// math below restates setup_conv_opts, get_num_cells, next235beven,
+// set_nhg_w and setup_gridder_plan; everything else runs as stream-ordered
+// kernels with no intermediate device synchronization (one small read of the
+// w range per call).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "cg_launch.cuh"
+#include "cg_plan.cuh"
+
+namespace cg {
+
+// ------------------------------------------------------------ scalar plan math
+// next235beven: common_utils.cu:76-101
+static int next235beven(int n, int b) {
+  if (n <= 2) return 2;
+  if (n % 2 == 1) n += 1;
+  int nplus = n - 2, numdiv = 2;
+  while ((numdiv > 1) || (nplus % b != 0)) {
+    nplus += 2;
+    numdiv = nplus;
+    while (numdiv % 2 == 0) numdiv /= 2;
+    while (numdiv % 3 == 0) numdiv /= 3;
+    while (numdiv % 5 == 0) numdiv /= 5;
+  }
+  return nplus;
+}
+
+// setup_conv_opts: conv_interp_invoker.cu:49-119
+static int setup_conv_opts(double eps, double sigma, double eps_floor, int& kw, double& beta,
+                           double& c) {
+  int st = CG_OK;
+  if (!(sigma > 1.0)) return CG_ERR_ARG;
+  if (!(eps >= eps_floor)) {  // also catches NaN / non-positive eps
+    eps = eps_floor;
+    st = CG_WARN_EPS_CLIPPED;
+  }
+  kw = (int)std::ceil(-std::log10(eps / 10.0));
+  if (sigma != 2.0) kw = (int)std::ceil(-std::log(eps) / (kPi * std::sqrt(1.0 - 1.0 / sigma)));
+  kw = std::max(2, kw);
+  kw = std::min(kMaxW, kw);
+  double betaoverns = 2.30;
+  if (kw == 2) betaoverns = 2.20;
+  if (kw == 3) betaoverns = 2.26;
+  if (kw == 4) betaoverns = 2.38;
+  if (sigma != 2.0) betaoverns = 0.97 * kPi * (1 - 1 / (2 * sigma));
+  beta = betaoverns * (double)kw;
+  c = 4.0 / (double)(kw * kw);
+  return st;
+}
+
+// get_num_cells: conv_interp_invoker.cu:30-47
+static int get_num_cells(int ms, double sigma, int kw) {
+  int nf = (int)(sigma * ms);
+  if (nf < 2 * kw) nf = 2 * kw;
+  return next235beven(nf, 1);
+}
+
+// set_nhg_w: utils.cu:670-709
+static void set_nhg_w(double S, double X, int kw, double sigma, int& nf, double& h, double& gam) {
+  int nss = kw + 1;
+  double Xsafe = X, Ssafe = S;
+  if (X == 0.0) {
+    if (S == 0.0) {
+      Xsafe = 1.0;
+      Ssafe = 1.0;
+    } else {
+      Xsafe = std::max(Xsafe, 1 / S);
+    }
+  } else {
+    Ssafe = std::max(Ssafe, 1 / X);
+  }
+  double nfd = 2.0 * sigma * Ssafe * Xsafe / kPi + nss;
+  if (!std::isfinite(nfd)) nfd = 0.0;
+  double capped = std::min(nfd, 1.0e9);
+  nf = (int)capped;
+  nf = nf % 2 + nf;
+  if (nf < 2 * kw) nf = 2 * kw;
+  h = 2 * kPi / nf;
+  gam = (double)nf / (2.0 * sigma * Ssafe);
+}
+
+// Gauss-Legendre nodes on [-1,1] (Newton on the Legendre recurrence),
+// decreasing order; the fseries uses the first (positive) half of 2p nodes
+// (deconv.cu:80-93).
+static void gauss_legendre(int n, double* x, double* w) {
+  for (int k = 0; k < n; k++) {
+    double z = std::cos(kPi * (k + 0.75) / (n + 0.5)), pp = 0;
+    for (int it = 0; it < 100; it++) {
+      double p0 = 1.0, p1 = z;
+      for (int j = 2; j <= n; j++) {
+        double p2 = ((2.0 * j - 1.0) * z * p1 - (j - 1.0) * p0) / j;
+        p0 = p1;
+        p1 = p2;
+      }
+      pp = n * (z * p1 - p0) / (z * z - 1.0);
+      double dz = p1 / pp;
+      z -= dz;
+      if (std::fabs(dz) < 1e-16) break;
+    }
+    double p0 = 1.0, p1 = z;
+    for (int j = 2; j <= n; j++) {
+      double p2 = ((2.0 * j - 1.0) * z * p1 - (j - 1.0) * p0) / j;
+      p0 = p1;
+      p1 = p2;
+    }
+    pp = n * (z * p1 - p0) / (z * z - 1.0);
+    x[k] = z;
+    w[k] = 2.0 / ((1.0 - z * z) * pp * pp);
+  }
+}
+
+// quadrature of the ES kernel Fourier series (deconv.cu:80-93)
+static void make_quad(int kw, double beta, double c, Quad& q) {
+  double alpha = kw / 2.0;
+  int p = (int)(2 + 3.0 * alpha);
+  double x[2 * kMaxQuad], w[2 * kMaxQuad];
+  gauss_legendre(2 * p, x, w);
+  q.p = p;
+  for (int n = 0; n < p; n++) {
+    double xn = x[n] * alpha;
+    double phi = (std::fabs(xn) <= alpha) ? std::exp(beta * std::sqrt(1.0 - c * xn * xn)) : 0.0;
+    q.x[n] = xn;
+    q.g[n] = alpha * w[n] * phi;
+  }
+}
+
+// fwkerhalf{1,2} (deconv.cu:12-26): (-1)^k folded into the cosine
+static void fseries_uv(const Quad& q, int nf, double* out) {
+  int N = nf / 2 + 1;
+  for (int k = 0; k < N; k++) {
+    double s = 0;
+    for (int i = 0; i < q.p; i++) s += q.g[i] * std::cos((q.x[i] - N + 1) / (double)(N - 1) * kPi * k);
+    out[k] = 2 * s;
+  }
+}
+
+// ------------------------------------------------------------ buffers
+int ensure(cg_dev_buf& b, size_t bytes) {
+  if (bytes == 0) bytes = 256;
+  if (b.cap >= bytes) return CG_OK;
+  if (b.p) {
+    cudaFree(b.p);
+    b.p = nullptr;
+    b.cap = 0;
+  }
+  CG_CUDA(cudaMalloc(&b.p, bytes));
+  b.cap = bytes;
+  return CG_OK;
+}
+
+void release(cg_dev_buf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+}
+
+size_t workspace_bytes(const cg_plan_s* P) {
+  const cg_dev_buf* bs[] = {&P->mm,   &P->K1,    &P->K2,         &P->K3q,   &P->zq,
+                            &P->grid, &P->recs,  &P->perm,       &P->skeys, &P->hive_start,
+                            &P->binws, &P->fftwork, &P->io_uvw, &P->io_vis, &P->io_wgt,
+                            &P->io_dirty};
+  size_t s = 0;
+  for (auto b : bs) s += b->cap;
+  return s;
+}
+
+// ------------------------------------------------------------ stage timers
+int timer_begin(cg_plan_s* P, int dir) {
+  cg_stage_timer& T = P->timer;
+  if (!T.on) return CG_OK;
+  if (!T.created) {
+    for (int s = 0; s < 2; s++)
+      for (int i = 0; i <= kMaxStages; i++) CG_CUDA(cudaEventCreate(&T.ev[s][i]));
+    T.created = true;
+  }
+  T.cur ^= 1;
+  T.n[T.cur] = 0;
+  T.dir[T.cur] = dir;
+  T.pending[T.cur] = true;
+  timer_mark(P);
+  return CG_OK;
+}
+
+void timer_mark(cg_plan_s* P) {
+  cg_stage_timer& T = P->timer;
+  if (!T.on || !T.created || T.n[T.cur] > kMaxStages) return;
+  cudaEventRecord(T.ev[T.cur][T.n[T.cur]], P->stream);
+  T.n[T.cur]++;
+}
+
+// reads a finished event set (its stream work is complete) into the totals
+void timer_flush(cg_plan_s* P, int set) {
+  cg_stage_timer& T = P->timer;
+  if (!T.created || !T.pending[set]) return;
+  for (int i = 1; i < T.n[set]; i++) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, T.ev[set][i - 1], T.ev[set][i]) == cudaSuccess)
+      T.acc[T.dir[set]][i - 1] += ms;
+  }
+  cudaGetLastError();
+  T.calls[T.dir[set]]++;
+  T.pending[set] = false;
+}
+
+int plan_configure(cg_plan_s* P, int nx, int ny, double fov, double eps, double sigma, int sign,
+                   int precision) {
+  if (nx <= 0 || ny <= 0 || (nx & 1) || (ny & 1)) {
+    set_last_error("nxdirty and nydirty must be positive and even");
+    return CG_ERR_ARG;
+  }
+  if (!(fov > 0.0) || !std::isfinite(fov)) {
+    set_last_error("fov must be positive and finite");
+    return CG_ERR_ARG;
+  }
+  if (precision != CG_PREC_FP64 && precision != CG_PREC_FP32) return CG_ERR_ARG;
+  bool same = P->kw > 0 && P->nx == nx && P->ny == ny && P->fov == fov && P->eps == eps &&
+              P->sigma == sigma && P->sign == sign && P->precision == precision;
+  if (same) return CG_OK;
+  double floor_eps = (precision == CG_PREC_FP64) ? 1.1e-16 : 6e-8;  // utils.h:34-38
+  int kw;
+  double beta, c;
+  int st = setup_conv_opts(eps, sigma, floor_eps, kw, beta, c);
+  if (st > 1) {
+    set_last_error("sigma must be > 1");
+    return st;
+  }
+  int nf1 = get_num_cells(ny, sigma, kw), nf2 = get_num_cells(nx, sigma, kw);
+  if (nf1 > 65535 || nf2 > 65535) {
+    set_last_error("grid larger than 65535 cells per axis");
+    return CG_ERR_SIZE;
+  }
+  P->nx = nx;
+  P->ny = ny;
+  P->fov = fov;
+  P->eps = eps;
+  P->sigma = sigma;
+  P->sign = sign;
+  P->precision = precision;
+  P->eps_status = st;
+  P->kw = kw;
+  P->beta = beta;
+  P->es_c = c;
+  P->nf1 = nf1;
+  P->nf2 = nf2;
+  make_quad(kw, beta, c, P->quad);
+  std::vector<double> k1(nf1 / 2 + 1), k2(nf2 / 2 + 1);
+  fseries_uv(P->quad, nf1, k1.data());
+  fseries_uv(P->quad, nf2, k2.data());
+  CG_TRY(ensure(P->K1, k1.size() * 8));
+  CG_TRY(ensure(P->K2, k2.size() * 8));
+  CG_CUDA(cudaMemcpy(P->K1.p, k1.data(), k1.size() * 8, cudaMemcpyHostToDevice));
+  CG_CUDA(cudaMemcpy(P->K2.p, k2.data(), k2.size() * 8, cudaMemcpyHostToDevice));
+  size_t nq = (size_t)(ny / 2 + 1) * (nx / 2 + 1);
+  CG_TRY(ensure(P->K3q, nq * 8));
+  CG_TRY(ensure(P->zq, nq * 8));
+  return CG_OK;
+}
+
+// ------------------------------------------------------------ per-call geometry
+// setup_gridder_plan (cugridder.cu:29-86) with the w range from the device.
+static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw) {
+  if (nrow < 0 || nrow > 2147483647LL) {
+    set_last_error("nrow out of range");
+    return nrow < 0 ? CG_ERR_ARG : CG_ERR_SIZE;
+  }
+  if (!(freq > 0.0) || !std::isfinite(freq)) {
+    set_last_error("freq must be positive and finite");
+    return CG_ERR_ARG;
+  }
+  cudaStream_t st = P->stream;
+  CG_TRY(ensure(P->mm, 64));
+  if (!P->h_mm) CG_CUDA(cudaMallocHost(&P->h_mm, 64));
+  unsigned long long* d_mm = (unsigned long long*)P->mm.p;
+  int* d_bad = (int*)(d_mm + 2);
+  CG_TRY(launch_wminmax(d_uvw, nrow, d_mm, d_bad, st));
+  CG_CUDA(cudaMemcpyAsync(P->h_mm, d_mm, 24, cudaMemcpyDeviceToHost, st));
+  CG_CUDA(cudaStreamSynchronize(st));
+  timer_flush(P, P->timer.cur ^ 1);
+  if (((int*)(P->h_mm + 2))[0]) {
+    set_last_error("non-finite uvw coordinate");
+    return CG_ERR_ARG;
+  }
+  Geom g{};
+  g.N1 = P->ny;
+  g.N2 = P->nx;
+  g.nf1 = P->nf1;
+  g.nf2 = P->nf2;
+  g.kw = P->kw;
+  g.beta = P->beta;
+  g.es_c = P->es_c;
+  g.pixx = P->fov / 180.0 * kPi / (double)g.N2;
+  g.pixy = P->fov / 180.0 * kPi / (double)g.N1;
+  g.foc = freq / kSpeedOfLight;
+  g.sign = P->sign;
+  double wmin = 0, wmax = 0;
+  if (nrow > 0) {
+    double rmin = decode_ordered(P->h_mm[0]), rmax = decode_ordered(P->h_mm[1]);
+    // same rounding chain as eff_coords(); monotone in w
+    auto scale = [&](double w) { return (w * (g.foc * (double)g.sign)) * (2 * kPi); };
+    double a = scale(rmin), b = scale(rmax);
+    wmin = std::min(a, b);
+    wmax = std::max(a, b);
+  }
+  double l_min = 0 - 0.5 * g.pixx * g.N2;
+  double m_min = 0 - 0.5 * g.pixy * g.N1;
+  double temp = 1.0 - std::pow(l_min, 2) - std::pow(m_min, 2);
+  double n_lm = temp <= 0 ? 0 : std::sqrt(temp);
+  g.i_center = (wmax + wmin) / 2.0;
+  g.i_half_width = (wmax - wmin) / 2.0;
+  double o_min = n_lm - 1;
+  g.o_center = o_min / 2.0;
+  g.o_half_width = std::fabs(o_min / 2.0);
+  set_nhg_w(g.o_half_width, g.i_half_width, g.kw, P->sigma, g.nw, g.h, g.gamma);
+  if (g.nw > 65535) {
+    set_last_error("number of w planes too large");
+    return CG_ERR_SIZE;
+  }
+  g.nhx = (g.nf1 - 1) / 8 + 1;
+  g.nhy = (g.nf2 - 1) / 8 + 1;
+  g.nhz = g.nw;
+  P->geom = g;
+  P->nrow = nrow;
+  int64_t nh = (int64_t)g.nhx * g.nhy * g.nhz;
+  P->key_bytes = ((unsigned long long)nh * 64ULL <= 0xFFFFFFFFULL) ? 4 : 8;
+  size_t tsz = (P->precision == CG_PREC_FP64) ? 8 : 4;
+  size_t G = (size_t)g.nf1 * g.nf2 * g.nw;
+  CG_TRY(ensure(P->grid, G * 2 * tsz));
+  CG_TRY(ensure(P->hive_start, (size_t)(nh + 1) * 4));
+  CG_TRY(ensure(P->perm, (size_t)nrow * 4));
+  CG_TRY(ensure(P->skeys, (size_t)nrow * P->key_bytes));
+  CG_TRY(ensure(P->binws, bin_workspace_bytes(nrow, P->key_bytes)));
+  CG_TRY(ensure(P->recs, (size_t)nrow * (tsz == 8 ? sizeof(Rec<double>) : sizeof(Rec<float>))));
+  return CG_OK;
+}
+
+static int fft_exec(cg_plan_s* P, void* d_grid, int direction) {
+  const Geom& g = P->geom;
+  if (!P->fft_valid || P->fft_nf1 != g.nf1 || P->fft_nf2 != g.nf2 || P->fft_nw != g.nw ||
+      P->precision == -1) {
+    if (P->fft_valid) {
+      cufftDestroy(P->fft);
+      P->fft_valid = false;
+    }
+    CG_CUFFT(cufftCreate(&P->fft));
+    P->fft_valid = true;
+    CG_CUFFT(cufftSetAutoAllocation(P->fft, 0));
+    long long n[2] = {g.nf2, g.nf1};
+    size_t ws = 0;
+    cufftType t = (P->precision == CG_PREC_FP64) ? CUFFT_Z2Z : CUFFT_C2C;
+    CG_CUFFT(cufftMakePlanMany64(P->fft, 2, n, nullptr, 1, 0, nullptr, 1, 0, t, g.nw, &ws));
+    CG_TRY(ensure(P->fftwork, ws));
+    CG_CUFFT(cufftSetWorkArea(P->fft, P->fftwork.p));
+    P->fft_nf1 = g.nf1;
+    P->fft_nf2 = g.nf2;
+    P->fft_nw = g.nw;
+    P->fft_work_bytes = ws;
+  }
+  CG_CUFFT(cufftSetStream(P->fft, P->stream));
+  if (P->precision == CG_PREC_FP64)
+    CG_CUFFT(cufftExecZ2Z(P->fft, (cufftDoubleComplex*)d_grid, (cufftDoubleComplex*)d_grid, direction));
+  else
+    CG_CUFFT(cufftExecC2C(P->fft, (cufftComplex*)d_grid, (cufftComplex*)d_grid, direction));
+  return CG_OK;
+}
+
+template <typename T>
+static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T* d_wgt,
+                      T* d_dirty) {
+  const Geom& g = P->geom;
+  cudaStream_t st = P->stream;
+  int64_t M = P->nrow;
+  timer_mark(P);  // stage 0: w range + geometry
+  CG_TRY(launch_quarter(g, P->quad, (double*)P->K3q.p, (double*)P->zq.p, st));
+  timer_mark(P);  // 1: quarter tables
+  CG_TRY(launch_bin(d_uvw, M, g, P->key_bytes, P->binws.p, P->binws.cap, (int*)P->perm.p,
+                    P->skeys.p, (int*)P->hive_start.p, st));
+  timer_mark(P);  // 2: binning
+  if (P->stop_stage == 1) return CG_OK;
+  CG_TRY(launch_build_stream<T>((const int*)P->perm.p, M, d_uvw, d_vis, d_wgt, g, true,
+                                (Rec<T>*)P->recs.p, st));
+  timer_mark(P);  // 3: sorted stream
+  size_t G = (size_t)g.nf1 * g.nf2 * g.nw;
+  CG_CUDA(cudaMemsetAsync(P->grid.p, 0, G * 2 * sizeof(T), st));
+  CG_TRY(launch_grid<T>((const Rec<T>*)P->recs.p, (const int*)P->hive_start.p, M, g,
+                        (T*)P->grid.p, 0, st));
+  timer_mark(P);  // 4: gridding
+  if (P->stop_stage == 2) return CG_OK;
+  CG_TRY(fft_exec(P, P->grid.p, CUFFT_INVERSE));
+  timer_mark(P);  // 5: FFT
+  if (P->stop_stage == 3) return CG_OK;
+  CG_TRY(launch_wdft_deconv<T>((const T*)P->grid.p, g, (const double*)P->K1.p,
+                               (const double*)P->K2.p, (const double*)P->K3q.p,
+                               (const double*)P->zq.p, d_dirty, st));
+  timer_mark(P);  // 6: w-DFT + corrections
+  return CG_OK;
+}
+
+template <typename T>
+static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const T* d_wgt,
+                      T* d_vis) {
+  const Geom& g = P->geom;
+  cudaStream_t st = P->stream;
+  int64_t M = P->nrow;
+  timer_mark(P);  // stage 0: w range + geometry
+  CG_TRY(launch_quarter(g, P->quad, (double*)P->K3q.p, (double*)P->zq.p, st));
+  timer_mark(P);  // 1: quarter tables
+  CG_TRY(launch_bin(d_uvw, M, g, P->key_bytes, P->binws.p, P->binws.cap, (int*)P->perm.p,
+                    P->skeys.p, (int*)P->hive_start.p, st));
+  timer_mark(P);  // 2: binning
+  if (P->stop_stage == 1) return CG_OK;
+  CG_TRY(launch_plane_fill<T>(d_dirty, g, (const double*)P->K1.p, (const double*)P->K2.p,
+                              (const double*)P->K3q.p, (const double*)P->zq.p, (T*)P->grid.p, st));
+  timer_mark(P);  // 3: plane fill
+  if (P->stop_stage == 2) return CG_OK;
+  CG_TRY(fft_exec(P, P->grid.p, CUFFT_FORWARD));
+  timer_mark(P);  // 4: FFT
+  if (P->stop_stage == 3) return CG_OK;
+  CG_TRY(launch_build_stream<T>((const int*)P->perm.p, M, d_uvw, (const T*)nullptr, d_wgt, g,
+                                false, (Rec<T>*)P->recs.p, st));
+  timer_mark(P);  // 5: sorted stream
+  CG_TRY(launch_degrid<T>((const Rec<T>*)P->recs.p, (const int*)P->perm.p,
+                          (const int*)P->hive_start.p, M, g, (const T*)P->grid.p, d_vis, 0, st));
+  timer_mark(P);  // 6: degridding
+  return CG_OK;
+}
+
+int ms2dirty_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw,
+                    const void* d_vis, const void* d_wgt, void* d_dirty) {
+  if (!d_dirty || (nrow > 0 && (!d_uvw || !d_vis))) {
+    set_last_error("null pointer");
+    return CG_ERR_ARG;
+  }
+  CG_CUDA(cudaSetDevice(P->device));
+  CG_TRY(timer_begin(P, 0));
+  CG_TRY(prepare(P, nrow, freq, d_uvw));
+  size_t tsz = (P->precision == CG_PREC_FP64) ? 8 : 4;
+  if (nrow == 0) {
+    CG_CUDA(cudaMemsetAsync(d_dirty, 0, (size_t)P->nx * P->ny * 2 * tsz, P->stream));
+    return P->eps_status;
+  }
+  int st = (P->precision == CG_PREC_FP64)
+               ? ms2dirty_t<double>(P, d_uvw, (const double*)d_vis, (const double*)d_wgt, (double*)d_dirty)
+               : ms2dirty_t<float>(P, d_uvw, (const float*)d_vis, (const float*)d_wgt, (float*)d_dirty);
+  return st != CG_OK ? st : P->eps_status;
+}
+
+int dirty2ms_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw,
+                    const void* d_dirty, const void* d_wgt, void* d_vis) {
+  if (!d_dirty || (nrow > 0 && (!d_uvw || !d_vis))) {
+    set_last_error("null pointer");
+    return CG_ERR_ARG;
+  }
+  CG_CUDA(cudaSetDevice(P->device));
+  CG_TRY(timer_begin(P, 1));
+  CG_TRY(prepare(P, nrow, freq, d_uvw));
+  if (nrow == 0) return P->eps_status;
+  int st = (P->precision == CG_PREC_FP64)
+               ? dirty2ms_t<double>(P, d_uvw, (const double*)d_dirty, (const double*)d_wgt, (double*)d_vis)
+               : dirty2ms_t<float>(P, d_uvw, (const float*)d_dirty, (const float*)d_wgt, (float*)d_vis);
+  return st != CG_OK ? st : P->eps_status;
+}
+
+}  // namespace cg

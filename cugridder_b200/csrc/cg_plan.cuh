@@ -1,0 +1,70 @@
+// Plan object behind the C ABI.  Replaces the reference's CURAFFT_PLAN +
+// ragridder_plan pair (curafft_plan.h:74-150, ragridder_plan.h:36-56), which
+// is created, filled and freed inside every call (cugridder.cu:309-388); here
+// the plan owns its device workspace and cuFFT plan and keeps them resident
+// across calls.
+#pragma once
+#include <mutex>
+
+#include "cg_internal.cuh"
+
+struct cg_dev_buf {
+  void* p = nullptr;
+  size_t cap = 0;
+};
+
+// Per-stage CUDA-event timers (two event sets, so one call's events are read
+// back at the next call's w-range synchronization instead of adding a sync).
+constexpr int kMaxStages = 8;
+struct cg_stage_timer {
+  bool on = false;
+  bool created = false;
+  cudaEvent_t ev[2][kMaxStages + 1];
+  int n[2] = {0, 0};
+  int dir[2] = {0, 0};
+  bool pending[2] = {false, false};
+  int cur = 0;
+  double acc[2][kMaxStages] = {};
+  long long calls[2] = {0, 0};
+};
+
+struct cg_plan_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  // user configuration
+  int nx = 0, ny = 0, sign = -1, precision = CG_PREC_FP64;
+  double fov = 0, eps = 0, sigma = 2.0;
+  int eps_status = CG_OK;  // CG_WARN_EPS_CLIPPED when epsilon was clipped
+  // kernel (setup_conv_opts, conv_interp_invoker.cu:49-119)
+  int kw = 0;
+  double beta = 0, es_c = 0;
+  int nf1 = 0, nf2 = 0;
+  cg::Quad quad;
+  // last call
+  cg::Geom geom{};
+  int64_t nrow = 0;
+  int key_bytes = 4;
+  int stop_stage = 0;
+  // device buffers
+  cg_dev_buf mm, K1, K2, K3q, zq, grid, recs, perm, skeys, hive_start, binws, fftwork, io_uvw,
+      io_vis, io_wgt, io_dirty;
+  unsigned long long* h_mm = nullptr;  // pinned, 2 words + flag
+  // cuFFT
+  cufftHandle fft = 0;
+  bool fft_valid = false;
+  int fft_nf1 = 0, fft_nf2 = 0, fft_nw = 0;
+  size_t fft_work_bytes = 0;
+  cg_stage_timer timer;
+  std::mutex mu;
+};
+
+namespace cg {
+int plan_configure(cg_plan_s* P, int nx, int ny, double fov, double eps, double sigma, int sign,
+                   int precision);
+int ensure(cg_dev_buf& b, size_t bytes);
+void release(cg_dev_buf& b);
+size_t workspace_bytes(const cg_plan_s* P);
+int timer_begin(cg_plan_s* P, int dir);
+void timer_mark(cg_plan_s* P);
+void timer_flush(cg_plan_s* P, int set);
+}  // namespace cg

@@ -1,0 +1,184 @@
+/*
+ * cugridder.h -- C ABI of libcugridder.so, the B200 (sm_100a) gridder.
+ *
+ * Drop-in for the ms2dirty / dirty2ms path of RapidsAtHKUST/cuGridder.
+ * The first eight functions have exactly the reference's names, argument
+ * order, argument meaning and return convention (include/cugridder.h:37-47
+ * of the reference; definitions src/astro/cugridder.cu:541-571):
+ *
+ *   - uvw is a HOST array [nrow][3] (u, v, w in metres), row-major;
+ *   - vis is a HOST array of nrow complex values (input of ms2dirty,
+ *     output of dirty2ms);
+ *   - dirty is a HOST array [nxdirty][nydirty] complex, row-major
+ *     (output of ms2dirty, input of dirty2ms);
+ *   - wgt (the _2 variants) is a HOST array of nrow real weights; both
+ *     directions MULTIPLY by it (the reference's dirty2ms "divide" invoker
+ *     launches the multiply kernel, src/utils.cu:661-668);
+ *   - fov is the field of view in degrees on both axes; freq in Hz;
+ *   - the phase is exp(+2 pi i f/c (u l + v m + sign w (n-1))) for ms2dirty
+ *     and its conjugate for dirty2ms, l = (x - nx/2) fov/nx,
+ *     m = (y - ny/2) fov/ny (src/astro/precomp.cu:48-72);
+ *   - return 0 on success, 1 when epsilon was below the precision floor and
+ *     was clipped (the reference's ier = 1), >= 2 on error.  The library
+ *     never calls exit().
+ *
+ * Complex arrays are interleaved (re, im) pairs, layout-compatible with
+ * std::complex<T>, C99 _Complex and numpy complex64/complex128.
+ */
+#ifndef CUGRIDDER_B200_H
+#define CUGRIDDER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { double re, im; } cg_c128;
+typedef struct { float re, im; } cg_c64;
+
+/* status codes */
+#define CG_OK 0
+#define CG_WARN_EPS_CLIPPED 1 /* epsilon below the floor, clipped (reference ier = 1) */
+#define CG_ERR_ARG 2          /* invalid argument (sizes, null pointers, non-finite uvw) */
+#define CG_ERR_CUDA 3         /* CUDA runtime error */
+#define CG_ERR_CUFFT 4        /* cuFFT error */
+#define CG_ERR_NOMEM 5        /* device memory exhausted */
+#define CG_ERR_SIZE 6         /* problem too large for this build (index range) */
+#define CG_ERR_NOGPU 7        /* no CUDA device */
+
+/* ---------------- reference-compatible entry points ----------------
+ * FP64: ms2dirty_1/_2, dirty2ms_1/_2 (reference cugridder.h:37-47 with
+ * PCS=double, CPX=std::complex<double>). */
+int ms2dirty_2(int nrow, int nxdirty, int nydirty, double fov, double freq, double *uvw,
+               cg_c128 *vis, double *wgt, cg_c128 *dirty, double epsilon, double sigma,
+               int sign);
+int ms2dirty_1(int nrow, int nxdirty, int nydirty, double fov, double freq, double *uvw,
+               cg_c128 *vis, cg_c128 *dirty, double epsilon, double sigma, int sign);
+int dirty2ms_1(int nrow, int nxdirty, int nydirty, double fov, double freq, double *uvw,
+               cg_c128 *vis, cg_c128 *dirty, double epsilon, double sigma, int sign);
+int dirty2ms_2(int nrow, int nxdirty, int nydirty, double fov, double freq, double *uvw,
+               cg_c128 *vis, double *wgt, cg_c128 *dirty, double epsilon, double sigma,
+               int sign);
+
+/* FP32 twins ms2dirtyf_1/_2, dirty2msf_1/_2 (reference cugridder.h:21-31,
+ * -DSINGLE: PCS=float).  uvw arrives in float as in the reference; the
+ * library widens it to FP64 for the coordinate scaling and the
+ * integer/fraction split, and grids in FP32. */
+int ms2dirtyf_2(int nrow, int nxdirty, int nydirty, float fov, float freq, float *uvw,
+                cg_c64 *vis, float *wgt, cg_c64 *dirty, float epsilon, float sigma, int sign);
+int ms2dirtyf_1(int nrow, int nxdirty, int nydirty, float fov, float freq, float *uvw,
+                cg_c64 *vis, cg_c64 *dirty, float epsilon, float sigma, int sign);
+int dirty2msf_1(int nrow, int nxdirty, int nydirty, float fov, float freq, float *uvw,
+                cg_c64 *vis, cg_c64 *dirty, float epsilon, float sigma, int sign);
+int dirty2msf_2(int nrow, int nxdirty, int nydirty, float fov, float freq, float *uvw,
+                cg_c64 *vis, float *wgt, cg_c64 *dirty, float epsilon, float sigma, int sign);
+
+/* ---------------- precision-split host entry points ----------------
+ * No reference counterpart: same argument order as ms2dirty_2 / dirty2ms_2,
+ * but uvw stays FP64 while vis, wgt and dirty are FP32 (complex64 / float).
+ * wgt may be NULL. */
+int cg_ms2dirty_mixed(int64_t nrow, int nxdirty, int nydirty, double fov, double freq,
+                      const double *uvw, const cg_c64 *vis, const float *wgt, cg_c64 *dirty,
+                      double epsilon, double sigma, int sign);
+int cg_dirty2ms_mixed(int64_t nrow, int nxdirty, int nydirty, double fov, double freq,
+                      const double *uvw, cg_c64 *vis, const float *wgt, const cg_c64 *dirty,
+                      double epsilon, double sigma, int sign);
+
+/* ---------------- plan API: device pointers, stream ordered ----------------
+ * Replaces the reference's gridder_setting / gridder_execution /
+ * gridder_destroy (reference cugridder.h:33-36; cugridder.cu:90-257) with a
+ * reusable plan whose workspace stays resident in HBM across calls.
+ *
+ * precision: CG_PREC_FP64  uvw f64, vis/dirty complex128, wgt f64
+ *            CG_PREC_FP32  uvw f64, vis/dirty complex64,  wgt f32
+ * stream:    a cudaStream_t (NULL = legacy default stream).  Calls are
+ *            stream ordered; each call performs one small device-to-host read
+ *            (the w range) and therefore synchronizes the stream once.
+ * All pointers passed to cg_plan_ms2dirty / cg_plan_dirty2ms are DEVICE
+ * pointers. d_wgt may be NULL. */
+#define CG_PREC_FP64 0
+#define CG_PREC_FP32 1
+
+typedef struct cg_plan_s cg_plan;
+
+typedef struct {
+    int kw;            /* kernel width W */
+    double beta;       /* ES beta */
+    int nf1, nf2;      /* grid sizes: nf1 <- nydirty, nf2 <- nxdirty */
+    int nw;            /* number of w planes of the last call */
+    double i_center, i_half_width, o_center, o_half_width, gamma, h;
+    double pixelsize_x, pixelsize_y;
+    int nhive[3];
+    int64_t nrow;      /* rows of the last call */
+    size_t workspace_bytes;
+} cg_plan_info;
+
+int cg_plan_create(cg_plan **plan, int nxdirty, int nydirty, double fov, double epsilon,
+                   double sigma, int sign, int precision, void *stream);
+int cg_plan_set_stream(cg_plan *plan, void *stream);
+int cg_plan_ms2dirty(cg_plan *plan, int64_t nrow, double freq, const double *d_uvw,
+                     const void *d_vis, const void *d_wgt, void *d_dirty);
+int cg_plan_dirty2ms(cg_plan *plan, int64_t nrow, double freq, const double *d_uvw,
+                     const void *d_dirty, const void *d_wgt, void *d_vis);
+int cg_plan_get_info(const cg_plan *plan, cg_plan_info *info);
+int cg_plan_destroy(cg_plan *plan);
+
+/* ---------------- inspection (tests / tools) ----------------
+ * After a call, copies an internal device buffer of the plan to HOST memory:
+ *   CG_BUF_HIVE_START  int32  [nhive0*nhive1*nhive2 + 1]  first sorted row of
+ *                      each 8x8x1 hive: the reference's hive_count
+ *                      (conv_interp_invoker.cu:121-224)
+ *   CG_BUF_PERM        int32  [nrow]  original row index of each sorted row
+ *   CG_BUF_SORTED_KEYS int64  [nrow]  hive-major cell key of each sorted row
+ *                      (the reference's histogram_3d_sparse key,
+ *                      utils.cu:105-132)
+ *   CG_BUF_GRID        complex (precision) [nw][nf2][nf1], the grid after the
+ *                      stage selected by cg_plan_set_stop_stage
+ *   CG_BUF_FSERIES_1 / _2  f64 [nf1/2+1] / [nf2/2+1] kernel Fourier series
+ *                      (deconv.cu:12-26, with the (-1)^k fold)
+ *   CG_BUF_FSERIES_W   f64 [(nx/2+1)*(ny/2+1)] w kernel correction on the
+ *                      quarter image (deconv.cu:49-65)
+ * bytes must be at least the size of the buffer; returns CG_ERR_ARG if not. */
+#define CG_BUF_HIVE_START 1
+#define CG_BUF_PERM 2
+#define CG_BUF_SORTED_KEYS 3
+#define CG_BUF_GRID 4
+#define CG_BUF_FSERIES_1 5
+#define CG_BUF_FSERIES_2 6
+#define CG_BUF_FSERIES_W 7
+int cg_plan_copy_buffer(cg_plan *plan, int which, void *host_dst, size_t bytes,
+                        size_t *bytes_needed);
+
+/* Stops the next calls after a stage (testing): 0 = run to the end,
+ * 1 = after binning, 2 = after gridding (ms2dirty) / plane fill (dirty2ms),
+ * 3 = after the FFT. */
+int cg_plan_set_stop_stage(cg_plan *plan, int stage);
+
+/* Per-stage CUDA-event timers of a plan (profiling; off by default).
+ * Stages of ms2dirty: 0 w range, 1 quarter tables, 2 binning, 3 sorted
+ * stream, 4 gridding, 5 FFT, 6 w-DFT + corrections.  Stages of dirty2ms:
+ * 0 w range, 1 quarter tables, 2 binning, 3 plane fill, 4 FFT, 5 sorted
+ * stream, 6 degridding.  cg_plan_set_timing resets the totals;
+ * cg_plan_get_timing synchronizes the plan's stream and returns the summed
+ * milliseconds per stage of direction 0 (ms2dirty) or 1 (dirty2ms). */
+int cg_plan_set_timing(cg_plan *plan, int on);
+int cg_plan_get_timing(cg_plan *plan, int direction, double *stage_ms, int cap, int *nstages,
+                       long long *ncalls);
+
+/* Host-pointer calls above keep one cached plan per precision so that
+ * repeated calls reuse device workspace; this frees it. */
+int cg_release_cache(void);
+
+/* Number of kernels libcugridder.so has launched in this process (its own
+ * kernels; cuFFT's are not counted). */
+long long cg_kernel_launches(void);
+
+const char *cg_last_error(void);
+int cg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CUGRIDDER_B200_H */

@@ -156,7 +156,12 @@ static inline double og_shift_rescale(double x, int N)
 {
     double t = x - floor(x / OG_M_2PI) * OG_M_2PI;
     double s = t - (double)(t >= OG_PI) * OG_M_2PI;
-    return (s * OG_M_1_2PI + 0.5) * N;
+    double X = (s * OG_M_1_2PI + 0.5) * N;
+    /* a value rounding onto N (or below 0) is folded back into [0, N); the
+     * reference keys such a row one hive row off -- a measure-zero case */
+    if (X >= (double)N) X -= (double)N;
+    if (X < 0.0) X += (double)N;
+    return X;
 }
 
 /* Plan setup: gridder_setting + setup_gridder_plan (cugridder.cu:29-210).
