@@ -7,6 +7,7 @@
 // share one cached plan per precision so repeated calls reuse HBM workspace;
 // cg_release_cache() frees it.  Errors are returned, never exit()ed.
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -204,6 +205,7 @@ int cg_plan_create(cg_plan** plan, int nxdirty, int nydirty, double fov, double 
   cg_plan_s* P = new cg_plan_s();
   cudaGetDevice(&P->device);
   P->stream = (cudaStream_t)stream;
+  if (const char* m = getenv("CG_GRID_METHOD")) P->grid_method = atoi(m) == 0 ? 0 : 1;
   st = cg::plan_configure(P, nxdirty, nydirty, fov, epsilon, sigma, sign, precision);
   if (st > 1) {
     destroy_plan(P);
@@ -259,6 +261,12 @@ int cg_plan_get_info(const cg_plan* plan, cg_plan_info* info) {
 
 int cg_plan_destroy(cg_plan* plan) {
   destroy_plan(plan);
+  return CG_OK;
+}
+
+int cg_plan_set_method(cg_plan* plan, int method) {
+  if (!plan || method < 0 || method > 1) return CG_ERR_ARG;
+  plan->grid_method = method;
   return CG_OK;
 }
 

@@ -81,6 +81,13 @@ __device__ __forceinline__ int taps(T f, T beta, T c, T* k) {
   return o;
 }
 
+// true modulo (any number of periods)
+__device__ __forceinline__ int modi(int i, int n) {
+  i %= n;
+  return i < 0 ? i + n : i;
+}
+
+// one-period wrap: i in [-n, 2n)
 __device__ __forceinline__ int wrapi(int i, int n) {
   i = (i >= n) ? i - n : i;
   return (i < 0) ? i + n : i;

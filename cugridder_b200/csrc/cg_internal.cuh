@@ -55,6 +55,15 @@ struct alignas(16) Rec {
   T c[2];
 };
 
+// Tiling of the grid for the tiled spreading / interpolation kernels: tiles of
+// TX x TY cells (multiples of the 8x8 hive) times batches of PB planes.
+struct TileCfg {
+  int TX, TY, PB;
+  int ntx, nty, npb, nitems;
+  int threads;
+  size_t smem;
+};
+
 // ---- pipeline entry points (cg_pipeline.cu) ----
 }  // namespace cg
 

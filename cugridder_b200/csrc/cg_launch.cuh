@@ -23,12 +23,19 @@ int launch_build_stream(const int* d_perm, int64_t M, const double* d_uvw, const
                         cudaStream_t st);
 
 // ---- spreading / interpolation (cg_spread.cu) ----
+// method 0: direct (global atomics / global gathers); 1: tiled (shared memory).
+// d_counter: one device int used as the work-queue head of the tiled kernels.
+constexpr int kGridDirect = 0;
+constexpr int kGridTiled = 1;
+template <typename T>
+TileCfg grid_tiling(const Geom& g, bool degrid);
 template <typename T>
 int launch_grid(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, const Geom& g, T* d_fw,
-                int method, cudaStream_t st);
+                int method, int* d_counter, cudaStream_t st);
 template <typename T>
 int launch_degrid(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_start, int64_t M,
-                  const Geom& g, const T* d_fw, T* d_vis, int method, cudaStream_t st);
+                  const Geom& g, const T* d_fw, T* d_vis, int method, int* d_counter,
+                  cudaStream_t st);
 
 // ---- w stage (cg_wstage.cu) ----
 int launch_quarter(const Geom& g, const Quad& q, double* d_K3q, double* d_zq, cudaStream_t st);

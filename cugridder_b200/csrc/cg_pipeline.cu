@@ -371,6 +371,9 @@ static int fft_exec(cg_plan_s* P, void* d_grid, int direction) {
   return CG_OK;
 }
 
+// work-queue head of the tiled kernels: a word of the small scratch buffer
+static int* queue_counter(cg_plan_s* P) { return (int*)((char*)P->mm.p + 32); }
+
 template <typename T>
 static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T* d_wgt,
                       T* d_dirty) {
@@ -387,10 +390,8 @@ static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T
   CG_TRY(launch_build_stream<T>((const int*)P->perm.p, M, d_uvw, d_vis, d_wgt, g, true,
                                 (Rec<T>*)P->recs.p, st));
   timer_mark(P);  // 3: sorted stream
-  size_t G = (size_t)g.nf1 * g.nf2 * g.nw;
-  CG_CUDA(cudaMemsetAsync(P->grid.p, 0, G * 2 * sizeof(T), st));
   CG_TRY(launch_grid<T>((const Rec<T>*)P->recs.p, (const int*)P->hive_start.p, M, g,
-                        (T*)P->grid.p, 0, st));
+                        (T*)P->grid.p, P->grid_method, queue_counter(P), st));
   timer_mark(P);  // 4: gridding
   if (P->stop_stage == 2) return CG_OK;
   CG_TRY(fft_exec(P, P->grid.p, CUFFT_INVERSE));
@@ -427,7 +428,8 @@ static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const
                                 false, (Rec<T>*)P->recs.p, st));
   timer_mark(P);  // 5: sorted stream
   CG_TRY(launch_degrid<T>((const Rec<T>*)P->recs.p, (const int*)P->perm.p,
-                          (const int*)P->hive_start.p, M, g, (const T*)P->grid.p, d_vis, 0, st));
+                          (const int*)P->hive_start.p, M, g, (const T*)P->grid.p, d_vis,
+                          P->grid_method, queue_counter(P), st));
   timer_mark(P);  // 6: degridding
   return CG_OK;
 }

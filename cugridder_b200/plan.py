@@ -64,6 +64,10 @@ class Plan:
         _lib.check(self._lib.cg_plan_get_info(self._h, ctypes.byref(inf)))
         return inf.as_dict()
 
+    def set_method(self, method):
+        """1 = tiled shared-memory spreading/interpolation (default), 0 = direct."""
+        _lib.check(self._lib.cg_plan_set_method(self._h, int(method)))
+
     def set_stop_stage(self, stage):
         _lib.check(self._lib.cg_plan_set_stop_stage(self._h, int(stage)))
 
