@@ -21,6 +21,7 @@
 // global gathers (kept as a cross-check).
 #include <algorithm>
 #include <cstdlib>
+#include <type_traits>
 
 #include "cg_coords.cuh"
 #include "cg_launch.cuh"
@@ -219,6 +220,11 @@ __device__ __forceinline__ int find_segment(const int* __restrict__ pref, int ns
 }
 
 // ---------------------------------------------------------------- gridding
+// Shared accumulator: planar re / im arrays, row stride RS = TX + 8 so that
+// the bank of cell (x, y) is (x + 8 y) mod 32: the rows of a warp (spread over
+// one 8x8 hive) hit distinct banks.
+__host__ __device__ __forceinline__ int acc_row_stride(int TX) { return TX + 8; }
+
 template <typename T, int W>
 __global__ void __launch_bounds__(512) k_grid_tiled(const Rec<T>* __restrict__ recs,
                                                     const int* __restrict__ hive_start, Geom g,
@@ -227,9 +233,11 @@ __global__ void __launch_bounds__(512) k_grid_tiled(const Rec<T>* __restrict__ r
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int lo = Halo<W>::lo, hi = Halo<W>::hi;
   const int TX = tc.TX, TY = tc.TY, PB = tc.PB;
-  const int ncell = TX * TY * PB;
-  T* acc = (T*)smem;
-  int* tb = (int*)(acc + 2 * (size_t)ncell);
+  const int RS = acc_row_stride(TX);
+  const int nacc = RS * TY * PB;
+  T* acc_re = (T*)smem;
+  T* acc_im = acc_re + nacc;
+  int* tb = (int*)(acc_im + nacc);
   const int ts = nslots_max + 1;
   SegTable t{tb, tb + ts, tb + 2 * ts, tb + 3 * ts, tb + 4 * ts};
   __shared__ int s_warp[33];
@@ -238,6 +246,7 @@ __global__ void __launch_bounds__(512) k_grid_tiled(const Rec<T>* __restrict__ r
   const int nf1 = g.nf1, nf2 = g.nf2, nw = g.nw;
   const size_t plane = (size_t)nf1 * nf2;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  const int ncell = TX * TY * PB;
 
   for (;;) {
     if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
@@ -247,11 +256,29 @@ __global__ void __launch_bounds__(512) k_grid_tiled(const Rec<T>* __restrict__ r
     const int tix = item % tc.ntx, tiy = (item / tc.ntx) % tc.nty, tib = item / (tc.ntx * tc.nty);
     const int tx0 = tix * TX, ty0 = tiy * TY, p0 = tib * PB;
     const int tx1 = min(tx0 + TX, nf1), ty1 = min(ty0 + TY, nf2), p1 = min(p0 + PB, nw);
-    for (int i = threadIdx.x; i < 2 * ncell; i += blockDim.x) acc[i] = (T)0;
+    const int wx = tx1 - tx0;
     const int nslots = build_segments(g, hive_start, floordiv8(tx0 - hi), floordiv8(tx1 - 1 + lo),
                                       floordiv8(ty0 - hi), floordiv8(ty1 - 1 + lo), p0 - hi,
                                       p1 - 1 + lo, t, s_warp);
     const int total = t.pref[nslots];
+    if (total == 0) {
+      // no row reaches this tile: write zeros straight to the grid
+      for (int i = threadIdx.x; i < ncell; i += blockDim.x) {
+        const int x = i % TX, y = (i / TX) % TY, z = i / (TX * TY);
+        if (x < wx && ty0 + y < ty1 && p0 + z < p1) {
+          const size_t o = (size_t)(p0 + z) * plane + (size_t)(ty0 + y) * nf1 + tx0 + x;
+          fw[2 * o] = (T)0;
+          fw[2 * o + 1] = (T)0;
+        }
+      }
+      __syncthreads();
+      continue;
+    }
+    for (int i = threadIdx.x; i < nacc; i += blockDim.x) {
+      acc_re[i] = (T)0;
+      acc_im[i] = (T)0;
+    }
+    __syncthreads();
     // within a chunk of blockDim rows, lane-major order keeps the lanes of a
     // warp on different cells; every row is visited exactly once
     for (int q0 = 0; q0 < total; q0 += blockDim.x) {
@@ -278,27 +305,27 @@ __global__ void __launch_bounds__(512) k_grid_tiled(const Rec<T>* __restrict__ r
         const T cr = r.c[0] * kz[z - oz], ci = r.c[1] * kz[z - oz];
         for (int y = ya; y < yb; y++) {
           const T vr = cr * ky[y - oy], vi = ci * ky[y - oy];
-          T* row = acc + 2 * (((z - p0) * TY + (y - ty0)) * TX - tx0);
+          const int rowo = ((z - p0) * TY + (y - ty0)) * RS - tx0;
 #pragma unroll
           for (int e = 0; e < W; e++) {
             const int x = ox + e;
             if (x >= xa && x < xb) {
-              atomicAdd(row + 2 * x, vr * kx[e]);
-              atomicAdd(row + 2 * x + 1, vi * kx[e]);
+              atomicAdd(acc_re + rowo + x, vr * kx[e]);
+              atomicAdd(acc_im + rowo + x, vi * kx[e]);
             }
           }
         }
       }
     }
     __syncthreads();
-    // flush: every cell of the tile written once
-    const int wx = tx1 - tx0;
+    // flush: every cell of the tile written once, coalesced along x
     for (int i = threadIdx.x; i < ncell; i += blockDim.x) {
       const int x = i % TX, y = (i / TX) % TY, z = i / (TX * TY);
       if (x < wx && ty0 + y < ty1 && p0 + z < p1) {
         const size_t o = (size_t)(p0 + z) * plane + (size_t)(ty0 + y) * nf1 + tx0 + x;
-        fw[2 * o] = acc[2 * i];
-        fw[2 * o + 1] = acc[2 * i + 1];
+        const int a = (z * TY + y) * RS + x;
+        fw[2 * o] = acc_re[a];
+        fw[2 * o + 1] = acc_im[a];
       }
     }
     __syncthreads();
@@ -319,9 +346,10 @@ __global__ void __launch_bounds__(512) k_degrid_tiled(const Rec<T>* __restrict__
   const int nw = g.nw, nf1 = g.nf1, nf2 = g.nf2;
   const bool all_planes = (PB >= nw);
   const int SX = TX + lo + hi, SY = TY + lo + hi, SZ = all_planes ? nw : PB + lo + hi;
+  const int SXP = SX + 1;  // padded row stride (complex elements)
   const int nstage = SX * SY * SZ;
   T* stg = (T*)smem;
-  int* tb = (int*)(stg + 2 * (size_t)nstage);
+  int* tb = (int*)(stg + 2 * (size_t)SXP * SY * SZ);
   const int ts = nslots_max + 1;
   SegTable t{tb, tb + ts, tb + 2 * ts, tb + 3 * ts, tb + 4 * ts};
   __shared__ int s_warp[33];
@@ -339,18 +367,21 @@ __global__ void __launch_bounds__(512) k_degrid_tiled(const Rec<T>* __restrict__
     const int tx1 = min(tx0 + TX, nf1), ty1 = min(ty0 + TY, nf2);
     const int p1 = all_planes ? nw : min(p0 + PB, nw);
     const int gx0 = tx0 - lo, gy0 = ty0 - lo, gz0 = all_planes ? 0 : p0 - lo;
-    // stage the tile + halo (periodic)
-    for (int i = threadIdx.x; i < nstage; i += blockDim.x) {
-      const int sx = i % SX, sy = (i / SX) % SY, sz = i / (SX * SY);
-      const int gx = modi(gx0 + sx, nf1), gy = modi(gy0 + sy, nf2), gz = modi(gz0 + sz, nw);
-      const size_t o = (size_t)gz * plane + (size_t)gy * nf1 + gx;
-      stg[2 * i] = fw[2 * o];
-      stg[2 * i + 1] = fw[2 * o + 1];
-    }
     // runs of the tile's own hives (each row belongs to exactly one tile)
     const int nslots = build_segments(g, hive_start, tx0 >> 3, (tx1 - 1) >> 3, ty0 >> 3,
                                       (ty1 - 1) >> 3, p0, p1 - 1, t, s_warp);
     const int total = t.pref[nslots];
+    if (total == 0) continue;  // uniform across the block: nothing to interpolate here
+    // stage the tile + halo (periodic); row stride SXP = SX + 1 complex
+    using V = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+    V* stv = reinterpret_cast<V*>(stg);
+    const V* fwv = reinterpret_cast<const V*>(fw);
+    for (int i = threadIdx.x; i < nstage; i += blockDim.x) {
+      const int sx = i % SX, sy = (i / SX) % SY, sz = i / (SX * SY);
+      const int gx = modi(gx0 + sx, nf1), gy = modi(gy0 + sy, nf2), gz = modi(gz0 + sz, nw);
+      stv[(sz * SY + sy) * SXP + sx] = fwv[(size_t)gz * plane + (size_t)gy * nf1 + gx];
+    }
+    __syncthreads();
     for (int q = threadIdx.x; q < total; q += blockDim.x) {
       const int sgi = find_segment(t.pref, nslots, q);
       const int sidx = t.start[sgi] + (q - t.pref[sgi]);
@@ -367,7 +398,7 @@ __global__ void __launch_bounds__(512) k_degrid_tiled(const Rec<T>* __restrict__
         zz = all_planes ? wrapi(zz, nw) : min(max(zz, 0), SZ - 1);
         T pr = 0, pi = 0;
         for (int b = 0; b < W; b++) {
-          const T* row = stg + 2 * (((size_t)zz * SY + (ly + b)) * SX + lx);
+          const T* row = stg + 2 * ((zz * SY + (ly + b)) * SXP + lx);
           T qr = 0, qi = 0;
 #pragma unroll
           for (int e = 0; e < W; e++) {
@@ -420,8 +451,8 @@ TileCfg grid_tiling(const Geom& g, bool degrid) {
   TY = std::max(8, (TY / 8) * 8);
   int PB = env_int("CG_TILE_PLANES", 0);
   auto bytes = [&](int tx, int ty, int pb) -> size_t {
-    size_t cells = degrid ? (size_t)(tx + W) * (ty + W) * (pb >= g.nw ? g.nw : pb + W)
-                          : (size_t)tx * ty * pb;
+    size_t cells = degrid ? (size_t)(tx + W + 1) * (ty + W) * (pb >= g.nw ? g.nw : pb + W)
+                          : (size_t)acc_row_stride(tx) * ty * pb;
     return cells * 2 * sizeof(T) + (size_t)(slots_for(ty, pb, W) + 1) * 4 * 5;
   };
   if (PB <= 0) {
