@@ -219,116 +219,231 @@ __device__ __forceinline__ int find_segment(const int* __restrict__ pref, int ns
   return lo;
 }
 
+static int env_int(const char* name, int dflt) {
+  const char* v = getenv(name);
+  return v ? atoi(v) : dflt;
+}
+
+static int num_sms() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) n = 148;
+  }
+  return n;
+}
+
+
 // ---------------------------------------------------------------- gridding
-// Shared accumulator: planar re / im arrays, row stride RS = TX + 8 so that
-// the bank of cell (x, y) is (x + 8 y) mod 32: the rows of a warp (spread over
-// one 8x8 hive) hit distinct banks.
-__host__ __device__ __forceinline__ int acc_row_stride(int TX) { return TX + 8; }
+// Warp-owned tiles: every warp accumulates its own TX x TY x PB tile in
+// shared memory, so no two threads ever update the same cell concurrently
+// and no atomics are needed; the result is deterministic.  Candidate rows
+// (own hives plus a one-hive ring, clipped to the tile) are pre-scanned 32 at
+// a time; each overlapping row is then spread by the whole warp: lane l takes
+// the tap pairs p = l + 32 r, (dy, dz) = (p % W, p / W), and walks the W taps
+// along x.  Cell (x, y, z) of a warp tile lives at z*PS + y*RS + x (complex
+// units) with RS = 1 and PS = W (mod 16): the 16 lanes of a half-warp touch
+// 16 distinct 8-byte bank pairs.
+struct WarpTile {
+  int TX, TY, PB, RS, PS, slots;
+  int ntx, nty, npb, nitems;
+  int warps;  // per CTA
+  size_t warp_bytes, smem;
+};
+
+__device__ __forceinline__ int warp_excl_scan(int x, int& total) {
+  const int lane = threadIdx.x & 31;
+  int inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  total = __shfl_sync(0xffffffffu, inc, 31);
+  return inc - x;
+}
+
+// warp-level version of build_segments (same slot layout)
+__device__ int warp_build_segments(const Geom& g, const int* __restrict__ hive_start, int hxa,
+                                   int hxb, int hya, int hyb, int za, int zb, SegTable t) {
+  const int lane = threadIdx.x & 31;
+  const int ny_raw = hyb - hya + 1, nz_raw = zb - za + 1;
+  const int rows = ny_raw * nz_raw;
+  const int nhx = g.nhx, nhy = g.nhy, nw = g.nw;
+  int carry = 0;
+  for (int base = 0; base < rows; base += 32) {
+    const int r = base + lane;
+    int cnt[3] = {0, 0, 0};
+    if (r < rows) {
+      const int hy_raw = hya + r % ny_raw, hz_raw = za + r / ny_raw;
+      int hy = hy_raw, shy = 0;
+      if (hy < 0) { hy += nhy; shy = -g.nf2; }
+      else if (hy >= nhy) { hy -= nhy; shy = g.nf2; }
+      int hz = hz_raw, shz = 0;
+      if (hz < 0) { hz += nw; shz = -nw; }
+      else if (hz >= nw) { hz -= nw; shz = nw; }
+      const int64_t rowbase = ((int64_t)hz * nhy + hy) * nhx;
+      const int lo_k[3] = {hxa, max(hxa, 0), max(hxa, nhx)};
+      const int hi_k[3] = {min(hxb, -1), min(hxb, nhx - 1), hxb};
+      const int off_k[3] = {nhx, 0, -nhx};
+      const int shx_k[3] = {-g.nf1, 0, g.nf1};
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        const int slot = r * 3 + k;
+        int st = 0, c = 0;
+        if (lo_k[k] <= hi_k[k]) {
+          st = hive_start[rowbase + lo_k[k] + off_k[k]];
+          c = hive_start[rowbase + hi_k[k] + off_k[k] + 1] - st;
+        }
+        t.start[slot] = st;
+        t.sx[slot] = shx_k[k];
+        t.sy[slot] = shy;
+        t.sz[slot] = shz;
+        cnt[k] = c;
+      }
+    }
+    int tot;
+    const int ex = carry + warp_excl_scan(cnt[0] + cnt[1] + cnt[2], tot);
+    if (r < rows) {
+      t.pref[r * 3] = ex;
+      t.pref[r * 3 + 1] = ex + cnt[0];
+      t.pref[r * 3 + 2] = ex + cnt[0] + cnt[1];
+    }
+    carry += tot;
+  }
+  if (lane == 0) t.pref[rows * 3] = carry;
+  __syncwarp();
+  return rows * 3;
+}
+
+template <typename T>
+struct Cplx;
+template <>
+struct Cplx<float> { using type = float2; };
+template <>
+struct Cplx<double> { using type = double2; };
 
 template <typename T, int W>
-__global__ void __launch_bounds__(512) k_grid_tiled(const Rec<T>* __restrict__ recs,
-                                                    const int* __restrict__ hive_start, Geom g,
-                                                    TileCfg tc, int nslots_max,
-                                                    T* __restrict__ fw, int* __restrict__ counter) {
+__global__ void __launch_bounds__(256) k_grid_warp(const Rec<T>* __restrict__ recs,
+                                                   const int* __restrict__ hive_start, Geom g,
+                                                   WarpTile tc, T* __restrict__ fw) {
+  using C = typename Cplx<T>::type;
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int lo = Halo<W>::lo, hi = Halo<W>::hi;
-  const int TX = tc.TX, TY = tc.TY, PB = tc.PB;
-  const int RS = acc_row_stride(TX);
-  const int nacc = RS * TY * PB;
-  T* acc_re = (T*)smem;
-  T* acc_im = acc_re + nacc;
-  int* tb = (int*)(acc_im + nacc);
-  const int ts = nslots_max + 1;
+  constexpr int NP = W * W;                 // (dy, dz) tap pairs
+  constexpr int NR = (NP + 31) / 32;        // rounds of pairs
+  constexpr int NKV = (3 * W + 31) / 32;    // kernel-value registers per lane
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int TX = tc.TX, TY = tc.TY, PB = tc.PB, RS = tc.RS, PS = tc.PS;
+  C* acc = reinterpret_cast<C*>(smem + (size_t)wib * tc.warp_bytes);
+  int* tb = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(acc) + (size_t)PB * PS * sizeof(C));
+  const int ts = tc.slots + 1;
   SegTable t{tb, tb + ts, tb + 2 * ts, tb + 3 * ts, tb + 4 * ts};
-  __shared__ int s_warp[33];
-  __shared__ int s_item;
-  const T beta = (T)g.beta, c = (T)g.es_c;
+  const T beta = (T)g.beta, c = (T)g.es_c, halfw = (T)W * (T)0.5;
   const int nf1 = g.nf1, nf2 = g.nf2, nw = g.nw;
   const size_t plane = (size_t)nf1 * nf2;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-  const int ncell = TX * TY * PB;
+  const int gwarp = blockIdx.x * tc.warps + wib, nwarps = gridDim.x * tc.warps;
+  C* fwc = reinterpret_cast<C*>(fw);
+  const C zero = {(T)0, (T)0};
 
-  for (;;) {
-    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
-    __syncthreads();
-    const int item = s_item;
-    if (item >= tc.nitems) break;
+  for (int item = gwarp; item < tc.nitems; item += nwarps) {
     const int tix = item % tc.ntx, tiy = (item / tc.ntx) % tc.nty, tib = item / (tc.ntx * tc.nty);
     const int tx0 = tix * TX, ty0 = tiy * TY, p0 = tib * PB;
     const int tx1 = min(tx0 + TX, nf1), ty1 = min(ty0 + TY, nf2), p1 = min(p0 + PB, nw);
-    const int wx = tx1 - tx0;
-    const int nslots = build_segments(g, hive_start, floordiv8(tx0 - hi), floordiv8(tx1 - 1 + lo),
-                                      floordiv8(ty0 - hi), floordiv8(ty1 - 1 + lo), p0 - hi,
-                                      p1 - 1 + lo, t, s_warp);
+    const int wx = tx1 - tx0, wy = ty1 - ty0, wz = p1 - p0;
+    const int nslots = warp_build_segments(g, hive_start, floordiv8(tx0 - hi),
+                                           floordiv8(tx1 - 1 + lo), floordiv8(ty0 - hi),
+                                           floordiv8(ty1 - 1 + lo), p0 - hi, p1 - 1 + lo, t);
     const int total = t.pref[nslots];
+    __syncwarp();  // every lane has read the table head before it can be rebuilt
     if (total == 0) {
-      // no row reaches this tile: write zeros straight to the grid
-      for (int i = threadIdx.x; i < ncell; i += blockDim.x) {
-        const int x = i % TX, y = (i / TX) % TY, z = i / (TX * TY);
-        if (x < wx && ty0 + y < ty1 && p0 + z < p1) {
-          const size_t o = (size_t)(p0 + z) * plane + (size_t)(ty0 + y) * nf1 + tx0 + x;
-          fw[2 * o] = (T)0;
-          fw[2 * o + 1] = (T)0;
-        }
+      for (int i = lane; i < wx * wy * wz; i += 32) {
+        const int x = i % wx, y = (i / wx) % wy, z = i / (wx * wy);
+        fwc[(size_t)(p0 + z) * plane + (size_t)(ty0 + y) * nf1 + tx0 + x] = zero;
       }
-      __syncthreads();
       continue;
     }
-    for (int i = threadIdx.x; i < nacc; i += blockDim.x) {
-      acc_re[i] = (T)0;
-      acc_im[i] = (T)0;
-    }
-    __syncthreads();
-    // within a chunk of blockDim rows, lane-major order keeps the lanes of a
-    // warp on different cells; every row is visited exactly once
-    for (int q0 = 0; q0 < total; q0 += blockDim.x) {
-      const int q = q0 + lane * nwarp + warp;
-      if (q >= total) continue;
-      const int sgi = find_segment(t.pref, nslots, q);
-      const int idx = t.start[sgi] + (q - t.pref[sgi]);
-      const Rec<T> r = recs[idx];
-      const int bx = (int)(r.bxy & 0xFFFFu) + t.sx[sgi];
-      const int by = (int)(r.bxy >> 16) + t.sy[sgi];
-      const int bz = (int)r.bz + t.sz[sgi];
-      const int ox = bx + tap_offset<W>(r.f[0]);
-      const int oy = by + tap_offset<W>(r.f[1]);
-      const int oz = bz + tap_offset<W>(r.f[2]);
-      const int xa = max(ox, tx0), xb = min(ox + W, tx1);
-      const int ya = max(oy, ty0), yb = min(oy + W, ty1);
-      const int za = max(oz, p0), zb = min(oz + W, p1);
-      if (xa >= xb || ya >= yb || za >= zb) continue;
-      T kx[W], ky[W], kz[W];
-      taps<T, W>(r.f[0], beta, c, kx);
-      taps<T, W>(r.f[1], beta, c, ky);
-      taps<T, W>(r.f[2], beta, c, kz);
-      for (int z = za; z < zb; z++) {
-        const T cr = r.c[0] * kz[z - oz], ci = r.c[1] * kz[z - oz];
-        for (int y = ya; y < yb; y++) {
-          const T vr = cr * ky[y - oy], vi = ci * ky[y - oy];
-          const int rowo = ((z - p0) * TY + (y - ty0)) * RS - tx0;
+    for (int i = lane; i < PB * PS; i += 32) acc[i] = zero;
+    __syncwarp();
+    for (int q0 = 0; q0 < total; q0 += 32) {
+      // pre-scan: each lane loads one candidate row and tests its overlap
+      const int q = q0 + lane;
+      bool take = false;
+      T f0 = 0, f1 = 0, f2 = 0, c0 = 0, c1 = 0;
+      int ox = 0, oy = 0, oz = 0;
+      if (q < total) {
+        const int sgi = find_segment(t.pref, nslots, q);
+        const Rec<T> r = recs[t.start[sgi] + (q - t.pref[sgi])];
+        f0 = r.f[0]; f1 = r.f[1]; f2 = r.f[2]; c0 = r.c[0]; c1 = r.c[1];
+        ox = (int)(r.bxy & 0xFFFFu) + t.sx[sgi] + tap_offset<W>(f0);
+        oy = (int)(r.bxy >> 16) + t.sy[sgi] + tap_offset<W>(f1);
+        oz = (int)r.bz + t.sz[sgi] + tap_offset<W>(f2);
+        take = max(ox, tx0) < min(ox + W, tx1) && max(oy, ty0) < min(oy + W, ty1) &&
+               max(oz, p0) < min(oz + W, p1);
+      }
+      unsigned mask = __ballot_sync(0xffffffffu, take);
+      while (mask) {
+        const int src = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const T g0 = __shfl_sync(0xffffffffu, f0, src), g1 = __shfl_sync(0xffffffffu, f1, src);
+        const T g2 = __shfl_sync(0xffffffffu, f2, src);
+        const T vr0 = __shfl_sync(0xffffffffu, c0, src), vi0 = __shfl_sync(0xffffffffu, c1, src);
+        const int vx = __shfl_sync(0xffffffffu, ox, src) - tx0;
+        const int vy = __shfl_sync(0xffffffffu, oy, src) - ty0;
+        const int vz = __shfl_sync(0xffffffffu, oz, src) - p0;
+        // kernel values: lane slot s = axis * W + i, s < 3W
+        T kv[NKV];
 #pragma unroll
-          for (int e = 0; e < W; e++) {
-            const int x = ox + e;
-            if (x >= xa && x < xb) {
-              atomicAdd(acc_re + rowo + x, vr * kx[e]);
-              atomicAdd(acc_im + rowo + x, vi * kx[e]);
+        for (int k = 0; k < NKV; k++) {
+          const int sl = lane + 32 * k;
+          const int axis = sl / W, i = sl - axis * W;
+          const T f = axis == 0 ? g0 : (axis == 1 ? g1 : g2);
+          kv[k] = (sl < 3 * W) ? es_kernel<T>((T)(tap_offset<W>(f) + i) - f, beta, c, halfw) : (T)0;
+        }
+        T kx[W];
+        unsigned xmask = 0;
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+          kx[e] = __shfl_sync(0xffffffffu, kv[0], e);
+          xmask |= ((unsigned)(vx + e >= 0 && vx + e < wx)) << e;
+        }
+#pragma unroll
+        for (int rr = 0; rr < NR; rr++) {
+          const int pp = lane + 32 * rr;
+          const int dy = pp % W, dz = pp / W;
+          const T ky = __shfl_sync(0xffffffffu, kv[0], W + dy);
+          const int zs = 2 * W + dz;
+          T kz = __shfl_sync(0xffffffffu, kv[0], zs & 31);
+          if (NKV > 1) {
+            const T kz1 = __shfl_sync(0xffffffffu, kv[NKV - 1], zs & 31);
+            kz = zs >= 32 ? kz1 : kz;
+          }
+          const int y = vy + dy, z = vz + dz;
+          if (pp < NP && y >= 0 && y < wy && z >= 0 && z < wz) {
+            const T k = ky * kz;
+            const T vr = vr0 * k, vi = vi0 * k;
+            C* a = acc + z * PS + y * RS + vx;
+#pragma unroll
+            for (int e = 0; e < W; e++) {
+              if (xmask & (1u << e)) {
+                C cur = a[e];
+                cur.x += vr * kx[e];
+                cur.y += vi * kx[e];
+                a[e] = cur;
+              }
             }
           }
         }
+        __syncwarp();
       }
     }
-    __syncthreads();
-    // flush: every cell of the tile written once, coalesced along x
-    for (int i = threadIdx.x; i < ncell; i += blockDim.x) {
-      const int x = i % TX, y = (i / TX) % TY, z = i / (TX * TY);
-      if (x < wx && ty0 + y < ty1 && p0 + z < p1) {
-        const size_t o = (size_t)(p0 + z) * plane + (size_t)(ty0 + y) * nf1 + tx0 + x;
-        const int a = (z * TY + y) * RS + x;
-        fw[2 * o] = acc_re[a];
-        fw[2 * o + 1] = acc_im[a];
-      }
+    // flush the tile, coalesced along x
+    for (int i = lane; i < wx * wy * wz; i += 32) {
+      const int x = i % wx, y = (i / wx) % wy, z = i / (wx * wy);
+      fwc[(size_t)(p0 + z) * plane + (size_t)(ty0 + y) * nf1 + tx0 + x] = acc[z * PS + y * RS + x];
     }
-    __syncthreads();
+    __syncwarp();
   }
 }
 
@@ -421,21 +536,6 @@ __global__ void __launch_bounds__(512) k_degrid_tiled(const Rec<T>* __restrict__
 }
 
 // ======================================================================= launch
-static int env_int(const char* name, int dflt) {
-  const char* v = getenv(name);
-  return v ? atoi(v) : dflt;
-}
-
-static int num_sms() {
-  static int n = 0;
-  if (!n) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) n = 148;
-  }
-  return n;
-}
-
 static int slots_for(int TY, int PB, int W) { return ((TY >> 3) + 2) * (PB + W + 1) * 3; }
 
 // Tile shape: 32 x 32 cells by default, the plane batch covering all planes
@@ -452,7 +552,7 @@ TileCfg grid_tiling(const Geom& g, bool degrid) {
   int PB = env_int("CG_TILE_PLANES", 0);
   auto bytes = [&](int tx, int ty, int pb) -> size_t {
     size_t cells = degrid ? (size_t)(tx + W + 1) * (ty + W) * (pb >= g.nw ? g.nw : pb + W)
-                          : (size_t)acc_row_stride(tx) * ty * pb;
+                          : (size_t)(tx + 8) * ty * pb;
     return cells * 2 * sizeof(T) + (size_t)(slots_for(ty, pb, W) + 1) * 4 * 5;
   };
   if (PB <= 0) {
@@ -477,9 +577,39 @@ TileCfg grid_tiling(const Geom& g, bool degrid) {
   return tc;
 }
 
+// Warp tiles: 16 x 16 cells by default (CG_WTILE_X / CG_WTILE_Y); the plane
+// batch and warps per CTA are chosen so that two CTAs fit on an SM.
+template <typename T>
+static WarpTile warp_tiling(const Geom& g) {
+  WarpTile tc{};
+  const int W = g.kw;
+  tc.TX = std::max(16, (env_int("CG_WTILE_X", 16) / 16) * 16);
+  tc.TY = std::max(8, (env_int("CG_WTILE_Y", 16) / 8) * 8);
+  tc.RS = tc.TX + 1;
+  int PB = env_int("CG_WTILE_PLANES", 0);
+  if (PB <= 0) PB = std::min(g.nw, 7);
+  PB = std::min(PB, g.nw);
+  tc.PB = PB;
+  int ps = tc.TY * tc.RS;
+  ps += ((W % 16) - (ps % 16) + 16) % 16;  // PS = W (mod 16)
+  tc.PS = ps;
+  tc.slots = ((tc.TY >> 3) + 2) * (PB + W) * 3;
+  tc.warp_bytes = ((size_t)PB * tc.PS * 2 * sizeof(T) + (size_t)(tc.slots + 1) * 5 * 4 + 15) & ~(size_t)15;
+  int warps = env_int("CG_WTILE_WARPS", 0);
+  if (warps <= 0) warps = (int)std::max<size_t>(1, std::min<size_t>(8, (110 * 1024) / tc.warp_bytes));
+  tc.warps = warps;
+  tc.smem = tc.warp_bytes * warps;
+  tc.ntx = (g.nf1 + tc.TX - 1) / tc.TX;
+  tc.nty = (g.nf2 + tc.TY - 1) / tc.TY;
+  tc.npb = (g.nw + PB - 1) / PB;
+  tc.nitems = tc.ntx * tc.nty * tc.npb;
+  return tc;
+}
+
 template <typename T, int W>
 static int grid_w(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, const Geom& g, T* d_fw,
                   int method, int* d_counter, cudaStream_t st) {
+  (void)d_counter;
   if (method == kGridDirect) {
     size_t G = (size_t)g.nf1 * g.nf2 * g.nw;
     CG_CUDA(cudaMemsetAsync(d_fw, 0, G * 2 * sizeof(T), st));
@@ -491,21 +621,18 @@ static int grid_w(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, cons
     CG_CUDA(cudaGetLastError());
     return CG_OK;
   }
-  TileCfg tc = grid_tiling<T>(g, false);
-  int nslots = slots_for(tc.TY, tc.PB, W);
-  CG_CUDA(cudaFuncSetAttribute(k_grid_tiled<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  WarpTile tc = warp_tiling<T>(g);
+  CG_CUDA(cudaFuncSetAttribute(k_grid_warp<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)tc.smem));
   int per_sm = 0;
-  CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_tiled<T, W>, tc.threads,
+  CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_warp<T, W>, tc.warps * 32,
                                                         tc.smem));
   if (per_sm < 1) {
-    set_last_error("tiled gridding does not fit on an SM");
+    set_last_error("warp-tiled gridding does not fit on an SM");
     return CG_ERR_ARG;
   }
-  int blocks = std::min(tc.nitems, per_sm * num_sms());
-  CG_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(int), st));
-  k_grid_tiled<T, W><<<blocks, tc.threads, tc.smem, st>>>(d_recs, d_hive_start, g, tc, nslots,
-                                                          d_fw, d_counter);
+  int blocks = per_sm * num_sms();
+  k_grid_warp<T, W><<<blocks, tc.warps * 32, tc.smem, st>>>(d_recs, d_hive_start, g, tc, d_fw);
   count_launches(1);
   CG_CUDA(cudaGetLastError());
   return CG_OK;
