@@ -33,43 +33,64 @@ double decode_ordered(unsigned long long k) {
   return x;
 }
 
-// min/max of the raw w column (utils.cu:43-54 takes them of the scaled w;
-// scaling by f/c*sign*2pi is monotone, so the host maps the extremes) and a
-// flag for non-finite coordinates.
+// min/max of the raw u, v, w columns (utils.cu:43-54 takes min/max of the
+// scaled w; scaling by f/c*sign*2pi is monotone, so the host maps the
+// extremes) and a flag for non-finite coordinates.  The u and v ranges give
+// the band of grid rows / columns the data can touch (FFT pruning).
+// mm layout: [u_min, u_max, v_min, v_max, w_min, w_max] as order-preserving
+// integer keys, then the non-finite flag.
 __global__ void k_wminmax(const double* __restrict__ uvw, int64_t M, unsigned long long* mm,
                           int* bad) {
-  double lo = DBL_MAX, hi = -DBL_MAX;
+  double lo[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, hi[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
   int nf = 0;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M;
        i += (int64_t)gridDim.x * blockDim.x) {
-    double u = uvw[3 * i], v = uvw[3 * i + 1], w = uvw[3 * i + 2];
-    nf |= !(isfinite(u) && isfinite(v) && isfinite(w));
-    lo = fmin(lo, w);
-    hi = fmax(hi, w);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const double x = uvw[3 * i + a];
+      nf |= !isfinite(x);
+      lo[a] = fmin(lo[a], x);
+      hi[a] = fmax(hi[a], x);
+    }
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-    nf |= __shfl_xor_sync(0xffffffffu, nf, o);
-  }
-  __shared__ double slo[32], shi[32];
+#pragma unroll
+  for (int a = 0; a < 3; a++)
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[a] = fmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+      hi[a] = fmax(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+    }
+  for (int o = 16; o > 0; o >>= 1) nf |= __shfl_xor_sync(0xffffffffu, nf, o);
+  __shared__ double slo[3][32], shi[3][32];
   __shared__ int snf[32];
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) { slo[warp] = lo; shi[warp] = hi; snf[warp] = nf; }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      slo[a][warp] = lo[a];
+      shi[a][warp] = hi[a];
+    }
+    snf[warp] = nf;
+  }
   __syncthreads();
   if (warp == 0) {
-    int nw = blockDim.x >> 5;
-    lo = lane < nw ? slo[lane] : DBL_MAX;
-    hi = lane < nw ? shi[lane] : -DBL_MAX;
-    nf = lane < nw ? snf[lane] : 0;
-    for (int o = 16; o > 0; o >>= 1) {
-      lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-      hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
-      nf |= __shfl_xor_sync(0xffffffffu, nf, o);
+    const int nwp = blockDim.x >> 5;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      lo[a] = lane < nwp ? slo[a][lane] : DBL_MAX;
+      hi[a] = lane < nwp ? shi[a][lane] : -DBL_MAX;
+      for (int o = 16; o > 0; o >>= 1) {
+        lo[a] = fmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+        hi[a] = fmax(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+      }
     }
+    nf = lane < nwp ? snf[lane] : 0;
+    for (int o = 16; o > 0; o >>= 1) nf |= __shfl_xor_sync(0xffffffffu, nf, o);
     if (lane == 0) {
-      atomicMin(&mm[0], ordered_key(lo));
-      atomicMax(&mm[1], ordered_key(hi));
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        atomicMin(&mm[2 * a], ordered_key(lo[a]));
+        atomicMax(&mm[2 * a + 1], ordered_key(hi[a]));
+      }
       if (nf) atomicOr(bad, 1);
     }
   }
@@ -77,7 +98,7 @@ __global__ void k_wminmax(const double* __restrict__ uvw, int64_t M, unsigned lo
 
 int launch_wminmax(const double* d_uvw, int64_t M, unsigned long long* d_mm, int* d_bad,
                    cudaStream_t st) {
-  unsigned long long init[2] = {~0ULL, 0ULL};
+  unsigned long long init[6] = {~0ULL, 0ULL, ~0ULL, 0ULL, ~0ULL, 0ULL};
   CG_CUDA(cudaMemcpyAsync(d_mm, init, sizeof(init), cudaMemcpyHostToDevice, st));
   CG_CUDA(cudaMemsetAsync(d_bad, 0, sizeof(int), st));
   if (M == 0) return CG_OK;

@@ -45,6 +45,8 @@ void destroy_plan(cg_plan_s* P) {
   if (!P) return;
   cudaSetDevice(P->device);
   if (P->fft_valid) cufftDestroy(P->fft);
+  if (P->rows_valid) cufftDestroy(P->fft_rows);
+  if (P->cols_valid) cufftDestroy(P->fft_cols);
   cg_dev_buf* bs[] = {&P->mm,   &P->K1,    &P->K2,     &P->K3q,    &P->zq,     &P->grid,
                       &P->recs, &P->perm,  &P->skeys,  &P->hive_start, &P->binws, &P->fftwork,
                       &P->io_uvw, &P->io_vis, &P->io_wgt, &P->io_dirty};
@@ -206,6 +208,7 @@ int cg_plan_create(cg_plan** plan, int nxdirty, int nydirty, double fov, double 
   cudaGetDevice(&P->device);
   P->stream = (cudaStream_t)stream;
   if (const char* m = getenv("CG_GRID_METHOD")) P->grid_method = atoi(m) == 0 ? 0 : 1;
+  if (const char* m = getenv("CG_FFT_PRUNE")) P->fft_pruning = atoi(m) != 0;
   st = cg::plan_configure(P, nxdirty, nydirty, fov, epsilon, sigma, sign, precision);
   if (st > 1) {
     destroy_plan(P);

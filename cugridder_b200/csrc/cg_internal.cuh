@@ -34,6 +34,9 @@ struct Geom {
   int sign;
   double i_center, i_half_width, o_center, o_half_width, gamma, h;
   int nhx, nhy, nhz; // 8 x 8 x 1 hives
+  // grid rows (g1) / columns (g0) the data can touch, inclusive; the full
+  // range when the data wraps around the grid edge
+  int band_r0, band_r1, band_c0, band_c1;
 };
 
 // Kernel Fourier-series quadrature: phi_hat(k) = sum_i g[i] * 2 cos(x[i] k)

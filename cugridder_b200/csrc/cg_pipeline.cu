@@ -276,15 +276,15 @@ static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw)
     return CG_ERR_ARG;
   }
   cudaStream_t st = P->stream;
-  CG_TRY(ensure(P->mm, 64));
+  CG_TRY(ensure(P->mm, 128));
   if (!P->h_mm) CG_CUDA(cudaMallocHost(&P->h_mm, 64));
   unsigned long long* d_mm = (unsigned long long*)P->mm.p;
-  int* d_bad = (int*)(d_mm + 2);
+  int* d_bad = (int*)(d_mm + 6);
   CG_TRY(launch_wminmax(d_uvw, nrow, d_mm, d_bad, st));
-  CG_CUDA(cudaMemcpyAsync(P->h_mm, d_mm, 24, cudaMemcpyDeviceToHost, st));
+  CG_CUDA(cudaMemcpyAsync(P->h_mm, d_mm, 52, cudaMemcpyDeviceToHost, st));
   CG_CUDA(cudaStreamSynchronize(st));
   timer_flush(P, P->timer.cur ^ 1);
-  if (((int*)(P->h_mm + 2))[0]) {
+  if (((int*)(P->h_mm + 6))[0]) {
     set_last_error("non-finite uvw coordinate");
     return CG_ERR_ARG;
   }
@@ -302,7 +302,7 @@ static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw)
   g.sign = P->sign;
   double wmin = 0, wmax = 0;
   if (nrow > 0) {
-    double rmin = decode_ordered(P->h_mm[0]), rmax = decode_ordered(P->h_mm[1]);
+    double rmin = decode_ordered(P->h_mm[4]), rmax = decode_ordered(P->h_mm[5]);
     // same rounding chain as eff_coords(); monotone in w
     auto scale = [&](double w) { return (w * (g.foc * (double)g.sign)) * (2 * kPi); };
     double a = scale(rmin), b = scale(rmax);
@@ -326,6 +326,27 @@ static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw)
   g.nhx = (g.nf1 - 1) / 8 + 1;
   g.nhy = (g.nf2 - 1) / 8 + 1;
   g.nhz = g.nw;
+  // band of grid rows (g1 <- u) / columns (g0 <- v) reached by the taps: the
+  // grid coordinate is monotone in u (v) while the scaled value stays inside
+  // [-pi, pi); otherwise the data wraps and the band is the whole axis.
+  g.band_r0 = 0;
+  g.band_r1 = g.nf2 - 1;
+  g.band_c0 = 0;
+  g.band_c1 = g.nf1 - 1;
+  if (nrow > 0) {
+    const int lo = (g.kw - 1) / 2 + 1, hi = (g.kw + 1) / 2 + 1;  // tap halo, one cell of margin
+    auto band = [&](double umin, double umax, double pix, int nf, int& b0, int& b1) {
+      const double a = ((umin * g.foc) * (2 * kPi)) * pix, b = ((umax * g.foc) * (2 * kPi)) * pix;
+      if (!(a > -kPi + 1e-9 && b < kPi - 1e-9)) return;
+      const double xa = (a * kM_1_2PI + 0.5) * nf, xb = (b * kM_1_2PI + 0.5) * nf;
+      const int r0 = (int)std::floor(xa) - lo, r1 = (int)std::floor(xb) + hi;
+      if (r0 < 0 || r1 >= nf) return;
+      b0 = r0;
+      b1 = r1;
+    };
+    band(decode_ordered(P->h_mm[0]), decode_ordered(P->h_mm[1]), g.pixx, g.nf2, g.band_r0, g.band_r1);
+    band(decode_ordered(P->h_mm[2]), decode_ordered(P->h_mm[3]), g.pixy, g.nf1, g.band_c0, g.band_c1);
+  }
   P->geom = g;
   P->nrow = nrow;
   int64_t nh = (int64_t)g.nhx * g.nhy * g.nhz;
@@ -356,7 +377,12 @@ static int fft_exec(cg_plan_s* P, void* d_grid, int direction) {
     size_t ws = 0;
     cufftType t = (P->precision == CG_PREC_FP64) ? CUFFT_Z2Z : CUFFT_C2C;
     CG_CUFFT(cufftMakePlanMany64(P->fft, 2, n, nullptr, 1, 0, nullptr, 1, 0, t, g.nw, &ws));
-    CG_TRY(ensure(P->fftwork, ws));
+    if (ws > P->fftwork.cap) {
+      CG_CUDA(cudaStreamSynchronize(P->stream));
+      CG_TRY(ensure(P->fftwork, ws));
+      if (P->rows_valid) CG_CUFFT(cufftSetWorkArea(P->fft_rows, P->fftwork.p));
+      if (P->cols_valid) CG_CUFFT(cufftSetWorkArea(P->fft_cols, P->fftwork.p));
+    }
     CG_CUFFT(cufftSetWorkArea(P->fft, P->fftwork.p));
     P->fft_nf1 = g.nf1;
     P->fft_nf2 = g.nf2;
@@ -372,7 +398,93 @@ static int fft_exec(cg_plan_s* P, void* d_grid, int direction) {
 }
 
 // work-queue head of the tiled kernels: a word of the small scratch buffer
-static int* queue_counter(cg_plan_s* P) { return (int*)((char*)P->mm.p + 32); }
+static int* queue_counter(cg_plan_s* P) { return (int*)((char*)P->mm.p + 64); }
+
+// 1-D cuFFT plans of the band-pruned transform (work areas shared with the
+// 2-D plan's buffer; the plans run one after another on the plan's stream).
+static int make_1d_plan(cg_plan_s* P, cufftHandle& h, bool& valid, int n, int stride, int batch) {
+  if (valid) {
+    cufftDestroy(h);
+    valid = false;
+  }
+  CG_CUFFT(cufftCreate(&h));
+  valid = true;
+  CG_CUFFT(cufftSetAutoAllocation(h, 0));
+  long long nn[1] = {n}, emb[1] = {n};
+  size_t ws = 0;
+  cufftType t = (P->precision == CG_PREC_FP64) ? CUFFT_Z2Z : CUFFT_C2C;
+  if (stride == 1)
+    CG_CUFFT(cufftMakePlanMany64(h, 1, nn, nullptr, 1, 0, nullptr, 1, 0, t, batch, &ws));
+  else
+    CG_CUFFT(cufftMakePlanMany64(h, 1, nn, emb, stride, 1, emb, stride, 1, t, batch, &ws));
+  if (ws > P->fftwork.cap) {
+    // grow the shared work buffer; every plan must point at the new one
+    CG_CUDA(cudaStreamSynchronize(P->stream));
+    CG_TRY(ensure(P->fftwork, ws));
+    if (P->fft_valid) CG_CUFFT(cufftSetWorkArea(P->fft, P->fftwork.p));
+    if (P->rows_valid && &h != &P->fft_rows) CG_CUFFT(cufftSetWorkArea(P->fft_rows, P->fftwork.p));
+    if (P->cols_valid && &h != &P->fft_cols) CG_CUFFT(cufftSetWorkArea(P->fft_cols, P->fftwork.p));
+  }
+  CG_CUFFT(cufftSetWorkArea(h, P->fftwork.p));
+  return CG_OK;
+}
+
+static int exec_c2c(cg_plan_s* P, cufftHandle h, void* data, int direction) {
+  CG_CUFFT(cufftSetStream(h, P->stream));
+  if (P->precision == CG_PREC_FP64)
+    CG_CUFFT(cufftExecZ2Z(h, (cufftDoubleComplex*)data, (cufftDoubleComplex*)data, direction));
+  else
+    CG_CUFFT(cufftExecC2C(h, (cufftComplex*)data, (cufftComplex*)data, direction));
+  return CG_OK;
+}
+
+// Separable 2-D transform restricted to what the pipeline uses:
+//   ms2dirty: rows of the data band (other rows are zero), then only the N1
+//             columns the image keeps (two column ranges of N1/2);
+//   dirty2ms: the N1 non-zero columns first, then only the rows the
+//             degridding reads.
+// Falls back to the full 2-D transform when the band saves little.
+static int fft_exec_pruned(cg_plan_s* P, void* d_grid, int direction) {
+  const Geom& g = P->geom;
+  const int nrows = g.band_r1 - g.band_r0 + 1;
+  const double full = 2.0 * g.nf1 * g.nf2;
+  const double pruned = (double)nrows * g.nf1 + (double)g.N1 * g.nf2;
+  if (!P->fft_pruning || pruned > 0.8 * full) return fft_exec(P, d_grid, direction);
+  // rows plan: batch rounded up to 64 rows (extra rows are zero or unused)
+  int batch = std::min(g.nf2, ((nrows + 63) / 64) * 64);
+  if (!P->rows_valid || P->rows_n != g.nf1 || P->rows_batch != batch) {
+    CG_TRY(make_1d_plan(P, P->fft_rows, P->rows_valid, g.nf1, 1, batch));
+    P->rows_n = g.nf1;
+    P->rows_batch = batch;
+  }
+  const int half = g.N1 / 2;
+  if (!P->cols_valid || P->cols_n != g.nf2 || P->cols_stride != g.nf1 || P->cols_batch != half) {
+    CG_TRY(make_1d_plan(P, P->fft_cols, P->cols_valid, g.nf2, g.nf1, half));
+    P->cols_n = g.nf2;
+    P->cols_stride = g.nf1;
+    P->cols_batch = half;
+  }
+  const size_t esz = (P->precision == CG_PREC_FP64) ? 16 : 8;
+  const size_t plane = (size_t)g.nf1 * g.nf2;
+  const int r0 = std::min(g.band_r0, g.nf2 - batch);
+  char* base = (char*)d_grid;
+  auto rows = [&](int p) { return exec_c2c(P, P->fft_rows, base + esz * (p * plane + (size_t)r0 * g.nf1), direction); };
+  auto cols = [&](int p) {
+    int s1 = exec_c2c(P, P->fft_cols, base + esz * (p * plane), direction);
+    if (s1 > 1) return s1;
+    return exec_c2c(P, P->fft_cols, base + esz * (p * plane + (size_t)(g.nf1 - half)), direction);
+  };
+  for (int p = 0; p < g.nw; p++) {
+    if (direction == CUFFT_INVERSE) {
+      CG_TRY(rows(p));
+      CG_TRY(cols(p));
+    } else {
+      CG_TRY(cols(p));
+      CG_TRY(rows(p));
+    }
+  }
+  return CG_OK;
+}
 
 template <typename T>
 static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T* d_wgt,
@@ -394,7 +506,7 @@ static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T
                         (T*)P->grid.p, P->grid_method, queue_counter(P), st));
   timer_mark(P);  // 4: gridding
   if (P->stop_stage == 2) return CG_OK;
-  CG_TRY(fft_exec(P, P->grid.p, CUFFT_INVERSE));
+  CG_TRY(fft_exec_pruned(P, P->grid.p, CUFFT_INVERSE));
   timer_mark(P);  // 5: FFT
   if (P->stop_stage == 3) return CG_OK;
   CG_TRY(launch_wdft_deconv<T>((const T*)P->grid.p, g, (const double*)P->K1.p,
@@ -421,7 +533,7 @@ static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const
                               (const double*)P->K3q.p, (const double*)P->zq.p, (T*)P->grid.p, st));
   timer_mark(P);  // 3: plane fill
   if (P->stop_stage == 2) return CG_OK;
-  CG_TRY(fft_exec(P, P->grid.p, CUFFT_FORWARD));
+  CG_TRY(fft_exec_pruned(P, P->grid.p, CUFFT_FORWARD));
   timer_mark(P);  // 4: FFT
   if (P->stop_stage == 3) return CG_OK;
   CG_TRY(launch_build_stream<T>((const int*)P->perm.p, M, d_uvw, (const T*)nullptr, d_wgt, g,

@@ -50,11 +50,15 @@ struct cg_plan_s {
   cg_dev_buf mm, K1, K2, K3q, zq, grid, recs, perm, skeys, hive_start, binws, fftwork, io_uvw,
       io_vis, io_wgt, io_dirty;
   unsigned long long* h_mm = nullptr;  // pinned, 2 words + flag
-  // cuFFT
+  // cuFFT: full 2-D batched plan, and the 1-D plans of the band-pruned path
   cufftHandle fft = 0;
   bool fft_valid = false;
   int fft_nf1 = 0, fft_nf2 = 0, fft_nw = 0;
   size_t fft_work_bytes = 0;
+  cufftHandle fft_rows = 0, fft_cols = 0;
+  bool rows_valid = false, cols_valid = false;
+  int rows_n = 0, rows_batch = 0, cols_n = 0, cols_stride = 0, cols_batch = 0;
+  int fft_pruning = 1;  // 0: always the full 2-D transform (CG_FFT_PRUNE=0)
   cg_stage_timer timer;
   std::mutex mu;
 };

@@ -338,3 +338,23 @@ def test_grid_smaller_than_a_tile(torch_cuda, oracle, eps):
     _, vis, _ = plan_dirty2ms(torch_cuda, d, im, "fp64", eps)
     ref, _ = oracle.dirty2ms(d["uvw"], im, d["wgt"], 2, 1e9, eps)
     assert rel_l2(vis, ref) < 1e-10
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-13), ("fp32", 1e-6)])
+def test_fft_band_pruning(torch_cuda, c1, precision, tol):
+    """The band-pruned separable FFT (rows of the data band, columns of the
+    image) gives the full 2-D transform's results in both directions."""
+    import os
+
+    img = synth.random_image(256, 256, seed=6)
+    out = {}
+    for prune in ("1", "0"):
+        os.environ["CG_FFT_PRUNE"] = prune
+        try:
+            _, d, _ = plan_ms2dirty(torch_cuda, c1, precision, EPS_C1)
+            _, v, _ = plan_dirty2ms(torch_cuda, c1, img, precision, EPS_C1)
+        finally:
+            del os.environ["CG_FFT_PRUNE"]
+        out[prune] = (d, v)
+    assert rel_l2(out["1"][0], out["0"][0]) < tol
+    assert rel_l2(out["1"][1], out["0"][1]) < tol
