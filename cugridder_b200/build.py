@@ -23,7 +23,8 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libcugridder.so")
 ALIAS = os.path.join(LIBDIR, "libcurafft.so")
 
-SOURCES = ["cg_bin.cu", "cg_spread.cu", "cg_wstage.cu", "cg_pipeline.cu", "cg_capi.cu"]
+SOURCES = ["cg_bin.cu", "cg_spread.cu", "cg_grid_mma.cu", "cg_wstage.cu", "cg_pipeline.cu",
+           "cg_capi.cu"]
 
 
 def _nvcc():

@@ -207,7 +207,10 @@ int cg_plan_create(cg_plan** plan, int nxdirty, int nydirty, double fov, double 
   cg_plan_s* P = new cg_plan_s();
   cudaGetDevice(&P->device);
   P->stream = (cudaStream_t)stream;
-  if (const char* m = getenv("CG_GRID_METHOD")) P->grid_method = atoi(m) == 0 ? 0 : 1;
+  if (const char* m = getenv("CG_GRID_METHOD")) {
+    const int v = atoi(m);
+    P->grid_method = (v >= 0 && v <= 2) ? v : 2;
+  }
   if (const char* m = getenv("CG_FFT_PRUNE")) P->fft_pruning = atoi(m) != 0;
   st = cg::plan_configure(P, nxdirty, nydirty, fov, epsilon, sigma, sign, precision);
   if (st > 1) {
@@ -268,7 +271,7 @@ int cg_plan_destroy(cg_plan* plan) {
 }
 
 int cg_plan_set_method(cg_plan* plan, int method) {
-  if (!plan || method < 0 || method > 1) return CG_ERR_ARG;
+  if (!plan || method < 0 || method > 2) return CG_ERR_ARG;
   plan->grid_method = method;
   return CG_OK;
 }

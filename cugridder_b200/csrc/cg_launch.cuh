@@ -27,6 +27,9 @@ int launch_build_stream(const int* d_perm, int64_t M, const double* d_uvw, const
 // d_counter: one device int used as the work-queue head of the tiled kernels.
 constexpr int kGridDirect = 0;
 constexpr int kGridTiled = 1;
+constexpr int kGridMma = 2;  // tensor-core gridding (FP32, W <= 8); degridding uses tiled
+int launch_grid_mma(const Rec<float>* d_recs, const int* d_hive_start, const Geom& g, float* d_fw,
+                    cudaStream_t st);
 template <typename T>
 TileCfg grid_tiling(const Geom& g, bool degrid);
 template <typename T>

@@ -694,6 +694,14 @@ static int degrid_w(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_s
 template <typename T>
 int launch_grid(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, const Geom& g, T* d_fw,
                 int method, int* d_counter, cudaStream_t st) {
+  if (method == kGridMma) {
+    // tensor-core path: FP32 and W <= 8; everything else on the SIMT kernels
+    if (sizeof(T) == 4) {
+      int s = launch_grid_mma((const Rec<float>*)d_recs, d_hive_start, g, (float*)d_fw, st);
+      if (s != CG_ERR_ARG) return s;
+    }
+    method = kGridTiled;
+  }
 #define CG_GRID_CALL(w) grid_w<T, w>(d_recs, d_hive_start, M, g, d_fw, method, d_counter, st)
   CG_W_SWITCH(g.kw, CG_GRID_CALL)
 #undef CG_GRID_CALL
@@ -703,6 +711,7 @@ template <typename T>
 int launch_degrid(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_start, int64_t M,
                   const Geom& g, const T* d_fw, T* d_vis, int method, int* d_counter,
                   cudaStream_t st) {
+  if (method == kGridMma) method = kGridTiled;
 #define CG_DEGRID_CALL(w) \
   degrid_w<T, w>(d_recs, d_perm, d_hive_start, M, g, d_fw, d_vis, method, d_counter, st)
   CG_W_SWITCH(g.kw, CG_DEGRID_CALL)

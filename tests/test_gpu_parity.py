@@ -282,10 +282,11 @@ def test_determinism(torch_cuda, c1_small):
 
 # ---------------------------------------------------------------- tiled kernels
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 2e-6)])
-@pytest.mark.parametrize("method", [0, 1])
+@pytest.mark.parametrize("method", [0, 1, 2])
 def test_grid_methods(torch_cuda, oracle, c1_small, precision, tol, method):
-    """Direct (global atomics) and tiled (shared-memory) gridding both match
-    the oracle's spreading of the same payload."""
+    """Direct (global atomics), warp-tiled (shared memory) and tensor-core
+    (3xTF32 hive GEMM, FP32 only; FP64 falls back to the tiled kernel)
+    gridding all match the oracle's spreading of the same payload."""
     import os
 
     os.environ["CG_GRID_METHOD"] = str(method)
@@ -358,3 +359,21 @@ def test_fft_band_pruning(torch_cuda, c1, precision, tol):
         out[prune] = (d, v)
     assert rel_l2(out["1"][0], out["0"][0]) < tol
     assert rel_l2(out["1"][1], out["0"][1]) < tol
+
+
+@pytest.mark.parametrize("eps", [5e-3, 1e-4, 1e-5, 1e-6, 1e-7])
+def test_tensor_core_gridding_widths(torch_cuda, oracle, eps):
+    """Tensor-core gridding for every kernel width it covers (W = 4..8, even
+    and odd), including sparse hives below the GEMM threshold, against the
+    oracle's spreading."""
+    import os
+
+    d = synth.make("ms2dirty_256_fp64", seed=17, nrow=30000)
+    os.environ["CG_GRID_METHOD"] = "2"
+    try:
+        plan, _, _ = plan_ms2dirty(torch_cuda, d, "fp32", eps, stop=2)
+    finally:
+        del os.environ["CG_GRID_METHOD"]
+    p = oracle.setup(d["uvw"], 256, 256, 2.0, 1e8, eps, eps_floor=6e-8)
+    ref = oracle.grid(p, oracle.grid_coords(p, d["uvw"]), _payload(d, p))
+    assert rel_l2(plan.copy_buffer(_lib.CG_BUF_GRID), ref) < 2e-6
