@@ -11,20 +11,25 @@
 //   A = Re/Im(c_j) * kz_j[z] * ky_j[y],   B = kx_j[x]
 //
 // i.e. M = 2*EZ*EXT (padded to 16), N = EXT (padded to 16), K = rows of the
-// hive (in chunks of 8).  The products run on the tensor cores as 3xTF32
-// mma.sync.m16n8k8 (hi*hi + hi*lo + lo*hi, ~2^-21 relative error) with FP32
-// accumulators held in registers, so no per-tap shared-memory read-modify-
-// write is needed; each hive's block is committed once to the zero-filled
+// hive (in chunks of 8).  The products run on the tensor cores as split-TF32
+// mma.sync.m16n8k8: every FP32 operand is split into two TF32 parts and all
+// four part products are summed (residual ~2^-22 relative); each chunk's
+// products go into a zeroed fragment that is added to the FP32 register
+// accumulator with IEEE adds, so the tensor core's own accumulation depth
+// stays 32 terms.  No per-tap shared-memory read-modify-write is needed;
+// each hive's block is committed once to the zero-filled
 // grid with vector reductions (red.global.add.v2.f32).  Hives with fewer than
 // kMmaMinRows rows are spread directly by the warp (lanes over taps).
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 
 #include "cg_coords.cuh"
 #include "cg_launch.cuh"
 
 namespace cg {
 
+// hives with fewer rows are spread directly (CG_MMA_MIN_ROWS overrides)
 constexpr int kMmaMinRows = 4;
 
 __device__ __forceinline__ uint32_t f2tf32(float x) {
@@ -62,6 +67,8 @@ struct MmaShape {
   static constexpr int MT = (M + 15) / 16;
   static constexpr int NT = (EXT + 7) / 8;
   static constexpr int TXS = NT * 8;                        // padded table width
+  // m-tiles per pass: large blocks run in two passes to bound the registers
+  static constexpr int MTB = MT > 10 ? (MT + 1) / 2 : MT;
 };
 
 // Per-warp shared tables of one chunk of 8 rows:
@@ -81,7 +88,7 @@ struct ChunkTables {
 template <int W>
 __global__ void __launch_bounds__(256) k_grid_mma(const Rec<float>* __restrict__ recs,
                                                   const int* __restrict__ hive_start, Geom g,
-                                                  float* __restrict__ fw) {
+                                                  float* __restrict__ fw, int min_rows) {
   using S = MmaShape<W>;
   __shared__ ChunkTables<W> tabs[8];  // one per warp (256 threads)
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -111,7 +118,7 @@ __global__ void __launch_bounds__(256) k_grid_mma(const Rec<float>* __restrict__
       // block origin in grid cells (may be negative: wrapped at commit)
       const int bx0 = hx * 8 + S::OMIN, by0 = hy * 8 + S::OMIN, bz0 = hz + S::OMIN;
 
-      if (n < kMmaMinRows) {
+      if (n < min_rows) {
         // direct: lanes over the W^3 taps of one row at a time
         for (int j = 0; j < n; j++) {
           const Rec<float> r = recs[start + j];
@@ -142,9 +149,10 @@ __global__ void __launch_bounds__(256) k_grid_mma(const Rec<float>* __restrict__
         continue;
       }
 
-      float acc[S::MT][S::NT][4];
+      for (int mbase = 0; mbase < S::MT; mbase += S::MTB) {
+      float acc[S::MTB][S::NT][4];
 #pragma unroll
-      for (int mt = 0; mt < S::MT; mt++)
+      for (int mt = 0; mt < S::MTB; mt++)
 #pragma unroll
         for (int nt = 0; nt < S::NT; nt++)
 #pragma unroll
@@ -208,7 +216,9 @@ __global__ void __launch_bounds__(256) k_grid_mma(const Rec<float>* __restrict__
         }
         // ---- A fragments (z, y, re/im) and the products
 #pragma unroll
-        for (int mt = 0; mt < S::MT; mt++) {
+        for (int mtl = 0; mtl < S::MTB; mtl++) {
+          const int mt = mbase + mtl;
+          if (mt >= S::MT) break;
           const int r0 = mt * 16 + gid, r1 = r0 + 8;
           const int ri = r0 & 1;  // r1 has the same parity
           const int zy0 = r0 >> 1, zy1 = r1 >> 1;
@@ -224,20 +234,28 @@ __global__ void __launch_bounds__(256) k_grid_mma(const Rec<float>* __restrict__
           for (int e = 0; e < 4; e++) split_tf32(a[e], ah[e], al[e]);
 #pragma unroll
           for (int nt = 0; nt < S::NT; nt++) {
-            mma_tf32(acc[mt][nt], al[0], al[1], al[2], al[3], bh[nt][0], bh[nt][1]);
-            mma_tf32(acc[mt][nt], ah[0], ah[1], ah[2], ah[3], bl[nt][0], bl[nt][1]);
-            mma_tf32(acc[mt][nt], ah[0], ah[1], ah[2], ah[3], bh[nt][0], bh[nt][1]);
+            // the chunk's four split products (smallest first) into a zeroed
+            // temporary; the running sum is kept with IEEE adds
+            float t[4] = {0.f, 0.f, 0.f, 0.f};
+            mma_tf32(t, al[0], al[1], al[2], al[3], bl[nt][0], bl[nt][1]);
+            mma_tf32(t, al[0], al[1], al[2], al[3], bh[nt][0], bh[nt][1]);
+            mma_tf32(t, ah[0], ah[1], ah[2], ah[3], bl[nt][0], bl[nt][1]);
+            mma_tf32(t, ah[0], ah[1], ah[2], ah[3], bh[nt][0], bh[nt][1]);
+#pragma unroll
+            for (int e = 0; e < 4; e++) acc[mtl][nt][e] += t[e];
           }
         }
       }
       // ---- commit: rows r (re) and r + 1 (im) of a cell live in lanes gid, gid + 1
 #pragma unroll
-      for (int mt = 0; mt < S::MT; mt++) {
+      for (int mtl = 0; mtl < S::MTB; mtl++) {
+        const int mt = mbase + mtl;
+        if (mt >= S::MT) break;
 #pragma unroll
         for (int nt = 0; nt < S::NT; nt++) {
           float im[4];
 #pragma unroll
-          for (int e = 0; e < 4; e++) im[e] = __shfl_down_sync(0xffffffffu, acc[mt][nt][e], 4);
+          for (int e = 0; e < 4; e++) im[e] = __shfl_down_sync(0xffffffffu, acc[mtl][nt][e], 4);
           if ((gid & 1) == 0) {
 #pragma unroll
             for (int hr = 0; hr < 2; hr++) {
@@ -249,7 +267,7 @@ __global__ void __launch_bounds__(256) k_grid_mma(const Rec<float>* __restrict__
 #pragma unroll
               for (int cx = 0; cx < 2; cx++) {
                 const int x = nt * 8 + 2 * tig + cx;
-                const float re = acc[mt][nt][2 * hr + cx], iv = im[2 * hr + cx];
+                const float re = acc[mtl][nt][2 * hr + cx], iv = im[2 * hr + cx];
                 if (x < S::EXT && (re != 0.f || iv != 0.f))
                   red_add_v2(fw + 2 * (rowo + modi(bx0 + x, nf1)), re, iv);
               }
@@ -257,6 +275,7 @@ __global__ void __launch_bounds__(256) k_grid_mma(const Rec<float>* __restrict__
           }
         }
       }
+      }  // m-tile passes
     }
   }
 }
@@ -275,7 +294,9 @@ static int grid_mma_w(const Rec<float>* d_recs, const int* d_hive_start, const G
   const int64_t nh = (int64_t)g.nhx * g.nhy * g.nhz;
   int64_t blocks = std::min<int64_t>((int64_t)per_sm * sms, (nh + 255) / 256);
   if (blocks < 1) blocks = 1;
-  k_grid_mma<W><<<(int)blocks, 256, 0, st>>>(d_recs, d_hive_start, g, d_fw);
+  const char* env = getenv("CG_MMA_MIN_ROWS");
+  const int min_rows = env ? atoi(env) : kMmaMinRows;
+  k_grid_mma<W><<<(int)blocks, 256, 0, st>>>(d_recs, d_hive_start, g, d_fw, min_rows);
   count_launches(1);
   CG_CUDA(cudaGetLastError());
   return CG_OK;
