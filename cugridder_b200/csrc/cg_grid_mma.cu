@@ -88,7 +88,8 @@ struct ChunkTables {
 template <int W>
 __global__ void __launch_bounds__(256) k_grid_mma(const Rec<float>* __restrict__ recs,
                                                   const int* __restrict__ hive_start, Geom g,
-                                                  float* __restrict__ fw, int min_rows) {
+                                                  float* __restrict__ fw, int min_rows,
+                                                  int64_t nchunks, int64_t perm_mul) {
   using S = MmaShape<W>;
   __shared__ ChunkTables<W> tabs[8];  // one per warp (256 threads)
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -100,7 +101,10 @@ __global__ void __launch_bounds__(256) k_grid_mma(const Rec<float>* __restrict__
   const int64_t gwarp = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
   const int64_t nwarps = (int64_t)gridDim.x * (blockDim.x >> 5);
 
-  for (int64_t hbase = gwarp * 32; hbase < nh; hbase += nwarps * 32) {
+  // chunks of 32 hives, visited in a multiplicative permutation of their
+  // order so that the dense part of the grid is spread over all warps
+  for (int64_t c = gwarp; c < nchunks; c += nwarps) {
+    const int64_t hbase = ((c * perm_mul) % nchunks) * 32;
     const int64_t hl = hbase + lane;
     int s0 = 0, cnt = 0;
     if (hl < nh) {
@@ -296,7 +300,18 @@ static int grid_mma_w(const Rec<float>* d_recs, const int* d_hive_start, const G
   if (blocks < 1) blocks = 1;
   const char* env = getenv("CG_MMA_MIN_ROWS");
   const int min_rows = env ? atoi(env) : kMmaMinRows;
-  k_grid_mma<W><<<(int)blocks, 256, 0, st>>>(d_recs, d_hive_start, g, d_fw, min_rows);
+  const int64_t nchunks = (nh + 31) / 32;
+  // a prime multiplier coprime with the chunk count (a permutation mod nchunks)
+  int64_t mul = 1;
+  const int64_t primes[] = {1000003, 999983, 1299709, 15485863, 32452843};
+  for (int64_t p : primes)
+    if (nchunks % p != 0) {
+      mul = p % nchunks;
+      if (mul == 0) mul = 1;
+      break;
+    }
+  k_grid_mma<W><<<(int)blocks, 256, 0, st>>>(d_recs, d_hive_start, g, d_fw, min_rows, nchunks,
+                                             mul);
   count_launches(1);
   CG_CUDA(cudaGetLastError());
   return CG_OK;
