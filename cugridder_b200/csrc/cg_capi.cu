@@ -209,7 +209,7 @@ int cg_plan_create(cg_plan** plan, int nxdirty, int nydirty, double fov, double 
   P->stream = (cudaStream_t)stream;
   if (const char* m = getenv("CG_GRID_METHOD")) {
     const int v = atoi(m);
-    P->grid_method = (v >= 0 && v <= 2) ? v : 2;
+    P->grid_method = (v >= 0 && v <= 2) ? v : 1;
   }
   if (const char* m = getenv("CG_FFT_PRUNE")) P->fft_pruning = atoi(m) != 0;
   st = cg::plan_configure(P, nxdirty, nydirty, fov, epsilon, sigma, sign, precision);

@@ -45,7 +45,7 @@ struct cg_plan_s {
   int64_t nrow = 0;
   int key_bytes = 4;
   int stop_stage = 0;
-  int grid_method = 2;  // 0 direct, 1 tiled SIMT, 2 tensor-core (cg_plan_set_method, CG_GRID_METHOD)
+  int grid_method = 1;  // 0 direct, 1 tiled SIMT, 2 tensor-core (cg_plan_set_method, CG_GRID_METHOD)
   // device buffers
   cg_dev_buf mm, K1, K2, K3q, zq, grid, recs, perm, skeys, hive_start, binws, fftwork, io_uvw,
       io_vis, io_wgt, io_dirty;

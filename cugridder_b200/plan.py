@@ -65,7 +65,7 @@ class Plan:
         return inf.as_dict()
 
     def set_method(self, method):
-        """2 = tensor-core gridding where supported (default), 1 = tiled SIMT, 0 = direct."""
+        """1 = tiled SIMT (default), 2 = tensor-core gridding where supported, 0 = direct."""
         _lib.check(self._lib.cg_plan_set_method(self._h, int(method)))
 
     def set_stop_stage(self, stage):

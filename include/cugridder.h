@@ -151,10 +151,10 @@ int cg_plan_destroy(cg_plan *plan);
 int cg_plan_copy_buffer(cg_plan *plan, int which, void *host_dst, size_t bytes,
                         size_t *bytes_needed);
 
-/* Spreading / interpolation method: 2 = tensor-core gridding for FP32 with
- * W <= 8, tiled shared-memory kernels otherwise (default); 1 = tiled
- * shared-memory kernels; 0 = direct kernels with global atomics / gathers
- * (cross-check). */
+/* Spreading / interpolation method: 1 = tiled shared-memory kernels
+ * (default); 2 = tensor-core gridding (split-TF32 mma.sync per hive) for FP32
+ * with W <= 8, tiled kernels otherwise; 0 = direct kernels with global
+ * atomics / gathers (cross-check). */
 int cg_plan_set_method(cg_plan *plan, int method);
 
 /* Stops the next calls after a stage (testing): 0 = run to the end,
