@@ -82,6 +82,9 @@ SIGNATURES = {
     "cg_plan_set_timing": (c_int, [c_void_p, c_int]),
     "cg_plan_get_timing": (c_int, [c_void_p, c_int, ctypes.POINTER(c_double), c_int,
                                    ctypes.POINTER(c_int), ctypes.POINTER(ctypes.c_longlong)]),
+    "cg_bin_static": (c_int, [c_int64, c_int, c_int, c_double, c_double, _PTR, c_double, c_double,
+                              c_int, c_int, _PTR, _PTR, c_int64, ctypes.POINTER(c_int64), c_void_p]),
+    "cg_bin_static_max_rows": (c_int64, []),
     "cg_release_cache": (c_int, []),
     "cg_last_error": (ctypes.c_char_p, []),
     "cg_kernel_launches": (ctypes.c_longlong, []),

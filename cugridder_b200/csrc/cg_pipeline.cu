@@ -34,7 +34,7 @@ static int next235beven(int n, int b) {
 }
 
 // setup_conv_opts: conv_interp_invoker.cu:49-119
-static int setup_conv_opts(double eps, double sigma, double eps_floor, int& kw, double& beta,
+int setup_conv_opts(double eps, double sigma, double eps_floor, int& kw, double& beta,
                            double& c) {
   int st = CG_OK;
   if (!(sigma > 1.0)) return CG_ERR_ARG;
@@ -57,14 +57,14 @@ static int setup_conv_opts(double eps, double sigma, double eps_floor, int& kw, 
 }
 
 // get_num_cells: conv_interp_invoker.cu:30-47
-static int get_num_cells(int ms, double sigma, int kw) {
+int get_num_cells(int ms, double sigma, int kw) {
   int nf = (int)(sigma * ms);
   if (nf < 2 * kw) nf = 2 * kw;
   return next235beven(nf, 1);
 }
 
 // set_nhg_w: utils.cu:670-709
-static void set_nhg_w(double S, double X, int kw, double sigma, int& nf, double& h, double& gam) {
+void set_nhg_w(double S, double X, int kw, double sigma, int& nf, double& h, double& gam) {
   int nss = kw + 1;
   double Xsafe = X, Ssafe = S;
   if (X == 0.0) {

@@ -173,6 +173,26 @@ int cg_plan_set_timing(cg_plan *plan, int on);
 int cg_plan_get_timing(cg_plan *plan, int direction, double *stage_ms, int cap, int *nstages,
                        long long *ncalls);
 
+/* Allocation-free hive binning (no reference counterpart).  Runs the binning
+ * stage of a plan call -- w range, stable sort of the rows by the hive-major
+ * cell key, hive offsets -- on DEVICE uvw [nrow][3] and writes the same
+ * d_perm [nrow] (original row of each sorted row, as CG_BUF_PERM) and
+ * d_hive_start [n_hives + 1] (as CG_BUF_HIVE_START) that a plan with the same
+ * nxdirty, nydirty, fov, epsilon, sigma, sign and precision computes.
+ * It allocates nothing: its scratch is a fixed 15 MiB device array inside the
+ * library, so nrow is limited to cg_bin_static_max_rows() (524,288) and
+ * larger nrow returns CG_ERR_SIZE.  When hive_start_len < n_hives + 1 (or
+ * d_hive_start is NULL) it stores n_hives, returns CG_ERR_SIZE and writes no
+ * output.  Synchronizes `stream` once (w range read-back).  The first call on
+ * a device looks up the scratch address (module load); make it before any
+ * stream capture.  Overlapping calls on one device race on the shared
+ * scratch. */
+int cg_bin_static(int64_t nrow, int nxdirty, int nydirty, double fov, double freq,
+                  const double *d_uvw, double epsilon, double sigma, int sign, int precision,
+                  int *d_perm, int *d_hive_start, int64_t hive_start_len, int64_t *n_hives,
+                  void *stream);
+int64_t cg_bin_static_max_rows(void);
+
 /* Host-pointer calls above keep one cached plan per precision so that
  * repeated calls reuse device workspace; this frees it. */
 int cg_release_cache(void);
