@@ -25,6 +25,8 @@ CG_BUF_GRID = 4
 CG_BUF_FSERIES_1 = 5
 CG_BUF_FSERIES_2 = 6
 CG_BUF_FSERIES_W = 7
+CG_KERNEL_ES = 0
+CG_KERNEL_POLY = 1
 
 STATUS = {
     0: "ok", 1: "epsilon clipped to the precision floor", 2: "invalid argument",
@@ -85,6 +87,20 @@ SIGNATURES = {
     "cg_bin_static": (c_int, [c_int64, c_int, c_int, c_double, c_double, _PTR, c_double, c_double,
                               c_int, c_int, _PTR, _PTR, c_int64, ctypes.POINTER(c_int64), c_void_p]),
     "cg_bin_static_max_rows": (c_int64, []),
+    "cg_plan_set_kernel": (c_int, [c_void_p, c_int, c_int, _PTR]),
+    "cg_learn_theta_size": (c_int, []),
+    "cg_learn_phi_forward": (c_int, [_PTR, c_float, c_int, c_int64, _PTR, _PTR, c_void_p]),
+    "cg_learn_phi_backward": (c_int, [_PTR, c_float, c_int, c_int64, _PTR, _PTR, _PTR, c_void_p]),
+    "cg_learn_spread2d": (c_int, [c_int, c_int, c_int, c_int, _PTR, _PTR, _PTR, _PTR, _PTR, _PTR,
+                                  c_void_p]),
+    "cg_learn_spread2d_adjoint": (c_int, [c_int, c_int, c_int, c_int, _PTR, _PTR, _PTR, _PTR, _PTR,
+                                          _PTR, _PTR, _PTR, c_void_p]),
+    "cg_learn_dft2": (c_int, [c_int, c_int, c_int, _PTR, _PTR, _PTR, c_int, _PTR, _PTR, _PTR,
+                              c_void_p]),
+    "cg_explicit_ms2dirty": (c_int, [c_int64, c_int, c_int, c_double, c_double, _PTR, _PTR, _PTR,
+                                     c_int, c_int64, _PTR, _PTR, c_void_p]),
+    "cg_explicit_dirty2ms": (c_int, [c_int64, c_int, c_int, c_double, c_double, _PTR, _PTR, _PTR,
+                                     c_int, c_int64, _PTR, _PTR, c_void_p]),
     "cg_release_cache": (c_int, []),
     "cg_last_error": (ctypes.c_char_p, []),
     "cg_kernel_launches": (ctypes.c_longlong, []),

@@ -24,7 +24,8 @@ LIB = os.path.join(LIBDIR, "libcugridder.so")
 ALIAS = os.path.join(LIBDIR, "libcurafft.so")
 
 SOURCES = ["cg_bin.cu", "cg_spread.cu", "cg_grid_mma.cu", "cg_wstage.cu", "cg_pipeline.cu",
-           "cg_capi.cu", "cg_static.cu"]
+           "cg_capi.cu", "cg_static.cu", "cg_learn.cu",
+           "cg_explicit.cu"]
 
 
 def _nvcc():

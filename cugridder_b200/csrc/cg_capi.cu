@@ -6,6 +6,7 @@
 // device buffer and cuFFT plan inside each call (cugridder.cu:309-388), they
 // share one cached plan per precision so repeated calls reuse HBM workspace;
 // cg_release_cache() frees it.  Errors are returned, never exit()ed.
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -49,7 +50,7 @@ void destroy_plan(cg_plan_s* P) {
   if (P->cols_valid) cufftDestroy(P->fft_cols);
   cg_dev_buf* bs[] = {&P->mm,   &P->K1,    &P->K2,     &P->K3q,    &P->zq,     &P->grid,
                       &P->recs, &P->perm,  &P->skeys,  &P->hive_start, &P->binws, &P->fftwork,
-                      &P->io_uvw, &P->io_vis, &P->io_wgt, &P->io_dirty};
+                      &P->io_uvw, &P->io_vis, &P->io_wgt, &P->io_dirty, &P->polyf, &P->polyd};
   for (auto b : bs) cg::release(*b);
   if (P->h_mm) cudaFreeHost(P->h_mm);
   if (P->timer.created)
@@ -274,6 +275,36 @@ int cg_plan_set_method(cg_plan* plan, int method) {
   if (!plan || method < 0 || method > 2) return CG_ERR_ARG;
   plan->grid_method = method;
   return CG_OK;
+}
+
+int cg_plan_set_kernel(cg_plan* plan, int kind, int W, const double* coef) {
+  if (!plan || (kind != CG_KERNEL_ES && kind != CG_KERNEL_POLY)) return CG_ERR_ARG;
+  std::lock_guard<std::mutex> lock(plan->mu);
+  if (kind == CG_KERNEL_POLY) {
+    if (W < 2 || W > cg::kMaxW || !coef) {
+      cg::set_last_error("polynomial kernel needs 2 <= W <= 16 and W*8 coefficients");
+      return CG_ERR_ARG;
+    }
+    for (int i = 0; i < W * cg::kPolyCoef; i++)
+      if (!std::isfinite(coef[i])) {
+        cg::set_last_error("non-finite kernel coefficient");
+        return CG_ERR_ARG;
+      }
+    memcpy(plan->poly, coef, sizeof(double) * W * cg::kPolyCoef);
+    plan->poly_w = W;
+  } else {
+    if (W != 0 && (W < 2 || W > cg::kMaxW)) {
+      cg::set_last_error("ES kernel width must be 0 (from epsilon) or 2..16");
+      return CG_ERR_ARG;
+    }
+    plan->es_w = W;
+  }
+  plan->kernel_kind = kind;
+  CG_CUDA(cudaSetDevice(plan->device));
+  plan->kw = 0;  // force plan_configure to recompute W, grid sizes and the Fourier series
+  int st = cg::plan_configure(plan, plan->nx, plan->ny, plan->fov, plan->eps, plan->sigma,
+                              plan->sign, plan->precision);
+  return st > 1 ? st : CG_OK;
 }
 
 int cg_plan_set_stop_stage(cg_plan* plan, int stage) {

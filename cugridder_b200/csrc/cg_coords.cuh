@@ -72,12 +72,44 @@ template <int W, typename T>
 __device__ __forceinline__ int tap_offset(T f) {
   return (W % 2 == 0) ? 1 - W / 2 : (f < (T)0.5 ? -(W / 2) : 1 - (W / 2));
 }
+// Piecewise-polynomial kernel: segment i covers d in [i - W/2, i + 1 - W/2);
+// tap i of a row evaluates segment i at z = (first tap - b) + W/2 - f, which
+// lies in (0, 1] for every tap, as P_i(2z - 1) = sum_n a[i][n] (2z - 1)^n.
+template <typename T>
+__device__ __forceinline__ T poly_eval(const T* __restrict__ a, T t) {
+  T v = a[kPolyCoef - 1];
+#pragma unroll
+  for (int n = kPolyCoef - 2; n >= 0; n--) v = fma(v, t, a[n]);
+  return v;
+}
+template <int W, typename T>
+__device__ __forceinline__ T poly_arg(T f) {
+  return (T)2 * (((T)tap_offset<W>(f) + (T)W * (T)0.5) - f) - (T)1;
+}
+template <typename T>
+__device__ __forceinline__ const T* geom_poly(const Geom& g);
+template <>
+__device__ __forceinline__ const float* geom_poly<float>(const Geom& g) { return g.polyf; }
+template <>
+__device__ __forceinline__ const double* geom_poly<double>(const Geom& g) { return g.polyd; }
+
+template <typename T>
+inline const T* geom_poly_host(const Geom& g) {
+  if constexpr (sizeof(T) == 4) return (const T*)g.polyf; else return (const T*)g.polyd;
+}
+
 template <typename T, int W>
-__device__ __forceinline__ int taps(T f, T beta, T c, T* k) {
+__device__ __forceinline__ int taps(T f, T beta, T c, const T* __restrict__ poly, T* k) {
   const T halfw = (T)W * (T)0.5;
   int o = tap_offset<W>(f);
+  if (poly) {
+    const T t = poly_arg<W>(f);
 #pragma unroll
-  for (int i = 0; i < W; i++) k[i] = es_kernel<T>((T)(o + i) - f, beta, c, halfw);
+    for (int i = 0; i < W; i++) k[i] = poly_eval(poly + i * kPolyCoef, t);
+  } else {
+#pragma unroll
+    for (int i = 0; i < W; i++) k[i] = es_kernel<T>((T)(o + i) - f, beta, c, halfw);
+  }
   return o;
 }
 

@@ -37,7 +37,13 @@ struct Geom {
   // grid rows (g1) / columns (g0) the data can touch, inclusive; the full
   // range when the data wraps around the grid edge
   int band_r0, band_r1, band_c0, band_c1;
+  // piecewise-polynomial kernel (learned kernel): W segments x kPolyCoef
+  // coefficients in the working precision; null pointers select ES
+  const float* polyf;
+  const double* polyd;
 };
+
+constexpr int kPolyCoef = 8;  // degree-7 Horner polynomial per segment
 
 // Kernel Fourier-series quadrature: phi_hat(k) = sum_i g[i] * 2 cos(x[i] k)
 struct Quad {

@@ -33,6 +33,16 @@ static int next235beven(int n, int b) {
   return nplus;
 }
 
+// beta / W of the ES kernel for width kw (conv_interp_invoker.cu:87-114)
+static double es_beta_over_w(int kw, double sigma) {
+  double betaoverns = 2.30;
+  if (kw == 2) betaoverns = 2.20;
+  if (kw == 3) betaoverns = 2.26;
+  if (kw == 4) betaoverns = 2.38;
+  if (sigma != 2.0) betaoverns = 0.97 * kPi * (1 - 1 / (2 * sigma));
+  return betaoverns;
+}
+
 // setup_conv_opts: conv_interp_invoker.cu:49-119
 int setup_conv_opts(double eps, double sigma, double eps_floor, int& kw, double& beta,
                            double& c) {
@@ -46,12 +56,7 @@ int setup_conv_opts(double eps, double sigma, double eps_floor, int& kw, double&
   if (sigma != 2.0) kw = (int)std::ceil(-std::log(eps) / (kPi * std::sqrt(1.0 - 1.0 / sigma)));
   kw = std::max(2, kw);
   kw = std::min(kMaxW, kw);
-  double betaoverns = 2.30;
-  if (kw == 2) betaoverns = 2.20;
-  if (kw == 3) betaoverns = 2.26;
-  if (kw == 4) betaoverns = 2.38;
-  if (sigma != 2.0) betaoverns = 0.97 * kPi * (1 - 1 / (2 * sigma));
-  beta = betaoverns * (double)kw;
+  beta = es_beta_over_w(kw, sigma) * (double)kw;
   c = 4.0 / (double)(kw * kw);
   return st;
 }
@@ -117,8 +122,21 @@ static void gauss_legendre(int n, double* x, double* w) {
   }
 }
 
-// quadrature of the ES kernel Fourier series (deconv.cu:80-93)
-static void make_quad(int kw, double beta, double c, Quad& q) {
+// piecewise-polynomial kernel value at d (segment floor(d + W/2)); 0 outside
+static double poly_phi(const double* poly, int kw, double d) {
+  const double u = d + 0.5 * kw;
+  const int s = (int)std::floor(u);
+  if (s < 0 || s >= kw) return 0.0;
+  const double t = 2.0 * (u - s) - 1.0;
+  const double* a = poly + s * kPolyCoef;
+  double v = a[kPolyCoef - 1];
+  for (int n = kPolyCoef - 2; n >= 0; n--) v = v * t + a[n];
+  return v;
+}
+
+// quadrature of the kernel Fourier series (deconv.cu:80-93): ES, or the
+// piecewise-polynomial kernel when poly is given
+static void make_quad(int kw, double beta, double c, const double* poly, Quad& q) {
   double alpha = kw / 2.0;
   int p = (int)(2 + 3.0 * alpha);
   double x[2 * kMaxQuad], w[2 * kMaxQuad];
@@ -126,7 +144,8 @@ static void make_quad(int kw, double beta, double c, Quad& q) {
   q.p = p;
   for (int n = 0; n < p; n++) {
     double xn = x[n] * alpha;
-    double phi = (std::fabs(xn) <= alpha) ? std::exp(beta * std::sqrt(1.0 - c * xn * xn)) : 0.0;
+    double phi = poly ? poly_phi(poly, kw, xn)
+                      : ((std::fabs(xn) <= alpha) ? std::exp(beta * std::sqrt(1.0 - c * xn * xn)) : 0.0);
     q.x[n] = xn;
     q.g[n] = alpha * w[n] * phi;
   }
@@ -232,6 +251,16 @@ int plan_configure(cg_plan_s* P, int nx, int ny, double fov, double eps, double 
     set_last_error("sigma must be > 1");
     return st;
   }
+  const bool poly = P->kernel_kind == CG_KERNEL_POLY;
+  if (poly) {  // the kernel's own width replaces the width chosen from epsilon
+    kw = P->poly_w;
+    beta = 0.0;
+    c = 0.0;
+  } else if (P->es_w > 0) {  // ES at a forced width: the same beta rule for that W
+    kw = P->es_w;
+    beta = es_beta_over_w(kw, sigma) * kw;
+    c = 4.0 / (double)(kw * kw);
+  }
   int nf1 = get_num_cells(ny, sigma, kw), nf2 = get_num_cells(nx, sigma, kw);
   if (nf1 > 65535 || nf2 > 65535) {
     set_last_error("grid larger than 65535 cells per axis");
@@ -250,7 +279,15 @@ int plan_configure(cg_plan_s* P, int nx, int ny, double fov, double eps, double 
   P->es_c = c;
   P->nf1 = nf1;
   P->nf2 = nf2;
-  make_quad(kw, beta, c, P->quad);
+  make_quad(kw, beta, c, poly ? P->poly : nullptr, P->quad);
+  if (poly) {
+    float pf[kMaxW * kPolyCoef];
+    for (int i = 0; i < kw * kPolyCoef; i++) pf[i] = (float)P->poly[i];
+    CG_TRY(ensure(P->polyd, sizeof(double) * kw * kPolyCoef));
+    CG_TRY(ensure(P->polyf, sizeof(float) * kw * kPolyCoef));
+    CG_CUDA(cudaMemcpy(P->polyd.p, P->poly, sizeof(double) * kw * kPolyCoef, cudaMemcpyHostToDevice));
+    CG_CUDA(cudaMemcpy(P->polyf.p, pf, sizeof(float) * kw * kPolyCoef, cudaMemcpyHostToDevice));
+  }
   std::vector<double> k1(nf1 / 2 + 1), k2(nf2 / 2 + 1);
   fseries_uv(P->quad, nf1, k1.data());
   fseries_uv(P->quad, nf2, k2.data());
@@ -300,6 +337,9 @@ static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw)
   g.pixy = P->fov / 180.0 * kPi / (double)g.N1;
   g.foc = freq / kSpeedOfLight;
   g.sign = P->sign;
+  const bool poly = P->kernel_kind == CG_KERNEL_POLY;
+  g.polyf = poly ? (const float*)P->polyf.p : nullptr;
+  g.polyd = poly ? (const double*)P->polyd.p : nullptr;
   double wmin = 0, wmax = 0;
   if (nrow > 0) {
     double rmin = decode_ordered(P->h_mm[4]), rmax = decode_ordered(P->h_mm[5]);

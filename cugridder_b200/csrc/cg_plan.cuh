@@ -46,9 +46,15 @@ struct cg_plan_s {
   int key_bytes = 4;
   int stop_stage = 0;
   int grid_method = 1;  // 0 direct, 1 tiled SIMT, 2 tensor-core (cg_plan_set_method, CG_GRID_METHOD)
+  // gridding kernel: CG_KERNEL_ES (W from epsilon) or CG_KERNEL_POLY (W and
+  // piecewise-polynomial coefficients given by cg_plan_set_kernel)
+  int kernel_kind = CG_KERNEL_ES;
+  int poly_w = 0;
+  int es_w = 0;  // CG_KERNEL_ES with a forced width (0: from epsilon)
+  double poly[cg::kMaxW * cg::kPolyCoef] = {};
   // device buffers
   cg_dev_buf mm, K1, K2, K3q, zq, grid, recs, perm, skeys, hive_start, binws, fftwork, io_uvw,
-      io_vis, io_wgt, io_dirty;
+      io_vis, io_wgt, io_dirty, polyf, polyd;
   unsigned long long* h_mm = nullptr;  // pinned, 2 words + flag
   // cuFFT: full 2-D batched plan, and the 1-D plans of the band-pruned path
   cufftHandle fft = 0;

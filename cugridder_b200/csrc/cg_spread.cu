@@ -33,6 +33,7 @@ template <typename T, int W>
 __global__ void __launch_bounds__(256) k_grid_direct(const Rec<T>* __restrict__ recs, int64_t M,
                                                      Geom g, T* __restrict__ fw) {
   const T beta = (T)g.beta, c = (T)g.es_c;
+  const T* __restrict__ poly = geom_poly<T>(g);
   const int nf1 = g.nf1, nf2 = g.nf2, nw = g.nw;
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < M;
        s += (int64_t)gridDim.x * blockDim.x) {
@@ -40,9 +41,9 @@ __global__ void __launch_bounds__(256) k_grid_direct(const Rec<T>* __restrict__ 
     T kx[W], ky[W], kz[W];
     const int bx = (int)(r.bxy & 0xFFFFu), by = (int)(r.bxy >> 16), bz = (int)r.bz;
     if (bx >= nf1 || by >= nf2 || bz >= nw) continue;  // cells always in range; never indexes wild
-    const int ox = bx + taps<T, W>(r.f[0], beta, c, kx);
-    const int oy = by + taps<T, W>(r.f[1], beta, c, ky);
-    const int oz = bz + taps<T, W>(r.f[2], beta, c, kz);
+    const int ox = bx + taps<T, W>(r.f[0], beta, c, poly, kx);
+    const int oy = by + taps<T, W>(r.f[1], beta, c, poly, ky);
+    const int oz = bz + taps<T, W>(r.f[2], beta, c, poly, kz);
 #pragma unroll 1
     for (int a = 0; a < W; a++) {
       const int zz = wrapi(oz + a, nw);
@@ -69,6 +70,7 @@ __global__ void __launch_bounds__(256) k_degrid_direct(const Rec<T>* __restrict_
                                                        Geom g, const T* __restrict__ fw,
                                                        T* __restrict__ vis) {
   const T beta = (T)g.beta, c = (T)g.es_c;
+  const T* __restrict__ poly = geom_poly<T>(g);
   const int nf1 = g.nf1, nf2 = g.nf2, nw = g.nw;
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < M;
        s += (int64_t)gridDim.x * blockDim.x) {
@@ -76,9 +78,9 @@ __global__ void __launch_bounds__(256) k_degrid_direct(const Rec<T>* __restrict_
     T kx[W], ky[W], kz[W];
     const int bx = (int)(r.bxy & 0xFFFFu), by = (int)(r.bxy >> 16), bz = (int)r.bz;
     if (bx >= nf1 || by >= nf2 || bz >= nw) continue;
-    const int ox = bx + taps<T, W>(r.f[0], beta, c, kx);
-    const int oy = by + taps<T, W>(r.f[1], beta, c, ky);
-    const int oz = bz + taps<T, W>(r.f[2], beta, c, kz);
+    const int ox = bx + taps<T, W>(r.f[0], beta, c, poly, kx);
+    const int oy = by + taps<T, W>(r.f[1], beta, c, poly, ky);
+    const int oz = bz + taps<T, W>(r.f[2], beta, c, poly, kz);
     T sr = 0, si = 0;
 #pragma unroll 1
     for (int a = 0; a < W; a++) {
@@ -324,7 +326,7 @@ struct Cplx<float> { using type = float2; };
 template <>
 struct Cplx<double> { using type = double2; };
 
-template <typename T, int W>
+template <typename T, int W, bool kPoly>
 __global__ void __launch_bounds__(256) k_grid_warp(const Rec<T>* __restrict__ recs,
                                                    const int* __restrict__ hive_start, Geom g,
                                                    WarpTile tc, T* __restrict__ fw) {
@@ -341,6 +343,18 @@ __global__ void __launch_bounds__(256) k_grid_warp(const Rec<T>* __restrict__ re
   const int ts = tc.slots + 1;
   SegTable t{tb, tb + ts, tb + 2 * ts, tb + 3 * ts, tb + 4 * ts};
   const T beta = (T)g.beta, c = (T)g.es_c, halfw = (T)W * (T)0.5;
+  // piecewise-polynomial kernel (kPoly): the coefficients of each lane's
+  // kernel-value slots (segment i of slot s = axis * W + i), loaded once
+  T pc[kPoly ? NKV : 1][kPolyCoef];
+  if constexpr (kPoly) {
+    const T* __restrict__ poly = geom_poly<T>(g);
+#pragma unroll
+    for (int k = 0; k < NKV; k++) {
+      const int sl = lane + 32 * k, i = sl % W;
+#pragma unroll
+      for (int n = 0; n < kPolyCoef; n++) pc[k][n] = (sl < 3 * W) ? poly[i * kPolyCoef + n] : (T)0;
+    }
+  }
   const int nf1 = g.nf1, nf2 = g.nf2, nw = g.nw;
   const size_t plane = (size_t)nf1 * nf2;
   const int gwarp = blockIdx.x * tc.warps + wib, nwarps = gridDim.x * tc.warps;
@@ -399,7 +413,10 @@ __global__ void __launch_bounds__(256) k_grid_warp(const Rec<T>* __restrict__ re
           const int sl = lane + 32 * k;
           const int axis = sl / W, i = sl - axis * W;
           const T f = axis == 0 ? g0 : (axis == 1 ? g1 : g2);
-          kv[k] = (sl < 3 * W) ? es_kernel<T>((T)(tap_offset<W>(f) + i) - f, beta, c, halfw) : (T)0;
+          if constexpr (kPoly)
+            kv[k] = (sl < 3 * W) ? poly_eval(pc[k], poly_arg<W>(f)) : (T)0;
+          else
+            kv[k] = (sl < 3 * W) ? es_kernel<T>((T)(tap_offset<W>(f) + i) - f, beta, c, halfw) : (T)0;
         }
         T kx[W];
         unsigned xmask = 0;
@@ -470,6 +487,7 @@ __global__ void __launch_bounds__(512) k_degrid_tiled(const Rec<T>* __restrict__
   __shared__ int s_warp[33];
   __shared__ int s_item;
   const T beta = (T)g.beta, c = (T)g.es_c;
+  const T* __restrict__ poly = geom_poly<T>(g);
   const size_t plane = (size_t)nf1 * nf2;
 
   for (;;) {
@@ -503,9 +521,9 @@ __global__ void __launch_bounds__(512) k_degrid_tiled(const Rec<T>* __restrict__
       const Rec<T> r = recs[sidx];
       const int bx = (int)(r.bxy & 0xFFFFu), by = (int)(r.bxy >> 16), bz = (int)r.bz;
       T kx[W], ky[W], kz[W];
-      const int lx = bx + taps<T, W>(r.f[0], beta, c, kx) - gx0;
-      const int ly = by + taps<T, W>(r.f[1], beta, c, ky) - gy0;
-      const int lz = bz + taps<T, W>(r.f[2], beta, c, kz) - gz0;
+      const int lx = bx + taps<T, W>(r.f[0], beta, c, poly, kx) - gx0;
+      const int ly = by + taps<T, W>(r.f[1], beta, c, poly, ky) - gy0;
+      const int lz = bz + taps<T, W>(r.f[2], beta, c, poly, kz) - gz0;
       if (lx < 0 || ly < 0 || lx + W > SX || ly + W > SY) continue;  // cannot happen: tile rows only
       T sr = 0, si = 0;
       for (int a = 0; a < W; a++) {
@@ -622,17 +640,16 @@ static int grid_w(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, cons
     return CG_OK;
   }
   WarpTile tc = warp_tiling<T>(g);
-  CG_CUDA(cudaFuncSetAttribute(k_grid_warp<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)tc.smem));
+  auto* kern = geom_poly_host<T>(g) ? k_grid_warp<T, W, true> : k_grid_warp<T, W, false>;
+  CG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc.smem));
   int per_sm = 0;
-  CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_grid_warp<T, W>, tc.warps * 32,
-                                                        tc.smem));
+  CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, tc.warps * 32, tc.smem));
   if (per_sm < 1) {
     set_last_error("warp-tiled gridding does not fit on an SM");
     return CG_ERR_ARG;
   }
   int blocks = per_sm * num_sms();
-  k_grid_warp<T, W><<<blocks, tc.warps * 32, tc.smem, st>>>(d_recs, d_hive_start, g, tc, d_fw);
+  kern<<<blocks, tc.warps * 32, tc.smem, st>>>(d_recs, d_hive_start, g, tc, d_fw);
   count_launches(1);
   CG_CUDA(cudaGetLastError());
   return CG_OK;
@@ -695,8 +712,8 @@ template <typename T>
 int launch_grid(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, const Geom& g, T* d_fw,
                 int method, int* d_counter, cudaStream_t st) {
   if (method == kGridMma) {
-    // tensor-core path: FP32 and W <= 8; everything else on the SIMT kernels
-    if (sizeof(T) == 4) {
+    // tensor-core path: FP32, ES kernel and W <= 8; everything else on the SIMT kernels
+    if (sizeof(T) == 4 && !g.polyf) {
       int s = launch_grid_mma((const Rec<float>*)d_recs, d_hive_start, g, (float*)d_fw, st);
       if (s != CG_ERR_ARG) return s;
     }

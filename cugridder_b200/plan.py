@@ -68,6 +68,16 @@ class Plan:
         """1 = tiled SIMT (default), 2 = tensor-core gridding where supported, 0 = direct."""
         _lib.check(self._lib.cg_plan_set_method(self._h, int(method)))
 
+    def set_kernel(self, kind="es", W=None, coef=None):
+        """Gridding kernel: "es" (W from epsilon, or forced when W is given) or
+        "poly" with width W and a [W, 8] array of piecewise Horner coefficients
+        (a learned kernel, see cugridder_b200.learn)."""
+        if kind == "es":
+            _lib.check(self._lib.cg_plan_set_kernel(self._h, _lib.CG_KERNEL_ES, int(W or 0), None))
+            return
+        a = np.ascontiguousarray(np.asarray(coef, dtype=np.float64).reshape(int(W), 8))
+        _lib.check(self._lib.cg_plan_set_kernel(self._h, _lib.CG_KERNEL_POLY, int(W), a.ctypes.data))
+
     def set_stop_stage(self, stage):
         _lib.check(self._lib.cg_plan_set_stop_stage(self._h, int(stage)))
 

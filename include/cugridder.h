@@ -157,6 +157,22 @@ int cg_plan_copy_buffer(cg_plan *plan, int which, void *host_dst, size_t bytes,
  * atomics / gathers (cross-check). */
 int cg_plan_set_method(cg_plan *plan, int method);
 
+/* Gridding kernel of a plan (no reference counterpart; the reference always
+ * uses ES with W from epsilon).
+ *   CG_KERNEL_ES:   exp(beta sqrt(1 - (2d/W)^2)); W = 0 takes W and beta
+ *                   from epsilon (the default), W in 2..16 forces that width
+ *                   with the reference's beta for it; coef is ignored.
+ *   CG_KERNEL_POLY: a piecewise polynomial of width W (2..16): segment i
+ *                   (d in [i - W/2, i + 1 - W/2)) is
+ *                   sum_n coef[i*8 + n] * (2 (d + W/2 - i) - 1)^n, n < 8 --
+ *                   the Horner form of a learned kernel.  The kernel's
+ *                   Fourier series is computed by the same Gauss-Legendre
+ *                   quadrature as for ES, and the grid sizes follow from W.
+ * Takes effect from the next call. */
+#define CG_KERNEL_ES 0
+#define CG_KERNEL_POLY 1
+int cg_plan_set_kernel(cg_plan *plan, int kind, int W, const double *coef);
+
 /* Stops the next calls after a stage (testing): 0 = run to the end,
  * 1 = after binning, 2 = after gridding (ms2dirty) / plane fill (dirty2ms),
  * 3 = after the FFT. */
@@ -192,6 +208,56 @@ int cg_bin_static(int64_t nrow, int nxdirty, int nydirty, double fov, double fre
                   int *d_perm, int *d_hive_start, int64_t hive_start_len, int64_t *n_hives,
                   void *stream);
 int64_t cg_bin_static_max_rows(void);
+
+/* ---------------- learned kernel: training primitives ----------------
+ * No reference counterpart.  Device pointers, stream ordered, FP32 unless
+ * noted.  The learned kernel family is
+ *   phi(d) = exp(beta0 (sqrt(1 - t^2) - 1) + net(2 t^2 - 1)),  t = 2d/W, |t| < 1,
+ * net a 1-32-32-1 tanh MLP with cg_learn_theta_size() parameters laid out
+ * W1[32], b1[32], W2[32][32] (row = output unit), b2[32], w3[32], b3.
+ *   phi_forward:  phi[i] = phi(d[i])
+ *   phi_backward: dtheta += sum_i dphi[i] * d phi(d[i]) / d theta
+ *                 (accumulates; the caller zeroes dtheta)
+ *   spread2d:     grid[s][ix][iy] += c[s][j] phx[s][j][l] phy[s][j][m] at
+ *                 ix = gx0 + l, iy = gy0 + m mod nf (complex interleaved;
+ *                 accumulates)
+ *   spread2d_adjoint: dphx[s][j][l] = sum_m <ggrid, c> phy, dphy likewise,
+ *                 <a, b> = a.re b.re + a.im b.im
+ *   dft2 (FP64):  F[s][i] = sum_j c[s][j] exp(2 pi i (k1[s][i] X[s][j] +
+ *                 k2[s][i] Y[s][j]) / nf), the direct-sum target. */
+int cg_learn_theta_size(void);
+int cg_learn_phi_forward(const float *theta, float beta0, int W, int64_t n, const float *d,
+                         float *phi, void *stream);
+int cg_learn_phi_backward(const float *theta, float beta0, int W, int64_t n, const float *d,
+                          const float *dphi, float *dtheta, void *stream);
+int cg_learn_spread2d(int nsets, int M, int W, int nf, const float *c, const int *gx0,
+                      const int *gy0, const float *phx, const float *phy, float *grid,
+                      void *stream);
+int cg_learn_spread2d_adjoint(int nsets, int M, int W, int nf, const float *c, const int *gx0,
+                              const int *gy0, const float *phx, const float *phy,
+                              const float *ggrid, float *dphx, float *dphy, void *stream);
+int cg_learn_dft2(int nsets, int M, int nf, const double *X, const double *Y, const double *c,
+                  int nk, const int *k1, const int *k2, double *F, void *stream);
+
+/* ---------------- on-device FP64 direct DFT ----------------
+ * The exact sums that ms2dirty / dirty2ms approximate (the reference's
+ * explicit_gridder, precomp.cu:246-321, with the library's conventions:
+ * weights multiply, w enters with `sign`, n - 1 = -(l^2+m^2)/(1+n)), for
+ * error checks on large problems.  DEVICE pointers, stream ordered, FP64.
+ *   cg_explicit_ms2dirty: d_out[q] = sum_j wgt_j vis_j
+ *       exp(2 pi i f/c (u_j l + v_j m + sign w_j (n-1))) / n for pixel
+ *       d_pix[q] (flat index x*ny + y), q < npix; npix < 0: every pixel,
+ *       d_out [nx][ny].
+ *   cg_explicit_dirty2ms: d_out[q] = wgt_j sum_{x,y} dirty[x][y] / n
+ *       exp(-2 pi i f/c (...)) for row j = d_rows[q], q < nvis; nvis < 0:
+ *       every row.
+ * d_wgt may be NULL.  Outputs are overwritten; out-of-range indices give 0. */
+int cg_explicit_ms2dirty(int64_t nrow, int nxdirty, int nydirty, double fov, double freq,
+                         const double *d_uvw, const cg_c128 *d_vis, const double *d_wgt, int sign,
+                         int64_t npix, const int64_t *d_pix, cg_c128 *d_out, void *stream);
+int cg_explicit_dirty2ms(int64_t nrow, int nxdirty, int nydirty, double fov, double freq,
+                         const double *d_uvw, const cg_c128 *d_dirty, const double *d_wgt, int sign,
+                         int64_t nvis, const int64_t *d_rows, cg_c128 *d_out, void *stream);
 
 /* Host-pointer calls above keep one cached plan per precision so that
  * repeated calls reuse device workspace; this frees it. */

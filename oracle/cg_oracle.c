@@ -48,7 +48,38 @@ typedef struct {
     double i_center, i_half_width, o_center, o_half_width, gamma, h;
     int hivesize[3];         /* 8, 8, 1 (cuft.cu:253-264) */
     int nhive[3];
+    /* gridding kernel: 0 = ES (the reference's), 1 = piecewise polynomial
+     * (a learned kernel in Horner form, W segments x 8 coefficients) */
+    int kern;
+    double poly[OG_MAX_KW * 8];
 } og_params;
+
+/* kernel selected for the next og_setup (test infrastructure: not thread-safe) */
+static int og_kern_kind = 0, og_kern_w = 0;
+static double og_kern_poly[OG_MAX_KW * 8];
+
+void og_set_kernel(int kind, int W, const double *coef)
+{
+    og_kern_kind = kind;
+    og_kern_w = W;
+    if (kind == 1) memcpy(og_kern_poly, coef, sizeof(double) * 8 * W);
+}
+
+/* piecewise polynomial: segment s = floor(d + W/2) at t = 2 (d + W/2 - s) - 1 */
+static double og_poly_seg(const double *a, double t)
+{
+    double v = a[7];
+    for (int n = 6; n >= 0; n--) v = v * t + a[n];
+    return v;
+}
+
+static double og_poly_phi(const og_params *p, double d)
+{
+    double u = d + 0.5 * p->kw;
+    int s = (int)floor(u);
+    if (s < 0 || s >= p->kw) return 0.0;
+    return og_poly_seg(p->poly + 8 * s, 2.0 * (u - s) - 1.0);
+}
 
 /* ---------------------------------------------------------------- */
 /* next235beven: common_utils.cu:76-101                              */
@@ -175,6 +206,12 @@ int og_setup(og_params *p, int nrow, int nx, int ny, double fov, double freq,
     p->fov = fov; p->freq = freq; p->eps = eps; p->sigma = sigma; p->sign = sign;
     int ier = og_setup_conv_opts(eps, sigma, &p->kw, &p->beta, &p->es_c, &p->es_halfwidth, eps_floor);
     if (ier > 1) return ier;
+    if (og_kern_kind == 1) {
+        p->kern = 1;
+        p->kw = og_kern_w;
+        p->beta = 0; p->es_c = 0; p->es_halfwidth = og_kern_w / 2.0;
+        memcpy(p->poly, og_kern_poly, sizeof(double) * 8 * og_kern_w);
+    }
     p->pixelsize_x = fov / 180.0 * OG_PI / (double)p->N2;
     p->pixelsize_y = fov / 180.0 * OG_PI / (double)p->N1;
     double l_min = 0 - 0.5 * p->pixelsize_x * p->N2;
@@ -311,7 +348,9 @@ static int og_fseries_nodes(const og_params *p, double *xs, double *g)
     for (int n = 0; n < q; n++) {
         double xn = x[n] * alpha;
         double phi = 0.0;
-        if (fabs(xn) <= p->es_halfwidth)
+        if (p->kern)
+            phi = og_poly_phi(p, xn);
+        else if (fabs(xn) <= p->es_halfwidth)
             phi = exp(p->beta * (sqrt(1.0 - p->es_c * xn * xn) - 0));
         xs[n] = xn;
         g[n] = alpha * w[n] * phi;
@@ -371,6 +410,12 @@ static inline double og_phi(const og_params *p, double d)
 static inline int og_taps(const og_params *p, double X, double *k)
 {
     int x0 = (int)floor(X - p->kw / 2.0) + 1;
+    if (p->kern) {
+        /* tap i evaluates segment i at z = x0 + W/2 - X, z in (0, 1] */
+        double t = 2.0 * ((double)x0 + p->kw / 2.0 - X) - 1.0;
+        for (int i = 0; i < p->kw; i++) k[i] = og_poly_seg(p->poly + 8 * i, t);
+        return x0;
+    }
     for (int i = 0; i < p->kw; i++) k[i] = og_phi(p, (double)(x0 + i) - X);
     return x0;
 }
@@ -787,4 +832,68 @@ int og_num_threads(void)
 #else
     return 1;
 #endif
+}
+
+/* ---------------------------------------------------------------- */
+/* Learned kernel family (no reference counterpart; checker of the CUDA
+ * forward/backward kernels):
+ *   phi(d) = exp(beta0 (sqrt(1 - t^2) - 1) + net(2 t^2 - 1)), t = 2d/W, |t| < 1,
+ * net = w3 . tanh(W2 tanh(W1 x + b1) + b2) + b3, 32 hidden units per layer.
+ * theta: W1[32], b1[32], W2[32][32] (row = output unit), b2[32], w3[32], b3. */
+#define OG_H 32
+static double og_net(const double *th, double x, double *h1, double *h2)
+{
+    const double *W1 = th, *b1 = th + OG_H, *W2 = th + 2 * OG_H, *b2 = W2 + OG_H * OG_H;
+    const double *w3 = b2 + OG_H, *b3 = w3 + OG_H;
+    for (int m = 0; m < OG_H; m++) h1[m] = tanh(W1[m] * x + b1[m]);
+    double out = b3[0];
+    for (int k = 0; k < OG_H; k++) {
+        double a = b2[k];
+        for (int m = 0; m < OG_H; m++) a += W2[k * OG_H + m] * h1[m];
+        h2[k] = tanh(a);
+        out += w3[k] * h2[k];
+    }
+    return out;
+}
+
+void og_learn_phi(const double *th, double beta0, int W, int n, const double *d, double *phi)
+{
+    for (int i = 0; i < n; i++) {
+        double t = d[i] / (0.5 * W), t2 = t * t;
+        if (!(t2 < 1.0)) { phi[i] = 0.0; continue; }
+        double h1[OG_H], h2[OG_H];
+        phi[i] = exp(beta0 * (sqrt(1.0 - t2) - 1.0) + og_net(th, 2.0 * t2 - 1.0, h1, h2));
+    }
+}
+
+/* dtheta = sum_i dphi[i] * d phi(d[i]) / d theta (overwrites dtheta) */
+void og_learn_phi_grad(const double *th, double beta0, int W, int n, const double *d,
+                       const double *dphi, double *dtheta)
+{
+    const int NT = OG_H + OG_H + OG_H * OG_H + OG_H + OG_H + 1;
+    const double *W2 = th + 2 * OG_H, *w3 = W2 + OG_H * OG_H + OG_H;
+    double *gW1 = dtheta, *gb1 = dtheta + OG_H, *gW2 = dtheta + 2 * OG_H;
+    double *gb2 = gW2 + OG_H * OG_H, *gw3 = gb2 + OG_H, *gb3 = gw3 + OG_H;
+    memset(dtheta, 0, sizeof(double) * NT);
+    for (int i = 0; i < n; i++) {
+        double t = d[i] / (0.5 * W), t2 = t * t;
+        if (!(t2 < 1.0)) continue;
+        double x = 2.0 * t2 - 1.0, h1[OG_H], h2[OG_H], d2[OG_H];
+        double out = og_net(th, x, h1, h2);
+        double g = dphi[i] * exp(beta0 * (sqrt(1.0 - t2) - 1.0) + out);
+        gb3[0] += g;
+        for (int k = 0; k < OG_H; k++) {
+            gw3[k] += g * h2[k];
+            d2[k] = g * w3[k] * (1.0 - h2[k] * h2[k]);
+            gb2[k] += d2[k];
+            for (int m = 0; m < OG_H; m++) gW2[k * OG_H + m] += d2[k] * h1[m];
+        }
+        for (int m = 0; m < OG_H; m++) {
+            double a = 0;
+            for (int k = 0; k < OG_H; k++) a += d2[k] * W2[k * OG_H + m];
+            a *= 1.0 - h1[m] * h1[m];
+            gb1[m] += a;
+            gW1[m] += a * x;
+        }
+    }
 }

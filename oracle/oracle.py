@@ -37,6 +37,7 @@ class Params(ctypes.Structure):
         ("o_center", ctypes.c_double), ("o_half_width", ctypes.c_double),
         ("gamma", ctypes.c_double), ("h", ctypes.c_double),
         ("hivesize", ctypes.c_int * 3), ("nhive", ctypes.c_int * 3),
+        ("kern", ctypes.c_int), ("poly", ctypes.c_double * (16 * 8)),
     ]
 
     def as_dict(self):
@@ -84,6 +85,9 @@ def lib():
             fn.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                            D, D, D, ctypes.c_int, ctypes.c_int, I64, D]
         L.og_num_threads.restype = ctypes.c_int
+        L.og_set_kernel.argtypes = [ctypes.c_int, ctypes.c_int, D]
+        L.og_learn_phi.argtypes = [D, ctypes.c_double, ctypes.c_int, ctypes.c_int, D, D]
+        L.og_learn_phi_grad.argtypes = [D, ctypes.c_double, ctypes.c_int, ctypes.c_int, D, D, D]
         _lib = L
     return _lib
 
@@ -258,3 +262,31 @@ def dft_dirty2ms(uvw, dirty, wgt, fov, freq, sign=-1, rows=None):
 
 def num_threads():
     return lib().og_num_threads()
+
+
+# ---------------------------------------------------------------- learned kernel
+def set_kernel(kind="es", W=0, coef=None):
+    """Kernel used by every following setup / ms2dirty / dirty2ms call:
+    "es" (the reference's) or "poly" (piecewise Horner table [W, 8])."""
+    if kind == "es":
+        lib().og_set_kernel(0, 0, None)
+        return
+    a = np.ascontiguousarray(np.asarray(coef, dtype=np.float64).reshape(int(W), 8))
+    lib().og_set_kernel(1, int(W), _d(a))
+
+
+def learn_phi(theta, beta0, W, d):
+    th = _f64c(theta)
+    d = _f64c(d)
+    out = np.zeros_like(d)
+    lib().og_learn_phi(_d(th), float(beta0), int(W), d.size, _d(d), _d(out))
+    return out
+
+
+def learn_phi_grad(theta, beta0, W, d, dphi):
+    th = _f64c(theta)
+    d = _f64c(d)
+    g = _f64c(dphi)
+    out = np.zeros_like(th)
+    lib().og_learn_phi_grad(_d(th), float(beta0), int(W), d.size, _d(d), _d(g), _d(out))
+    return out
