@@ -47,7 +47,36 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--kernel", default="auto", choices=["auto", "es", "learned"],
+                    help="auto: the learned kernel at the smallest width that met epsilon in the "
+                         "committed width search, else ES")
+    ap.add_argument("--accuracy-samples", type=int, default=256,
+                    help="pixels / rows checked against the FP64 direct sums (0: skip)")
     return ap.parse_args()
+
+
+def select_kernel(args):
+    """Gridding kernel of the FP32 form: the learned kernel at the smallest W
+    that met epsilon in cugridder_b200/kernels/wsearch_2048_10M.json, else ES."""
+    from cugridder_b200.learn import available_widths, load_kernel
+    from cugridder_b200.learn.model import KERNEL_DIR
+
+    es = {"kind": "es", "W": 0, "coef": None, "label": "ES (W from epsilon)"}
+    if args.kernel == "es":
+        return es
+    p = os.path.join(KERNEL_DIR, "wsearch_2048_10M.json")
+    W = None
+    if os.path.exists(p):
+        with open(p) as f:
+            best = json.load(f).get("smallest_W", {})
+        W = (best.get("%g" % args.eps) or {}).get("learned")
+    if W is None or W not in available_widths():
+        if args.kernel == "learned":
+            raise SystemExit("no learned kernel meets eps %g" % args.eps)
+        return es
+    k = load_kernel(W)
+    return {"kind": "poly", "W": W, "coef": k.horner,
+            "label": "learned MLP kernel, W=%d, piecewise degree-7 Horner" % W}
 
 
 # --------------------------------------------------------------------------- ranks
@@ -223,7 +252,13 @@ def run_b200(args, rank, world, local):
     lib = _lib.load()
     clocks = ClockSampler(local)
 
-    def timed_run(prec, steps, warmup, sample_clocks=False, timing=False):
+    rng = np.random.Generator(np.random.PCG64(77))
+    nsamp = max(0, min(args.accuracy_samples, M, nx * ny))
+    pix = np.sort(rng.choice(nx * ny, nsamp, replace=False)).astype(np.int64)
+    rows = np.sort(rng.choice(M, nsamp, replace=False)).astype(np.int64)
+    kern = select_kernel(args)
+
+    def timed_run(prec, steps, warmup, sample_clocks=False, timing=False, kernel=None):
         cdt = torch.complex64 if prec == "fp32" else torch.complex128
         rdt = torch.float32 if prec == "fp32" else torch.float64
         vis = torch.from_numpy(d["vis"]).to(device=dev, dtype=cdt)
@@ -232,6 +267,8 @@ def run_b200(args, rank, world, local):
         dirty = torch.empty((nx, ny), dtype=cdt, device=dev)
         vout = torch.empty(M, dtype=cdt, device=dev)
         plan = Plan(nx, ny, fov, args.eps, precision=prec, stream=stream.cuda_stream)
+        if kernel is not None and kernel["kind"] == "poly":
+            plan.set_kernel("poly", kernel["W"], kernel["coef"])
 
         def step():
             plan.ms2dirty(uvw, freq, vis, wgt, dirty)
@@ -262,12 +299,16 @@ def run_b200(args, rank, world, local):
         out = {"ms": ms, "launches": launches, "info": plan.info()}
         if timing:
             out["timing"] = plan.timing()
+        if nsamp:
+            out["dirty_sub"] = dirty.reshape(-1).cpu().numpy()[pix].astype(np.complex128)
+            out["vis_sub"] = vout.cpu().numpy()[rows].astype(np.complex128)
         plan.close()
         del vis, wgt, dimg, dirty, vout
         torch.cuda.empty_cache()
         return out
 
-    main = timed_run("fp32", args.steps, args.warmup, sample_clocks=True, timing=True)
+    main = timed_run("fp32", args.steps, args.warmup, sample_clocks=True, timing=True, kernel=kern)
+    res["kernel"] = {"label": kern["label"], "W": main["info"]["kw"]}
     t_max = max_over_ranks(main["ms"], world)
     total_rows = sum_over_ranks(M, world)
     res["value"] = total_rows * args.steps / (t_max / 1e3) / 1e6
@@ -302,27 +343,69 @@ def run_b200(args, rank, world, local):
     res["clocks"] = clocks.summary()
 
     if not args.no_fp64:
-        fp = timed_run("fp64", max(2, args.steps // 3), 1)
+        fp = timed_run("fp64", max(2, args.steps // 3), args.warmup)
         t64 = max_over_ranks(fp["ms"], world)
         v64 = total_rows * max(2, args.steps // 3) / (t64 / 1e3) / 1e6
         res["fp64_plain"] = {"value": round(v64, 2), "ms_per_step": round(t64 / max(2, args.steps // 3), 3),
                              "eps": args.eps, "kw": fp["info"]["kw"], "nw": fp["info"]["nw"]}
         res["fp32_over_fp64"] = round(res["value"] / v64, 3)
 
+    if nsamp:
+        res["accuracy"] = accuracy(d, img, pix, rows, main, fp if not args.no_fp64 else None)
+
     if not args.no_e2e:
-        res["e2e"] = run_e2e(args, d, img, world)
+        res["e2e"] = run_e2e(args, d, img, world, kern)
     return res
 
 
-def run_e2e(args, d, img, world):
-    """Same metric through the public host API (cg_ms2dirty_mixed /
-    cg_dirty2ms_mixed) from pinned host buffers: every step copies its inputs
-    host->device and its outputs device->host."""
+def accuracy(d, img, pix, rows, main, fp64):
+    """Relative L2 error of each timed form against the FP64 direct sums
+    (on-device explicit gridder) on random pixel / row subsets."""
     import torch
 
     from cugridder_b200 import _lib
 
     lib = _lib.load()
+    dev = torch.device("cuda")
+    M, nx, ny = d["uvw"].shape[0], d["nx"], d["ny"]
+    st = torch.cuda.current_stream().cuda_stream
+    uvw = torch.from_numpy(d["uvw"]).to(dev)
+    vis = torch.from_numpy(d["vis"].astype(np.complex128)).to(dev)
+    wgt = torch.from_numpy(d["wgt"].astype(np.float64)).to(dev)
+    dimg = torch.from_numpy(img.astype(np.complex128)).to(dev)
+    tp, tr = torch.from_numpy(pix).to(dev), torch.from_numpy(rows).to(dev)
+    rd = torch.empty(pix.size, dtype=torch.complex128, device=dev)
+    rv = torch.empty(rows.size, dtype=torch.complex128, device=dev)
+    _lib.check(lib.cg_explicit_ms2dirty(M, nx, ny, d["fov"], d["freq"], uvw.data_ptr(), vis.data_ptr(),
+                                        wgt.data_ptr(), -1, pix.size, tp.data_ptr(), rd.data_ptr(), st))
+    _lib.check(lib.cg_explicit_dirty2ms(M, nx, ny, d["fov"], d["freq"], uvw.data_ptr(), dimg.data_ptr(),
+                                        wgt.data_ptr(), -1, rows.size, tr.data_ptr(), rv.data_ptr(), st))
+    torch.cuda.synchronize()
+    ref_d, ref_v = rd.cpu().numpy(), rv.cpu().numpy()
+
+    def err(r):
+        return {"ms2dirty_rel_l2": float(np.linalg.norm(r["dirty_sub"] - ref_d) / np.linalg.norm(ref_d)),
+                "dirty2ms_rel_l2": float(np.linalg.norm(r["vis_sub"] - ref_v) / np.linalg.norm(ref_v))}
+
+    out = {"reference": "FP64 direct sums on the device (cg_explicit_*) on %d pixels / %d rows"
+                        % (pix.size, rows.size), "value_form": err(main)}
+    if fp64 is not None:
+        out["fp64_plain"] = err(fp64)
+    return out
+
+
+def run_e2e(args, d, img, world, kern):
+    """Same metric through the public host API (cg_ms2dirty_mixed /
+    cg_dirty2ms_mixed, with the same gridding kernel selected by
+    cg_set_host_kernel) from pinned host buffers: every step copies its inputs
+    host->device and its outputs device->host."""
+    import torch
+
+    from cugridder_b200 import _lib, set_host_kernel
+
+    lib = _lib.load()
+    if kern["kind"] == "poly":
+        set_host_kernel("poly", kern["W"], kern["coef"])
     M = d["uvw"].shape[0]
     nx, ny = d["nx"], d["ny"]
 
@@ -359,6 +442,7 @@ def run_e2e(args, d, img, world):
     t = max_over_ranks(e0.elapsed_time(e1), world)
     total_rows = sum_over_ranks(M, world)
     lib.cg_release_cache()
+    set_host_kernel("es")
     h2d = 2 * uvw.nbytes + vis.nbytes + 2 * wgt.nbytes + dimg.nbytes
     d2h = dirty.nbytes + vout.nbytes
     return {"value": round(total_rows * args.e2e_steps / (t / 1e3) / 1e6, 2), "unit": "Mvis/s",
@@ -471,12 +555,13 @@ def main():
             "dtype": "f32 (fp64 uvw/coordinates)", "data": "synthetic",
             "config": {"workload": args.config, "nx": cfg["nx"], "ny": cfg["ny"], "fov_deg": cfg["fov"],
                        "nrow_per_gpu": args.nrow or cfg["nrow"], "freq_hz": cfg["freq"], "eps": args.eps,
-                       "kernel": "ES", "W": info["kw"], "nw": info["nw"], "grid": [info["nf1"], info["nf2"]],
+                       "kernel": res["kernel"]["label"], "W": info["kw"], "nw": info["nw"], "grid": [info["nf1"], info["nf2"]],
                        "parallelism": "independent datasets per GPU" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (uvw 480 MB, grid 7.5 GB)"},
             "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res.get("e2e"),
             "gpu_launches": res["gpu_launches"], "clocks": res["clocks"],
             "fp64_plain": res.get("fp64_plain"), "fp32_over_fp64": res.get("fp32_over_fp64"),
+            "accuracy": res.get("accuracy"),
             "stages": res["stages"],
         }
         print(json.dumps(line), flush=True)

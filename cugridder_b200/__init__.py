@@ -20,7 +20,7 @@ __all__ = [
     "ms2dirty", "dirty2ms", "vis2dirty", "dirty2vis", "Plan", "GridderError",
     "ms2dirty_1", "ms2dirty_2", "dirty2ms_1", "dirty2ms_2",
     "ms2dirtyf_1", "ms2dirtyf_2", "dirty2msf_1", "dirty2msf_2",
-    "ms2dirty_mixed", "dirty2ms_mixed", "release_cache",
+    "ms2dirty_mixed", "dirty2ms_mixed", "release_cache", "set_host_kernel",
 ]
 
 
@@ -59,3 +59,17 @@ def dirty2ms_mixed(uvw, freq, dirty, wgt, fov_deg, epsilon, sigma=2.0, sign=-1):
 def release_cache():
     """Free the device workspace cached by the host-pointer entry points."""
     _lib.check(_lib.load().cg_release_cache())
+
+
+def set_host_kernel(kind="es", W=0, coef=None):
+    """Gridding kernel of the host-pointer entry points (the reference-named
+    functions and *_mixed): "es" (W = 0: from epsilon, the reference's choice)
+    or "poly" with a [W, 8] Horner table, e.g. a learned kernel."""
+    import numpy as np
+
+    lib = _lib.load()
+    if kind == "es":
+        _lib.check(lib.cg_set_host_kernel(_lib.CG_KERNEL_ES, int(W or 0), None))
+        return
+    a = np.ascontiguousarray(np.asarray(coef, dtype=np.float64).reshape(int(W), 8))
+    _lib.check(lib.cg_set_host_kernel(_lib.CG_KERNEL_POLY, int(W), a.ctypes.data))

@@ -88,6 +88,7 @@ SIGNATURES = {
                               c_int, c_int, _PTR, _PTR, c_int64, ctypes.POINTER(c_int64), c_void_p]),
     "cg_bin_static_max_rows": (c_int64, []),
     "cg_plan_set_kernel": (c_int, [c_void_p, c_int, c_int, _PTR]),
+    "cg_set_host_kernel": (c_int, [c_int, c_int, _PTR]),
     "cg_learn_theta_size": (c_int, []),
     "cg_learn_phi_forward": (c_int, [_PTR, c_float, c_int, c_int64, _PTR, _PTR, c_void_p]),
     "cg_learn_phi_backward": (c_int, [_PTR, c_float, c_int, c_int64, _PTR, _PTR, _PTR, c_void_p]),

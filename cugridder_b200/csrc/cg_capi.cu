@@ -32,6 +32,32 @@ namespace {
 std::mutex g_cache_mu;
 cg_plan_s* g_cache[2] = {nullptr, nullptr};
 
+// gridding kernel of the host-pointer entry points (cg_set_host_kernel)
+struct HostKernel {
+  int kind = CG_KERNEL_ES;
+  int w = 0;  // ES: forced width (0 = from epsilon); POLY: width
+  double poly[cg::kMaxW * cg::kPolyCoef] = {};
+} g_host_kernel;
+
+// bring a cached plan's kernel in line with g_host_kernel (caller holds g_cache_mu)
+void apply_host_kernel(cg_plan_s* P) {
+  const HostKernel& k = g_host_kernel;
+  const bool poly = k.kind == CG_KERNEL_POLY;
+  const bool same = P->kernel_kind == k.kind &&
+                    (poly ? (P->poly_w == k.w &&
+                             memcmp(P->poly, k.poly, sizeof(double) * k.w * cg::kPolyCoef) == 0)
+                          : P->es_w == k.w);
+  if (same) return;
+  P->kernel_kind = k.kind;
+  if (poly) {
+    P->poly_w = k.w;
+    memcpy(P->poly, k.poly, sizeof(k.poly));
+  } else {
+    P->es_w = k.w;
+  }
+  P->kw = 0;  // reconfigure on the next plan_configure
+}
+
 int ensure_device() {
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
@@ -97,6 +123,7 @@ int host_call(bool to_dirty, int precision, int64_t nrow, int nx, int ny, double
   cg_plan_s* P = cached_plan(precision, st);
   if (!P) return st;
   CG_CUDA(cudaSetDevice(P->device));
+  apply_host_kernel(P);
   CG_TRY(cg::plan_configure(P, nx, ny, fov, eps, sigma, sign, precision));
   size_t tsz = precision == CG_PREC_FP64 ? 8 : 4;
   size_t n_uvw = (size_t)nrow * 3;
@@ -305,6 +332,21 @@ int cg_plan_set_kernel(cg_plan* plan, int kind, int W, const double* coef) {
   int st = cg::plan_configure(plan, plan->nx, plan->ny, plan->fov, plan->eps, plan->sigma,
                               plan->sign, plan->precision);
   return st > 1 ? st : CG_OK;
+}
+
+int cg_set_host_kernel(int kind, int W, const double* coef) {
+  if (kind != CG_KERNEL_ES && kind != CG_KERNEL_POLY) return CG_ERR_ARG;
+  if (kind == CG_KERNEL_POLY && (W < 2 || W > cg::kMaxW || !coef)) return CG_ERR_ARG;
+  if (kind == CG_KERNEL_ES && W != 0 && (W < 2 || W > cg::kMaxW)) return CG_ERR_ARG;
+  if (kind == CG_KERNEL_POLY)
+    for (int i = 0; i < W * cg::kPolyCoef; i++)
+      if (!std::isfinite(coef[i])) return CG_ERR_ARG;
+  std::lock_guard<std::mutex> lock(g_cache_mu);
+  g_host_kernel = HostKernel();
+  g_host_kernel.kind = kind;
+  g_host_kernel.w = W;
+  if (kind == CG_KERNEL_POLY) memcpy(g_host_kernel.poly, coef, sizeof(double) * W * cg::kPolyCoef);
+  return CG_OK;
 }
 
 int cg_plan_set_stop_stage(cg_plan* plan, int stage) {

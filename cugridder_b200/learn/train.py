@@ -188,7 +188,7 @@ class Problem:
         return ((fk - F).abs() ** 2).sum(1) / (F.abs() ** 2).sum(1)
 
 
-def train_one(torch, W, nsets=4096, nvis=10000, n=512, K=64, batch=16, epochs=4, lr=3e-3,
+def train_one(torch, W, nsets=4096, nvis=10000, n=512, K=64, batch=16, epochs=16, lr=3e-3,
               seed=0, log=print):
     t0 = time.time()
     sets = Sets(torch, nsets, nvis, n, K, seed=1000 + W, device="cuda")
@@ -257,11 +257,11 @@ def train_one(torch, W, nsets=4096, nvis=10000, n=512, K=64, batch=16, epochs=4,
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--W", type=int, nargs="+", default=[4, 5, 6, 7])
+    ap.add_argument("--W", type=int, nargs="+", default=[4, 5, 6, 7, 8])
     ap.add_argument("--sets", type=int, default=4096)
     ap.add_argument("--nvis", type=int, default=10000)
     ap.add_argument("--n", type=int, default=512)
-    ap.add_argument("--epochs", type=int, default=4)
+    ap.add_argument("--epochs", type=int, default=16)
     ap.add_argument("--batch", type=int, default=16)
     ap.add_argument("--lr", type=float, default=3e-3)
     ap.add_argument("--out", default=None, help="directory (default: the package's kernels/)")

@@ -173,6 +173,12 @@ int cg_plan_set_method(cg_plan *plan, int method);
 #define CG_KERNEL_POLY 1
 int cg_plan_set_kernel(cg_plan *plan, int kind, int W, const double *coef);
 
+/* The same choice for the host-pointer entry points (the eight reference
+ * functions and cg_*_mixed), process-wide: their cached plans switch kernel
+ * on their next call.  Default: CG_KERNEL_ES with W from epsilon, the
+ * reference's behaviour.  No reference counterpart. */
+int cg_set_host_kernel(int kind, int W, const double *coef);
+
 /* Stops the next calls after a stage (testing): 0 = run to the end,
  * 1 = after binning, 2 = after gridding (ms2dirty) / plane fill (dirty2ms),
  * 3 = after the FFT. */

@@ -192,3 +192,63 @@ def test_learned_kernels_gain_over_es(torch_cuda, oracle):
             errs[name] = (rel_l2(dirty.reshape(-1)[pix], dft), rel_l2(vis[rows], dft_v))
         assert errs["learned"][0] < errs["es"][0], (W, errs)
         assert errs["learned"][1] < errs["es"][1], (W, errs)
+
+
+# ---------------------------------------------------------------- on-device DFT
+def test_explicit_dft_vs_oracle(torch_cuda, oracle):
+    """The on-device FP64 direct sums equal the oracle's CPU direct DFT
+    (pixel subset and full image for ms2dirty, row subset for dirty2ms)."""
+    torch = torch_cuda
+    lib = _lib.load()
+    d = synth.make("ms2dirty_256_fp64", seed=8, nrow=3001, nx=48, ny=40, fov=2.0)
+    nx, ny = 48, 40
+    img = synth.random_image(nx, ny, seed=4)
+    rng = np.random.Generator(np.random.PCG64(9))
+    pix = rng.choice(nx * ny, 101, replace=False).astype(np.int64)
+    rows = rng.choice(3001, 77, replace=False).astype(np.int64)
+    uvw = to_dev(torch, d["uvw"], np.float64)
+    vis = to_dev(torch, d["vis"], np.complex128)
+    wgt = to_dev(torch, d["wgt"], np.float64)
+    dimg = to_dev(torch, img, np.complex128)
+    for sign in (-1, 1):
+        out = torch.empty(101, dtype=torch.complex128, device="cuda")
+        pd = to_dev(torch, pix)
+        _lib.check(lib.cg_explicit_ms2dirty(3001, nx, ny, d["fov"], d["freq"], uvw.data_ptr(),
+                                            vis.data_ptr(), wgt.data_ptr(), sign, 101, pd.data_ptr(),
+                                            out.data_ptr(), _stream(torch)))
+        ref = oracle.dft_ms2dirty(d["uvw"], d["vis"], d["wgt"], nx, ny, d["fov"], d["freq"],
+                                  sign=sign, pixels=pix)
+        assert rel_l2(out.cpu().numpy(), ref) < 1e-12
+        full = torch.empty((nx, ny), dtype=torch.complex128, device="cuda")
+        _lib.check(lib.cg_explicit_ms2dirty(3001, nx, ny, d["fov"], d["freq"], uvw.data_ptr(),
+                                            vis.data_ptr(), None, sign, -1, None, full.data_ptr(),
+                                            _stream(torch)))
+        ref_full = oracle.dft_ms2dirty(d["uvw"], d["vis"], None, nx, ny, d["fov"], d["freq"], sign=sign)
+        assert rel_l2(full.cpu().numpy(), ref_full.reshape(nx, ny)) < 1e-12
+        vout = torch.empty(77, dtype=torch.complex128, device="cuda")
+        rd = to_dev(torch, rows)
+        _lib.check(lib.cg_explicit_dirty2ms(3001, nx, ny, d["fov"], d["freq"], uvw.data_ptr(),
+                                            dimg.data_ptr(), wgt.data_ptr(), sign, 77, rd.data_ptr(),
+                                            vout.data_ptr(), _stream(torch)))
+        ref_v = oracle.dft_dirty2ms(d["uvw"], img, d["wgt"], d["fov"], d["freq"], sign=sign, rows=rows)
+        assert rel_l2(vout.cpu().numpy(), ref_v) < 1e-12
+
+
+def test_es_forced_width_matches_epsilon_choice(torch_cuda):
+    """ES forced to the width that epsilon would pick reproduces the default."""
+    torch = torch_cuda
+    d = synth.make("ms2dirty_256_fp64", seed=12, nrow=5000, nx=64, ny=64)
+    outs = []
+    for force in (False, True):
+        plan = Plan(64, 64, d["fov"], 1e-5, precision="fp64")
+        if force:
+            plan.set_kernel("es", 6)
+        uvw = to_dev(torch, d["uvw"], np.float64)
+        vis = to_dev(torch, d["vis"], np.complex128)
+        out = torch.zeros((64, 64), dtype=torch.complex128, device="cuda")
+        plan.ms2dirty(uvw, d["freq"], vis, None, out)
+        torch.cuda.synchronize()
+        assert plan.info()["kw"] == 6
+        outs.append(out.cpu().numpy())
+        plan.close()
+    assert np.array_equal(outs[0], outs[1])
