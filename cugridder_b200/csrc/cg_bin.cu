@@ -147,21 +147,31 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_upsweep(const K* __restrict__
   counts[(int64_t)threadIdx.x * ntiles + blockIdx.x] = hist[threadIdx.x];
 }
 
+__device__ __forceinline__ int block_excl_scan(int x, int* s_warp, int& total);
+
 // Tile layout: warp w owns rows [w*512, w*512+512) of the tile, item i of
 // lane l is row w*512 + i*32 + l; items are ranked in (w, i, l) order, which
-// is the row order, so the pass is stable.
+// is the row order, so the pass is stable.  The ranked tile is first
+// reordered in shared memory by digit, then written out with consecutive
+// threads on consecutive positions of each digit's run (coalesced stores).
 template <typename K>
 __global__ void __launch_bounds__(kRsThreads) k_rs_downsweep(
     const K* __restrict__ keys_in, const int* __restrict__ vals_in, K* __restrict__ keys_out,
     int* __restrict__ vals_out, int64_t M, int shift, int ntiles, const int* __restrict__ offsets) {
-  __shared__ int whist[8][256];
-  __shared__ int wpref[8][256];
+  extern __shared__ __align__(16) unsigned char rs_smem[];
+  K* skey = reinterpret_cast<K*>(rs_smem);                       // [kRsTile]
+  int* sval = reinterpret_cast<int*>(skey + kRsTile);            // [kRsTile]
+  int (*whist)[256] = reinterpret_cast<int (*)[256]>(sval + kRsTile);  // [8][256]
+  int (*wpref)[256] = whist + 8;                                  // [8][256]
+  int* dstart = &wpref[8][0];                                     // [256]
+  int* s_warp = dstart + 256;                                     // [33]
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int d = threadIdx.x; d < 8 * 256; d += kRsThreads) (&whist[0][0])[d] = 0;
   __syncthreads();
   K k[kRsItems];
   int v[kRsItems], r[kRsItems], dg[kRsItems];
-  int64_t base = (int64_t)blockIdx.x * kRsTile + warp * (kRsTile / 8);
+  const int64_t tile0 = (int64_t)blockIdx.x * kRsTile;
+  int64_t base = tile0 + warp * (kRsTile / 8);
   unsigned lt = (1u << lane) - 1u;
 #pragma unroll
   for (int i = 0; i < kRsItems; i++) {
@@ -179,6 +189,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_downsweep(
     dg[i] = d;
   }
   __syncthreads();
+  int total;
   {
     int d = threadIdx.x, run = 0;
 #pragma unroll
@@ -186,16 +197,30 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_downsweep(
       wpref[w][d] = run;
       run += whist[w][d];
     }
+    dstart[d] = block_excl_scan(run, s_warp, total);  // tile-local start of digit d
   }
   __syncthreads();
 #pragma unroll
   for (int i = 0; i < kRsItems; i++) {
     if (dg[i] < 256) {
-      int64_t pos = (int64_t)offsets[(int64_t)dg[i] * ntiles + blockIdx.x] + wpref[warp][dg[i]] + r[i];
-      keys_out[pos] = k[i];
-      vals_out[pos] = v[i];
+      const int p = dstart[dg[i]] + wpref[warp][dg[i]] + r[i];
+      skey[p] = k[i];
+      sval[p] = v[i];
     }
   }
+  __syncthreads();
+  for (int p = threadIdx.x; p < total; p += kRsThreads) {
+    const K key = skey[p];
+    const int d = (int)((key >> shift) & 0xFF);
+    const int64_t pos = (int64_t)offsets[(int64_t)d * ntiles + blockIdx.x] + (p - dstart[d]);
+    keys_out[pos] = key;
+    vals_out[pos] = sval[p];
+  }
+}
+
+template <typename K>
+constexpr size_t rs_down_smem() {
+  return (size_t)kRsTile * (sizeof(K) + 4) + (8 * 256 * 2 + 256 + 33) * 4;
 }
 
 // ---------------------------------------------------------------- scan
@@ -288,18 +313,39 @@ static int scan_exclusive(const int* d_in, int64_t n, int* d_out, int* d_sums, c
 }
 
 // ---------------------------------------------------------------- hive offsets
+// hive_start[h] = first sorted row whose key >= 64 h, for h = 0..nh.  Each
+// thread runs kHsIlp independent lower-bound searches in lockstep (hives
+// h0 + j * stride) so their dependent loads overlap.
+constexpr int kHsIlp = 8;
 template <typename K>
 __global__ void k_hive_start(const K* __restrict__ skeys, int64_t M, int64_t nh,
                              int* __restrict__ hive_start) {
-  for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h <= nh;
-       h += (int64_t)gridDim.x * blockDim.x) {
-    unsigned long long target = (unsigned long long)h * 64ULL;
-    int64_t lo = 0, hi = M;
-    while (lo < hi) {
-      int64_t mid = (lo + hi) >> 1;
-      if ((unsigned long long)skeys[mid] < target) lo = mid + 1; else hi = mid;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t h0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h0 <= nh;
+       h0 += stride * kHsIlp) {
+    unsigned long long target[kHsIlp];
+    int64_t lo[kHsIlp], hi[kHsIlp];
+#pragma unroll
+    for (int j = 0; j < kHsIlp; j++) {
+      target[j] = (unsigned long long)(h0 + j * stride) * 64ULL;
+      lo[j] = 0;
+      hi[j] = M;
     }
-    hive_start[h] = (int)lo;
+    bool busy = true;
+    while (busy) {
+      busy = false;
+#pragma unroll
+      for (int j = 0; j < kHsIlp; j++) {
+        if (lo[j] < hi[j]) {
+          const int64_t mid = (lo[j] + hi[j]) >> 1;
+          if ((unsigned long long)skeys[mid] < target[j]) lo[j] = mid + 1; else hi[j] = mid;
+          busy |= lo[j] < hi[j];
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kHsIlp; j++)
+      if (h0 + j * stride <= nh) hive_start[h0 + j * stride] = (int)lo[j];
   }
 }
 
@@ -342,14 +388,16 @@ static int bin_impl(const double* d_uvw, int64_t M, const Geom& g, void* d_ws, i
     k_keys<K><<<blocks, 256, 0, st>>>(d_uvw, M, g, ka, va);
   count_launches(1);
     CG_CUDA(cudaGetLastError());
+    CG_CUDA(cudaFuncSetAttribute(k_rs_downsweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)rs_down_smem<K>()));
     K* kin = ka; int* vin = va; K* kout = kb; int* vout = vb;
     for (int ps = 0; ps < passes; ps++) {
       int shift = 8 * ps;
       k_rs_upsweep<K><<<(int)ntiles, kRsThreads, 0, st>>>(kin, M, shift, (int)ntiles, counts);
       count_launches(1);
       CG_TRY(scan_exclusive(counts, ncount, offs, sums, st));
-      k_rs_downsweep<K><<<(int)ntiles, kRsThreads, 0, st>>>(kin, vin, kout, vout, M, shift,
-                                                             (int)ntiles, offs);
+      k_rs_downsweep<K><<<(int)ntiles, kRsThreads, rs_down_smem<K>(), st>>>(
+          kin, vin, kout, vout, M, shift, (int)ntiles, offs);
       count_launches(1);
       CG_CUDA(cudaGetLastError());
       K* tk = kin; kin = kout; kout = tk;
@@ -358,8 +406,8 @@ static int bin_impl(const double* d_uvw, int64_t M, const Geom& g, void* d_ws, i
     if (vin != d_perm) CG_CUDA(cudaMemcpyAsync(d_perm, vin, (size_t)M * 4, cudaMemcpyDeviceToDevice, st));
     CG_CUDA(cudaMemcpyAsync(d_sorted_keys, kin, (size_t)M * sizeof(K), cudaMemcpyDeviceToDevice, st));
   }
-  int hb = (int)((nh + 1 + 255) / 256);
-  if (hb > 148 * 32) hb = 148 * 32;
+  int hb = (int)((nh + 1 + 256 * kHsIlp - 1) / (256 * kHsIlp));
+  if (hb > 148 * 8) hb = 148 * 8;
   k_hive_start<K><<<hb, 256, 0, st>>>(d_sorted_keys, M, nh, d_hive_start);
   count_launches(1);
   CG_CUDA(cudaGetLastError());
@@ -381,62 +429,83 @@ int launch_bin(const double* d_uvw, int64_t M, const Geom& g, int key_bytes, voi
 //   gridding:   c = vis * wgt * exp(+i o_c w)   (ra_exec.cu:103-111; pre_stage_1 cuft.cu:46-66)
 //   degridding: factor = wgt * exp(-i o_c w)    (cura_fw ra_exec.cu:75-93; shift_corr :55-66)
 template <typename T, bool kGrid>
-__global__ void k_build_stream(const int* __restrict__ perm, int64_t M,
-                               const double* __restrict__ uvw, const T* __restrict__ vis,
-                               const T* __restrict__ wgt, Geom g, Rec<T>* __restrict__ recs) {
+__device__ __forceinline__ Rec<T> make_rec(int64_t i, const double* __restrict__ uvw,
+                                           const T* __restrict__ vis, const T* __restrict__ wgt,
+                                           const Geom& g) {
+  double X0, X1, X2, w;
+  grid_coords(uvw + 3 * i, g, X0, X1, X2, w);
+  double fb0 = floor(X0), fb1 = floor(X1), fb2 = floor(X2);
+  Rec<T> r;
+  r.f[0] = (T)(X0 - fb0);
+  r.f[1] = (T)(X1 - fb1);
+  r.f[2] = (T)(X2 - fb2);
+  // guard against a fraction rounding up to 1 in the working precision
+  const T below1 = sizeof(T) == 4 ? (T)0.99999994f : (T)0.99999999999999989;
+  if (r.f[0] >= (T)1) r.f[0] = below1;
+  if (r.f[1] >= (T)1) r.f[1] = below1;
+  if (r.f[2] >= (T)1) r.f[2] = below1;
+  r.bxy = (uint32_t)(int)fb0 | ((uint32_t)(int)fb1 << 16);
+  r.bz = (uint32_t)(int)fb2;
+  double sn, cs;
+  sincos(g.o_center * w * (kGrid ? 1.0 : -1.0), &sn, &cs);
+  double wt = wgt ? (double)wgt[i] : 1.0;
+  if (kGrid) {
+    double cr = (double)vis[2 * i] * wt, ci = (double)vis[2 * i + 1] * wt;
+    r.c[0] = (T)(cr * cs - ci * sn);
+    r.c[1] = (T)(cr * sn + ci * cs);
+  } else {
+    r.c[0] = (T)(wt * cs);
+    r.c[1] = (T)(wt * sn);
+  }
+  return r;
+}
+
+// records in the original row order (coalesced reads of uvw / vis / wgt)
+template <typename T, bool kGrid>
+__global__ void k_build_rows(int64_t M, const double* __restrict__ uvw, const T* __restrict__ vis,
+                             const T* __restrict__ wgt, Geom g, Rec<T>* __restrict__ tmp) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M;
+       i += (int64_t)gridDim.x * blockDim.x)
+    tmp[i] = make_rec<T, kGrid>(i, uvw, vis, wgt, g);
+}
+
+// sorted stream: recs[s] = tmp[perm[s]], one aligned record per gather
+template <typename T>
+__global__ void k_gather_recs(const int* __restrict__ perm, int64_t M, const Rec<T>* __restrict__ tmp,
+                              Rec<T>* __restrict__ recs) {
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < M;
        s += (int64_t)gridDim.x * blockDim.x) {
-    int64_t i = perm[s];
+    const int64_t i = perm[s];
     if (i < 0 || i >= M) continue;  // never taken for a valid permutation; no wild reads
-    double X0, X1, X2, w;
-    grid_coords(uvw + 3 * i, g, X0, X1, X2, w);
-    double fb0 = floor(X0), fb1 = floor(X1), fb2 = floor(X2);
-    Rec<T> r;
-    r.f[0] = (T)(X0 - fb0);
-    r.f[1] = (T)(X1 - fb1);
-    r.f[2] = (T)(X2 - fb2);
-    // guard against a fraction rounding up to 1 in the working precision
-    const T below1 = sizeof(T) == 4 ? (T)0.99999994f : (T)0.99999999999999989;
-    if (r.f[0] >= (T)1) r.f[0] = below1;
-    if (r.f[1] >= (T)1) r.f[1] = below1;
-    if (r.f[2] >= (T)1) r.f[2] = below1;
-    r.bxy = (uint32_t)(int)fb0 | ((uint32_t)(int)fb1 << 16);
-    r.bz = (uint32_t)(int)fb2;
-    double sn, cs;
-    sincos(g.o_center * w * (kGrid ? 1.0 : -1.0), &sn, &cs);
-    double wt = wgt ? (double)wgt[i] : 1.0;
-    if (kGrid) {
-      double cr = (double)vis[2 * i] * wt, ci = (double)vis[2 * i + 1] * wt;
-      r.c[0] = (T)(cr * cs - ci * sn);
-      r.c[1] = (T)(cr * sn + ci * cs);
-    } else {
-      r.c[0] = (T)(wt * cs);
-      r.c[1] = (T)(wt * sn);
-    }
-    recs[s] = r;
+    recs[s] = tmp[i];
   }
 }
 
+// The records are built in row order into d_tmp (M records) and gathered by
+// the sort permutation: random 24/8/4-byte reads of uvw/vis/wgt would each
+// pull whole DRAM sectors, a 32-byte record gather pulls one.
 template <typename T>
 int launch_build_stream(const int* d_perm, int64_t M, const double* d_uvw, const T* d_vis,
-                        const T* d_wgt, const Geom& g, bool grid_dir, Rec<T>* d_recs,
-                        cudaStream_t st) {
+                        const T* d_wgt, const Geom& g, bool grid_dir, Rec<T>* d_tmp,
+                        Rec<T>* d_recs, cudaStream_t st) {
   if (M == 0) return CG_OK;
   int blocks = (int)((M + 255) / 256);
   if (blocks > 148 * 32) blocks = 148 * 32;
   if (grid_dir)
-    k_build_stream<T, true><<<blocks, 256, 0, st>>>(d_perm, M, d_uvw, d_vis, d_wgt, g, d_recs);
+    k_build_rows<T, true><<<blocks, 256, 0, st>>>(M, d_uvw, d_vis, d_wgt, g, d_tmp);
   else
-    k_build_stream<T, false><<<blocks, 256, 0, st>>>(d_perm, M, d_uvw, d_vis, d_wgt, g, d_recs);
-  count_launches(1);
+    k_build_rows<T, false><<<blocks, 256, 0, st>>>(M, d_uvw, d_vis, d_wgt, g, d_tmp);
+  k_gather_recs<T><<<blocks, 256, 0, st>>>(d_perm, M, d_tmp, d_recs);
+  count_launches(2);
   CG_CUDA(cudaGetLastError());
   return CG_OK;
 }
 
 template int launch_build_stream<float>(const int*, int64_t, const double*, const float*,
-                                        const float*, const Geom&, bool, Rec<float>*, cudaStream_t);
+                                        const float*, const Geom&, bool, Rec<float>*, Rec<float>*,
+                                        cudaStream_t);
 template int launch_build_stream<double>(const int*, int64_t, const double*, const double*,
                                          const double*, const Geom&, bool, Rec<double>*,
-                                         cudaStream_t);
+                                         Rec<double>*, cudaStream_t);
 
 }  // namespace cg

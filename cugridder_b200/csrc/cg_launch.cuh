@@ -19,8 +19,8 @@ int launch_bin(const double* d_uvw, int64_t M, const Geom& g, int key_bytes, voi
 
 template <typename T>
 int launch_build_stream(const int* d_perm, int64_t M, const double* d_uvw, const T* d_vis,
-                        const T* d_wgt, const Geom& g, bool grid_dir, Rec<T>* d_recs,
-                        cudaStream_t st);
+                        const T* d_wgt, const Geom& g, bool grid_dir, Rec<T>* d_tmp,
+                        Rec<T>* d_recs, cudaStream_t st);
 
 // ---- spreading / interpolation (cg_spread.cu) ----
 // method 0: direct (global atomics / global gathers); 1: tiled (shared memory).

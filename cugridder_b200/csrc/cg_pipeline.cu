@@ -183,7 +183,7 @@ void release(cg_dev_buf& b) {
 
 size_t workspace_bytes(const cg_plan_s* P) {
   const cg_dev_buf* bs[] = {&P->mm,   &P->K1,    &P->K2,         &P->K3q,   &P->zq,
-                            &P->grid, &P->recs,  &P->perm,       &P->skeys, &P->hive_start,
+                            &P->grid, &P->recs,  &P->recs_tmp, &P->perm,       &P->skeys, &P->hive_start,
                             &P->binws, &P->fftwork, &P->io_uvw, &P->io_vis, &P->io_wgt,
                             &P->io_dirty};
   size_t s = 0;
@@ -399,6 +399,7 @@ static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw)
   CG_TRY(ensure(P->skeys, (size_t)nrow * P->key_bytes));
   CG_TRY(ensure(P->binws, bin_workspace_bytes(nrow, P->key_bytes)));
   CG_TRY(ensure(P->recs, (size_t)nrow * (tsz == 8 ? sizeof(Rec<double>) : sizeof(Rec<float>))));
+  CG_TRY(ensure(P->recs_tmp, (size_t)nrow * (tsz == 8 ? sizeof(Rec<double>) : sizeof(Rec<float>))));
   return CG_OK;
 }
 
@@ -540,7 +541,7 @@ static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T
   timer_mark(P);  // 2: binning
   if (P->stop_stage == 1) return CG_OK;
   CG_TRY(launch_build_stream<T>((const int*)P->perm.p, M, d_uvw, d_vis, d_wgt, g, true,
-                                (Rec<T>*)P->recs.p, st));
+                                (Rec<T>*)P->recs_tmp.p, (Rec<T>*)P->recs.p, st));
   timer_mark(P);  // 3: sorted stream
   CG_TRY(launch_grid<T>((const Rec<T>*)P->recs.p, (const int*)P->hive_start.p, M, g,
                         (T*)P->grid.p, P->grid_method, queue_counter(P), st));
@@ -577,7 +578,7 @@ static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const
   timer_mark(P);  // 4: FFT
   if (P->stop_stage == 3) return CG_OK;
   CG_TRY(launch_build_stream<T>((const int*)P->perm.p, M, d_uvw, (const T*)nullptr, d_wgt, g,
-                                false, (Rec<T>*)P->recs.p, st));
+                                false, (Rec<T>*)P->recs_tmp.p, (Rec<T>*)P->recs.p, st));
   timer_mark(P);  // 5: sorted stream
   CG_TRY(launch_degrid<T>((const Rec<T>*)P->recs.p, (const int*)P->perm.p,
                           (const int*)P->hive_start.p, M, g, (const T*)P->grid.p, d_vis,

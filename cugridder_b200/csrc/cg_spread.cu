@@ -335,6 +335,13 @@ __global__ void __launch_bounds__(256) k_grid_warp(const Rec<T>* __restrict__ re
   constexpr int lo = Halo<W>::lo, hi = Halo<W>::hi;
   constexpr int NP = W * W;                 // (dy, dz) tap pairs
   constexpr int NR = (NP + 31) / 32;        // rounds of pairs
+  // The last, partly filled round of pairs leaves lanes idle for all W x
+  // steps (W = 6: 4 of 36 pairs, 28 lanes idle).  When it is cheaper, those
+  // REM pairs' REM * W taps are instead spread one tap per lane ("tail").
+  constexpr int NFULL = NP / 32, REM = NP % 32;
+  constexpr int NTAIL = (REM * W + 31) / 32;
+  constexpr bool kTail = REM > 0 && 12 * NTAIL < 12 + 5 * W;
+  constexpr int NRR = kTail ? NFULL : NR;  // rounds walked pair by pair
   constexpr int NKV = (3 * W + 31) / 32;    // kernel-value registers per lane
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int TX = tc.TX, TY = tc.TY, PB = tc.PB, RS = tc.RS, PS = tc.PS;
@@ -380,44 +387,70 @@ __global__ void __launch_bounds__(256) k_grid_warp(const Rec<T>* __restrict__ re
     }
     for (int i = lane; i < PB * PS; i += 32) acc[i] = zero;
     __syncwarp();
-    for (int q0 = 0; q0 < total; q0 += 32) {
-      // pre-scan: each lane loads one candidate row and tests its overlap
-      const int q = q0 + lane;
-      bool take = false;
-      T f0 = 0, f1 = 0, f2 = 0, c0 = 0, c1 = 0;
-      int ox = 0, oy = 0, oz = 0;
-      if (q < total) {
+    // Candidates are pre-scanned 32 at a time (one per lane); the next
+    // chunk's records are loaded while the current chunk is spread.  Within a
+    // chunk, the next row's broadcast and kernel values are computed before
+    // the current row's shared-memory updates, so the two overlap.
+    struct Cand {
+      T f0, f1, f2, c0, c1;
+      int bx, by, bz;  // cell + periodic shift of the hive slot
+      bool ok;
+    };
+    auto load_cand = [&](int q) {
+      Cand cd{};
+      cd.ok = q < total;
+      if (cd.ok) {
         const int sgi = find_segment(t.pref, nslots, q);
         const Rec<T> r = recs[t.start[sgi] + (q - t.pref[sgi])];
-        f0 = r.f[0]; f1 = r.f[1]; f2 = r.f[2]; c0 = r.c[0]; c1 = r.c[1];
-        ox = (int)(r.bxy & 0xFFFFu) + t.sx[sgi] + tap_offset<W>(f0);
-        oy = (int)(r.bxy >> 16) + t.sy[sgi] + tap_offset<W>(f1);
-        oz = (int)r.bz + t.sz[sgi] + tap_offset<W>(f2);
-        take = max(ox, tx0) < min(ox + W, tx1) && max(oy, ty0) < min(oy + W, ty1) &&
-               max(oz, p0) < min(oz + W, p1);
+        cd.f0 = r.f[0]; cd.f1 = r.f[1]; cd.f2 = r.f[2]; cd.c0 = r.c[0]; cd.c1 = r.c[1];
+        cd.bx = (int)(r.bxy & 0xFFFFu) + t.sx[sgi];
+        cd.by = (int)(r.bxy >> 16) + t.sy[sgi];
+        cd.bz = (int)r.bz + t.sz[sgi];
       }
+      return cd;
+    };
+    struct Prep {
+      T kv[NKV];
+      T vr0, vi0;
+      int vx, vy, vz;
+    };
+    Cand nextc = load_cand(lane);
+    for (int q0 = 0; q0 < total; q0 += 32) {
+      const Cand cc = nextc;
+      if (q0 + 32 < total) nextc = load_cand(q0 + 32 + lane);
+      const int ox = cc.bx + tap_offset<W>(cc.f0);
+      const int oy = cc.by + tap_offset<W>(cc.f1);
+      const int oz = cc.bz + tap_offset<W>(cc.f2);
+      const bool take = cc.ok && max(ox, tx0) < min(ox + W, tx1) &&
+                        max(oy, ty0) < min(oy + W, ty1) && max(oz, p0) < min(oz + W, p1);
       unsigned mask = __ballot_sync(0xffffffffu, take);
-      while (mask) {
-        const int src = __ffs(mask) - 1;
-        mask &= mask - 1;
-        const T g0 = __shfl_sync(0xffffffffu, f0, src), g1 = __shfl_sync(0xffffffffu, f1, src);
-        const T g2 = __shfl_sync(0xffffffffu, f2, src);
-        const T vr0 = __shfl_sync(0xffffffffu, c0, src), vi0 = __shfl_sync(0xffffffffu, c1, src);
-        const int vx = __shfl_sync(0xffffffffu, ox, src) - tx0;
-        const int vy = __shfl_sync(0xffffffffu, oy, src) - ty0;
-        const int vz = __shfl_sync(0xffffffffu, oz, src) - p0;
-        // kernel values: lane slot s = axis * W + i, s < 3W
-        T kv[NKV];
+      // broadcast of row `src` and its kernel values: lane slot s = axis * W + i, s < 3W
+      auto prepare = [&](int src) {
+        Prep pr;
+        const T g0 = __shfl_sync(0xffffffffu, cc.f0, src), g1 = __shfl_sync(0xffffffffu, cc.f1, src);
+        const T g2 = __shfl_sync(0xffffffffu, cc.f2, src);
+        pr.vr0 = __shfl_sync(0xffffffffu, cc.c0, src);
+        pr.vi0 = __shfl_sync(0xffffffffu, cc.c1, src);
+        pr.vx = __shfl_sync(0xffffffffu, ox, src) - tx0;
+        pr.vy = __shfl_sync(0xffffffffu, oy, src) - ty0;
+        pr.vz = __shfl_sync(0xffffffffu, oz, src) - p0;
 #pragma unroll
         for (int k = 0; k < NKV; k++) {
           const int sl = lane + 32 * k;
           const int axis = sl / W, i = sl - axis * W;
           const T f = axis == 0 ? g0 : (axis == 1 ? g1 : g2);
           if constexpr (kPoly)
-            kv[k] = (sl < 3 * W) ? poly_eval(pc[k], poly_arg<W>(f)) : (T)0;
+            pr.kv[k] = (sl < 3 * W) ? poly_eval(pc[k], poly_arg<W>(f)) : (T)0;
           else
-            kv[k] = (sl < 3 * W) ? es_kernel<T>((T)(tap_offset<W>(f) + i) - f, beta, c, halfw) : (T)0;
+            pr.kv[k] = (sl < 3 * W) ? es_kernel<T>((T)(tap_offset<W>(f) + i) - f, beta, c, halfw) : (T)0;
         }
+        return pr;
+      };
+      // spread one prepared row into the warp tile
+      auto apply = [&](const Prep& cur) {
+        const T* kv = cur.kv;
+        const T vr0 = cur.vr0, vi0 = cur.vi0;
+        const int vx = cur.vx, vy = cur.vy, vz = cur.vz;
         T kx[W];
         unsigned xmask = 0;
 #pragma unroll
@@ -426,7 +459,7 @@ __global__ void __launch_bounds__(256) k_grid_warp(const Rec<T>* __restrict__ re
           xmask |= ((unsigned)(vx + e >= 0 && vx + e < wx)) << e;
         }
 #pragma unroll
-        for (int rr = 0; rr < NR; rr++) {
+        for (int rr = 0; rr < NRR; rr++) {
           const int pp = lane + 32 * rr;
           const int dy = pp % W, dz = pp / W;
           const T ky = __shfl_sync(0xffffffffu, kv[0], W + dy);
@@ -452,7 +485,59 @@ __global__ void __launch_bounds__(256) k_grid_warp(const Rec<T>* __restrict__ re
             }
           }
         }
-        __syncwarp();
+        if constexpr (kTail) {
+          // lane -> (pair, x tap) of the remaining pairs; all cells distinct
+#pragma unroll
+          for (int it = 0; it < NTAIL; it++) {
+            const int t = lane + 32 * it;
+            const int pp = 32 * NFULL + t / W, e = t - (t / W) * W;
+            const int dy = pp % W, dz = pp / W;
+            const T ky = __shfl_sync(0xffffffffu, kv[0], W + dy);
+            const int zs = 2 * W + dz;
+            T kz = __shfl_sync(0xffffffffu, kv[0], zs & 31);
+            if (NKV > 1) {
+              const T kz1 = __shfl_sync(0xffffffffu, kv[NKV - 1], zs & 31);
+              kz = zs >= 32 ? kz1 : kz;
+            }
+            const T kxe = __shfl_sync(0xffffffffu, kv[0], e);
+            const int x = vx + e, y = vy + dy, z = vz + dz;
+            if (t < REM * W && x >= 0 && x < wx && y >= 0 && y < wy && z >= 0 && z < wz) {
+              const T k = ky * kz;
+              const T vr = vr0 * k, vi = vi0 * k;
+              C* a = acc + z * PS + y * RS + x;
+              C cur = *a;
+              cur.x += vr * kxe;
+              cur.y += vi * kxe;
+              *a = cur;
+            }
+          }
+        }
+      };
+      if constexpr (kPoly) {
+        // polynomial kernel values are cheap: no look-ahead
+        while (mask) {
+          const Prep cur = prepare(__ffs(mask) - 1);
+          mask &= mask - 1;
+          apply(cur);
+          __syncwarp();
+        }
+      } else {
+        // ES values (exp, sqrt) of the next row are computed ahead
+        if (!mask) continue;
+        Prep cur = prepare(__ffs(mask) - 1);
+        mask &= mask - 1;
+        while (true) {
+          const bool more = mask != 0;
+          Prep nxt;
+          if (more) {
+            nxt = prepare(__ffs(mask) - 1);
+            mask &= mask - 1;
+          }
+          apply(cur);
+          __syncwarp();
+          if (!more) break;
+          cur = nxt;
+        }
       }
     }
     // flush the tile, coalesced along x
@@ -564,7 +649,9 @@ TileCfg grid_tiling(const Geom& g, bool degrid) {
   const size_t budget = 220 * 1024;
   const int W = g.kw;
   TileCfg tc{};
-  int TX = env_int("CG_TILE_X", 32), TY = env_int("CG_TILE_Y", 32);
+  // degridding: 32 x 16 tiles keep two CTAs per SM for FP32 at W <= 7 (one
+  // stages its tile while the other interpolates); 32 x 32 left one CTA per SM
+  int TX = env_int("CG_TILE_X", 32), TY = env_int("CG_TILE_Y", degrid ? 16 : 32);
   TX = std::max(8, (TX / 8) * 8);
   TY = std::max(8, (TY / 8) * 8);
   int PB = env_int("CG_TILE_PLANES", 0);
