@@ -77,6 +77,8 @@ SIGNATURES = {
     "cg_plan_ms2dirty": (c_int, [c_void_p, c_int64, c_double, _PTR, _PTR, _PTR, _PTR]),
     "cg_plan_dirty2ms": (c_int, [c_void_p, c_int64, c_double, _PTR, _PTR, _PTR, _PTR]),
     "cg_plan_get_info": (c_int, [c_void_p, ctypes.POINTER(PlanInfo)]),
+    "cg_plan_ms2dirty_chan": (c_int, [c_void_p, c_int64, c_int, _PTR, _PTR, _PTR, _PTR, _PTR]),
+    "cg_plan_dirty2ms_chan": (c_int, [c_void_p, c_int64, c_int, _PTR, _PTR, _PTR, _PTR, _PTR]),
     "cg_plan_destroy": (c_int, [c_void_p]),
     "cg_plan_copy_buffer": (c_int, [c_void_p, c_int, c_void_p, c_size_t, ctypes.POINTER(c_size_t)]),
     "cg_plan_set_stop_stage": (c_int, [c_void_p, c_int]),

@@ -14,6 +14,7 @@
 // Counts, offsets and cell membership equal the reference's; the order inside
 // a cell is the original row order (one of the orders the reference can
 // produce), so results are deterministic.
+#include <algorithm>
 #include <cfloat>
 
 #include "cg_coords.cuh"
@@ -313,39 +314,34 @@ static int scan_exclusive(const int* d_in, int64_t n, int* d_out, int* d_sums, c
 }
 
 // ---------------------------------------------------------------- hive offsets
-// hive_start[h] = first sorted row whose key >= 64 h, for h = 0..nh.  Each
-// thread runs kHsIlp independent lower-bound searches in lockstep (hives
-// h0 + j * stride) so their dependent loads overlap.
-constexpr int kHsIlp = 8;
+// hive_start[h] = first sorted row whose key >= 64 h, for h = 0..nh, by
+// binary search (used when no scan scratch is given).
 template <typename K>
 __global__ void k_hive_start(const K* __restrict__ skeys, int64_t M, int64_t nh,
                              int* __restrict__ hive_start) {
+  for (int64_t h = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h <= nh;
+       h += (int64_t)gridDim.x * blockDim.x) {
+    unsigned long long target = (unsigned long long)h * 64ULL;
+    int64_t lo = 0, hi = M;
+    while (lo < hi) {
+      int64_t mid = (lo + hi) >> 1;
+      if ((unsigned long long)skeys[mid] < target) lo = mid + 1; else hi = mid;
+    }
+    hive_start[h] = (int)lo;
+  }
+}
+
+// rows per hive from the sorted keys: runs of equal hives inside a warp are
+// counted with one atomic by their first lane (counts zeroed beforehand)
+template <typename K>
+__global__ void k_hive_count(const K* __restrict__ skeys, int64_t M, int* __restrict__ counts) {
+  const int lane = threadIdx.x & 31;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-  for (int64_t h0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; h0 <= nh;
-       h0 += stride * kHsIlp) {
-    unsigned long long target[kHsIlp];
-    int64_t lo[kHsIlp], hi[kHsIlp];
-#pragma unroll
-    for (int j = 0; j < kHsIlp; j++) {
-      target[j] = (unsigned long long)(h0 + j * stride) * 64ULL;
-      lo[j] = 0;
-      hi[j] = M;
-    }
-    bool busy = true;
-    while (busy) {
-      busy = false;
-#pragma unroll
-      for (int j = 0; j < kHsIlp; j++) {
-        if (lo[j] < hi[j]) {
-          const int64_t mid = (lo[j] + hi[j]) >> 1;
-          if ((unsigned long long)skeys[mid] < target[j]) lo[j] = mid + 1; else hi[j] = mid;
-          busy |= lo[j] < hi[j];
-        }
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < kHsIlp; j++)
-      if (h0 + j * stride <= nh) hive_start[h0 + j * stride] = (int)lo[j];
+  for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < M; base += stride) {
+    const int64_t s = base + threadIdx.x;
+    const long long h = s < M ? (long long)((unsigned long long)skeys[s] >> 6) : -1LL;
+    const unsigned peers = __match_any_sync(0xffffffffu, h);
+    if (h >= 0 && lane == __ffs(peers) - 1) atomicAdd(&counts[h], __popc(peers));
   }
 }
 
@@ -364,7 +360,7 @@ size_t bin_workspace_bytes(int64_t M, int key_bytes) {
 
 template <typename K>
 static int bin_impl(const double* d_uvw, int64_t M, const Geom& g, void* d_ws, int* d_perm,
-                    K* d_sorted_keys, int* d_hive_start, cudaStream_t st) {
+                    K* d_sorted_keys, int* d_hive_start, cudaStream_t st, int* d_hs_sums) {
   int64_t ntiles = (M + kRsTile - 1) / kRsTile;
   int64_t ncount = 256 * ntiles;
   char* p = (char*)d_ws;
@@ -406,8 +402,19 @@ static int bin_impl(const double* d_uvw, int64_t M, const Geom& g, void* d_ws, i
     if (vin != d_perm) CG_CUDA(cudaMemcpyAsync(d_perm, vin, (size_t)M * 4, cudaMemcpyDeviceToDevice, st));
     CG_CUDA(cudaMemcpyAsync(d_sorted_keys, kin, (size_t)M * sizeof(K), cudaMemcpyDeviceToDevice, st));
   }
-  int hb = (int)((nh + 1 + 256 * kHsIlp - 1) / (256 * kHsIlp));
-  if (hb > 148 * 8) hb = 148 * 8;
+  if (d_hs_sums) {
+    // counts per hive, then an in-place exclusive scan: O(M + nh), no search
+    CG_CUDA(cudaMemsetAsync(d_hive_start, 0, (size_t)(nh + 1) * 4, st));
+    if (M > 0) {
+      int cb = (int)std::min<int64_t>((M + 255) / 256, 148 * 16);
+      k_hive_count<K><<<cb, 256, 0, st>>>(d_sorted_keys, M, d_hive_start);
+      count_launches(1);
+      CG_CUDA(cudaGetLastError());
+    }
+    return scan_exclusive(d_hive_start, nh + 1, d_hive_start, d_hs_sums, st);
+  }
+  int hb = (int)((nh + 1 + 255) / 256);
+  if (hb > 148 * 32) hb = 148 * 32;
   k_hive_start<K><<<hb, 256, 0, st>>>(d_sorted_keys, M, nh, d_hive_start);
   count_launches(1);
   CG_CUDA(cudaGetLastError());
@@ -416,12 +423,13 @@ static int bin_impl(const double* d_uvw, int64_t M, const Geom& g, void* d_ws, i
 
 int launch_bin(const double* d_uvw, int64_t M, const Geom& g, int key_bytes, void* d_ws,
                size_t ws_bytes, int* d_perm, void* d_sorted_keys, int* d_hive_start,
-               cudaStream_t st) {
+               cudaStream_t st, int* d_hs_sums) {
   if (ws_bytes < bin_workspace_bytes(M, key_bytes)) return CG_ERR_ARG;
   if (key_bytes == 4)
-    return bin_impl<uint32_t>(d_uvw, M, g, d_ws, d_perm, (uint32_t*)d_sorted_keys, d_hive_start, st);
+    return bin_impl<uint32_t>(d_uvw, M, g, d_ws, d_perm, (uint32_t*)d_sorted_keys, d_hive_start, st,
+                              d_hs_sums);
   return bin_impl<unsigned long long>(d_uvw, M, g, d_ws, d_perm, (unsigned long long*)d_sorted_keys,
-                                      d_hive_start, st);
+                                      d_hive_start, st, d_hs_sums);
 }
 
 // ---------------------------------------------------------------- sorted stream

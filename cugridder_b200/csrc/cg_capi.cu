@@ -6,6 +6,7 @@
 // device buffer and cuFFT plan inside each call (cugridder.cu:309-388), they
 // share one cached plan per precision so repeated calls reuse HBM workspace;
 // cg_release_cache() frees it.  Errors are returned, never exit()ed.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -76,7 +77,8 @@ void destroy_plan(cg_plan_s* P) {
   if (P->cols_valid) cufftDestroy(P->fft_cols);
   cg_dev_buf* bs[] = {&P->mm,   &P->K1,    &P->K2,     &P->K3q,    &P->zq,     &P->grid,
                       &P->recs, &P->perm,  &P->skeys,  &P->hive_start, &P->binws, &P->fftwork,
-                      &P->io_uvw, &P->io_vis, &P->io_wgt, &P->io_dirty, &P->polyf, &P->polyd, &P->recs_tmp};
+                      &P->io_uvw, &P->io_vis, &P->io_wgt, &P->io_dirty, &P->polyf, &P->polyd, &P->recs_tmp,
+                      &P->chan_uvw, &P->chan_scale};
   for (auto b : bs) cg::release(*b);
   if (P->h_mm) cudaFreeHost(P->h_mm);
   if (P->timer.created)
@@ -107,6 +109,59 @@ __global__ void k_widen_uvw(const float* __restrict__ in, double* __restrict__ o
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x)
     out[i] = (double)in[i];
+}
+
+// Multi-channel rows: row r of channel c is the visibility at frequency f_c.
+// Its phase 2 pi f_c/c (u l + v m + w (n-1)) equals that of a row with
+// uvw * (f_c / f_0) at frequency f_0, so the channels are flattened into
+// nrow * nchan rows (index r * nchan + c, the layout of vis[nrow][nchan]) of
+// one call at f_0 = freqs[0]; channel 0 keeps its coordinates bit for bit.
+__global__ void k_expand_chan(const double* __restrict__ uvw, int64_t nrow, int nchan,
+                              const double* __restrict__ scale, double* __restrict__ out) {
+  const int64_t n = nrow * nchan;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = q / nchan;
+    const double s = scale[q - r * nchan];
+#pragma unroll
+    for (int k = 0; k < 3; k++) out[3 * q + k] = uvw[3 * r + k] * s;
+  }
+}
+
+int expand_channels(cg_plan_s* P, int64_t nrow, int nchan, const double* freqs,
+                    const double* d_uvw, const double** d_out) {
+  if (nchan < 1 || !freqs || nrow < 0) {
+    cg::set_last_error("nchan must be >= 1 with nchan frequencies");
+    return CG_ERR_ARG;
+  }
+  if (nrow * (int64_t)nchan > 2147483647LL) {
+    cg::set_last_error("nrow * nchan out of range");
+    return CG_ERR_SIZE;
+  }
+  std::vector<double> sc(nchan);
+  for (int c = 0; c < nchan; c++) {
+    if (!(freqs[c] > 0.0) || !std::isfinite(freqs[c])) {
+      cg::set_last_error("frequencies must be positive and finite");
+      return CG_ERR_ARG;
+    }
+    sc[c] = c == 0 ? 1.0 : freqs[c] / freqs[0];
+  }
+  if (nchan == 1 || nrow == 0) {
+    *d_out = d_uvw;
+    return CG_OK;
+  }
+  CG_TRY(ensure(P->chan_scale, sizeof(double) * nchan));
+  CG_TRY(ensure(P->chan_uvw, sizeof(double) * 3 * (size_t)nrow * nchan));
+  CG_CUDA(cudaMemcpyAsync(P->chan_scale.p, sc.data(), sizeof(double) * nchan,
+                          cudaMemcpyHostToDevice, P->stream));
+  int64_t n = nrow * nchan;
+  int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
+  k_expand_chan<<<blocks, 256, 0, P->stream>>>(d_uvw, nrow, nchan, (const double*)P->chan_scale.p,
+                                                (double*)P->chan_uvw.p);
+  cg::count_launches(1);
+  CG_CUDA(cudaGetLastError());
+  *d_out = (const double*)P->chan_uvw.p;
+  return CG_OK;
 }
 
 // Host-pointer driver shared by every host entry point.
@@ -267,6 +322,28 @@ int cg_plan_dirty2ms(cg_plan* plan, int64_t nrow, double freq, const double* d_u
   if (!plan) return CG_ERR_ARG;
   std::lock_guard<std::mutex> lock(plan->mu);
   return cg::dirty2ms_device(plan, nrow, freq, d_uvw, d_dirty, d_wgt, d_vis);
+}
+
+int cg_plan_ms2dirty_chan(cg_plan* plan, int64_t nrow, int nchan, const double* freqs,
+                          const double* d_uvw, const void* d_vis, const void* d_wgt,
+                          void* d_dirty) {
+  if (!plan) return CG_ERR_ARG;
+  std::lock_guard<std::mutex> lock(plan->mu);
+  CG_CUDA(cudaSetDevice(plan->device));
+  const double* u = nullptr;
+  CG_TRY(expand_channels(plan, nrow, nchan, freqs, d_uvw, &u));
+  return cg::ms2dirty_device(plan, nrow * nchan, freqs[0], u, d_vis, d_wgt, d_dirty);
+}
+
+int cg_plan_dirty2ms_chan(cg_plan* plan, int64_t nrow, int nchan, const double* freqs,
+                          const double* d_uvw, const void* d_dirty, const void* d_wgt,
+                          void* d_vis) {
+  if (!plan) return CG_ERR_ARG;
+  std::lock_guard<std::mutex> lock(plan->mu);
+  CG_CUDA(cudaSetDevice(plan->device));
+  const double* u = nullptr;
+  CG_TRY(expand_channels(plan, nrow, nchan, freqs, d_uvw, &u));
+  return cg::dirty2ms_device(plan, nrow * nchan, freqs[0], u, d_dirty, d_wgt, d_vis);
 }
 
 int cg_plan_get_info(const cg_plan* plan, cg_plan_info* info) {

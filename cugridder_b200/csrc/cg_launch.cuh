@@ -13,9 +13,12 @@ double decode_ordered(unsigned long long k);
 // Stable LSD radix sort of the reference's hive-major cell keys.
 // Workspace sizes in bytes for M rows and a key of key_bytes (4 or 8).
 size_t bin_workspace_bytes(int64_t M, int key_bytes);
+// d_hs_sums: scratch of hive_sums_ints(nh) ints for the counting hive
+// offsets; nullptr selects a binary search over the sorted keys instead.
 int launch_bin(const double* d_uvw, int64_t M, const Geom& g, int key_bytes, void* d_ws,
                size_t ws_bytes, int* d_perm, void* d_sorted_keys, int* d_hive_start,
-               cudaStream_t st);
+               cudaStream_t st, int* d_hs_sums = nullptr);
+inline int64_t hive_sums_ints(int64_t nh) { return (nh + 1 + 4095) / 4096; }
 
 template <typename T>
 int launch_build_stream(const int* d_perm, int64_t M, const double* d_uvw, const T* d_vis,

@@ -9,6 +9,7 @@
 // w range per call).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -394,7 +395,8 @@ static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw)
   size_t tsz = (P->precision == CG_PREC_FP64) ? 8 : 4;
   size_t G = (size_t)g.nf1 * g.nf2 * g.nw;
   CG_TRY(ensure(P->grid, G * 2 * tsz));
-  CG_TRY(ensure(P->hive_start, (size_t)(nh + 1) * 4));
+  // hive offsets followed by the scan scratch of the counting path
+  CG_TRY(ensure(P->hive_start, (size_t)(nh + 1 + hive_sums_ints(nh)) * 4));
   CG_TRY(ensure(P->perm, (size_t)nrow * 4));
   CG_TRY(ensure(P->skeys, (size_t)nrow * P->key_bytes));
   CG_TRY(ensure(P->binws, bin_workspace_bytes(nrow, P->key_bytes)));
@@ -498,7 +500,9 @@ static int fft_exec_pruned(cg_plan_s* P, void* d_grid, int direction) {
     P->rows_n = g.nf1;
     P->rows_batch = batch;
   }
-  const int half = g.N1 / 2;
+  // CG_FFT_COLS_ALL=1 (tuning): one column transform over every grid column
+  static const bool cols_all = getenv("CG_FFT_COLS_ALL") && atoi(getenv("CG_FFT_COLS_ALL")) != 0;
+  const int half = cols_all ? g.nf1 : g.N1 / 2;
   if (!P->cols_valid || P->cols_n != g.nf2 || P->cols_stride != g.nf1 || P->cols_batch != half) {
     CG_TRY(make_1d_plan(P, P->fft_cols, P->cols_valid, g.nf2, g.nf1, half));
     P->cols_n = g.nf2;
@@ -512,7 +516,7 @@ static int fft_exec_pruned(cg_plan_s* P, void* d_grid, int direction) {
   auto rows = [&](int p) { return exec_c2c(P, P->fft_rows, base + esz * (p * plane + (size_t)r0 * g.nf1), direction); };
   auto cols = [&](int p) {
     int s1 = exec_c2c(P, P->fft_cols, base + esz * (p * plane), direction);
-    if (s1 > 1) return s1;
+    if (s1 > 1 || cols_all) return s1;
     return exec_c2c(P, P->fft_cols, base + esz * (p * plane + (size_t)(g.nf1 - half)), direction);
   };
   for (int p = 0; p < g.nw; p++) {
@@ -527,6 +531,8 @@ static int fft_exec_pruned(cg_plan_s* P, void* d_grid, int direction) {
   return CG_OK;
 }
 
+static int64_t nh_of(const Geom& g) { return (int64_t)g.nhx * g.nhy * g.nhz; }
+
 template <typename T>
 static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T* d_wgt,
                       T* d_dirty) {
@@ -537,7 +543,8 @@ static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T
   CG_TRY(launch_quarter(g, P->quad, (double*)P->K3q.p, (double*)P->zq.p, st));
   timer_mark(P);  // 1: quarter tables
   CG_TRY(launch_bin(d_uvw, M, g, P->key_bytes, P->binws.p, P->binws.cap, (int*)P->perm.p,
-                    P->skeys.p, (int*)P->hive_start.p, st));
+                    P->skeys.p, (int*)P->hive_start.p, st,
+                    (int*)P->hive_start.p + (nh_of(g) + 1)));
   timer_mark(P);  // 2: binning
   if (P->stop_stage == 1) return CG_OK;
   CG_TRY(launch_build_stream<T>((const int*)P->perm.p, M, d_uvw, d_vis, d_wgt, g, true,
@@ -567,7 +574,8 @@ static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const
   CG_TRY(launch_quarter(g, P->quad, (double*)P->K3q.p, (double*)P->zq.p, st));
   timer_mark(P);  // 1: quarter tables
   CG_TRY(launch_bin(d_uvw, M, g, P->key_bytes, P->binws.p, P->binws.cap, (int*)P->perm.p,
-                    P->skeys.p, (int*)P->hive_start.p, st));
+                    P->skeys.p, (int*)P->hive_start.p, st,
+                    (int*)P->hive_start.p + (nh_of(g) + 1)));
   timer_mark(P);  // 2: binning
   if (P->stop_stage == 1) return CG_OK;
   CG_TRY(launch_plane_fill<T>(d_dirty, g, (const double*)P->K1.p, (const double*)P->K2.p,

@@ -59,6 +59,23 @@ class Plan:
                                        _lib.ptr(wgt), _lib.ptr(vis))
         return _lib.check(r)
 
+    def ms2dirty_chan(self, uvw, freqs, vis, wgt, dirty):
+        """Multi-channel ms2dirty: vis / wgt [nrow, nchan] on the device, freqs
+        a host sequence of nchan frequencies; every channel is summed into dirty."""
+        f = np.ascontiguousarray(np.asarray(freqs, dtype=np.float64).reshape(-1))
+        r = self._lib.cg_plan_ms2dirty_chan(self._h, int(uvw.shape[0]), f.size, f.ctypes.data,
+                                            _lib.ptr(uvw), _lib.ptr(vis), _lib.ptr(wgt),
+                                            _lib.ptr(dirty))
+        return _lib.check(r)
+
+    def dirty2ms_chan(self, uvw, freqs, dirty, wgt, vis):
+        """Multi-channel dirty2ms into vis [nrow, nchan] on the device."""
+        f = np.ascontiguousarray(np.asarray(freqs, dtype=np.float64).reshape(-1))
+        r = self._lib.cg_plan_dirty2ms_chan(self._h, int(uvw.shape[0]), f.size, f.ctypes.data,
+                                            _lib.ptr(uvw), _lib.ptr(dirty), _lib.ptr(wgt),
+                                            _lib.ptr(vis))
+        return _lib.check(r)
+
     def info(self):
         inf = _lib.PlanInfo()
         _lib.check(self._lib.cg_plan_get_info(self._h, ctypes.byref(inf)))

@@ -123,6 +123,20 @@ int cg_plan_ms2dirty(cg_plan *plan, int64_t nrow, double freq, const double *d_u
 int cg_plan_dirty2ms(cg_plan *plan, int64_t nrow, double freq, const double *d_uvw,
                      const void *d_dirty, const void *d_wgt, void *d_vis);
 int cg_plan_get_info(const cg_plan *plan, cg_plan_info *info);
+
+/* Multi-channel calls (no reference counterpart: the reference's C API takes
+ * one frequency, cursl.py:78 uses freq[0] only and the channel loop of
+ * w_s_gridder_test.cu:206-224 is broken).  freqs: HOST array of nchan
+ * frequencies; d_vis / d_wgt are [nrow][nchan] (d_wgt may be NULL).
+ * ms2dirty sums every (row, channel) visibility into one image, as NIFTY's
+ * ms2dirty does; dirty2ms fills every (row, channel).  The channels are
+ * flattened into nrow * nchan rows of one call (uvw scaled by f_c / f_0). */
+int cg_plan_ms2dirty_chan(cg_plan *plan, int64_t nrow, int nchan, const double *freqs,
+                          const double *d_uvw, const void *d_vis, const void *d_wgt,
+                          void *d_dirty);
+int cg_plan_dirty2ms_chan(cg_plan *plan, int64_t nrow, int nchan, const double *freqs,
+                          const double *d_uvw, const void *d_dirty, const void *d_wgt,
+                          void *d_vis);
 int cg_plan_destroy(cg_plan *plan);
 
 /* ---------------- inspection (tests / tools) ----------------
