@@ -78,7 +78,7 @@ void destroy_plan(cg_plan_s* P) {
   cg_dev_buf* bs[] = {&P->mm,   &P->K1,    &P->K2,     &P->K3q,    &P->zq,     &P->grid,
                       &P->recs, &P->perm,  &P->skeys,  &P->hive_start, &P->binws, &P->fftwork,
                       &P->io_uvw, &P->io_vis, &P->io_wgt, &P->io_dirty, &P->polyf, &P->polyd, &P->recs_tmp,
-                      &P->chan_uvw, &P->chan_scale};
+                      &P->chan_uvw, &P->chan_scale, &P->coltw};
   for (auto b : bs) cg::release(*b);
   if (P->h_mm) cudaFreeHost(P->h_mm);
   if (P->timer.created)
@@ -295,6 +295,7 @@ int cg_plan_create(cg_plan** plan, int nxdirty, int nydirty, double fov, double 
     P->grid_method = (v >= 0 && v <= 2) ? v : 1;
   }
   if (const char* m = getenv("CG_FFT_PRUNE")) P->fft_pruning = atoi(m) != 0;
+  if (const char* m = getenv("CG_COL_FFT")) P->col_fft = atoi(m) != 0;
   st = cg::plan_configure(P, nxdirty, nydirty, fov, epsilon, sigma, sign, precision);
   if (st > 1) {
     destroy_plan(P);

@@ -43,6 +43,13 @@ int launch_degrid(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_sta
                   const Geom& g, const T* d_fw, T* d_vis, int method, int* d_counter,
                   cudaStream_t st);
 
+// ---- column FFTs in shared memory (cg_fft.cu) ----
+bool col_fft_supported(int L, int na, int nb);
+size_t col_fft_twiddle_count(int L);
+int make_col_fft_twiddles(int L, float2* d_tw, cudaStream_t st);
+int launch_col_fft(float2* grid, int L, int nf1, size_t plane, int nplanes, int c0a, int na,
+                   int c0b, int nb, int sign, const float2* d_tw, cudaStream_t st);
+
 // ---- w stage (cg_wstage.cu) ----
 int launch_quarter(const Geom& g, const Quad& q, double* d_K3q, double* d_zq, cudaStream_t st);
 template <typename T>

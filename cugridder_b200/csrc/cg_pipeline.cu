@@ -519,6 +519,29 @@ static int fft_exec_pruned(cg_plan_s* P, void* d_grid, int direction) {
     if (s1 > 1 || cols_all) return s1;
     return exec_c2c(P, P->fft_cols, base + esz * (p * plane + (size_t)(g.nf1 - half)), direction);
   };
+  // FP32 power-of-two columns: the shared-memory column transform over every
+  // plane in one launch (the image's two column ranges of N1/2)
+  if (P->col_fft && !cols_all && P->precision == CG_PREC_FP32 &&
+      col_fft_supported(g.nf2, half, half)) {
+    if (P->coltw_n != g.nf2) {
+      CG_TRY(ensure(P->coltw, sizeof(float2) * col_fft_twiddle_count(g.nf2)));
+      CG_TRY(make_col_fft_twiddles(g.nf2, (float2*)P->coltw.p, P->stream));
+      P->coltw_n = g.nf2;
+    }
+    auto all_cols = [&]() {
+      return launch_col_fft((float2*)d_grid, g.nf2, g.nf1, plane, g.nw, 0, half, g.nf1 - half, half,
+                            direction == CUFFT_INVERSE ? 1 : -1, (const float2*)P->coltw.p,
+                            P->stream);
+    };
+    if (direction == CUFFT_INVERSE) {
+      for (int p = 0; p < g.nw; p++) CG_TRY(rows(p));
+      CG_TRY(all_cols());
+    } else {
+      CG_TRY(all_cols());
+      for (int p = 0; p < g.nw; p++) CG_TRY(rows(p));
+    }
+    return CG_OK;
+  }
   for (int p = 0; p < g.nw; p++) {
     if (direction == CUFFT_INVERSE) {
       CG_TRY(rows(p));
