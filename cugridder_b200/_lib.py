@@ -104,6 +104,12 @@ SIGNATURES = {
                                      c_int, c_int64, _PTR, _PTR, c_void_p]),
     "cg_explicit_dirty2ms": (c_int, [c_int64, c_int, c_int, c_double, c_double, _PTR, _PTR, _PTR,
                                      c_int, c_int64, _PTR, _PTR, c_void_p]),
+    "cg_nufft_create": (c_int, [ctypes.POINTER(c_void_p), c_int, c_int, _PTR, c_int, c_double,
+                                c_double, c_int, c_void_p]),
+    "cg_nufft_setpts": (c_int, [c_void_p, c_int64, _PTR, _PTR, _PTR]),
+    "cg_nufft_execute": (c_int, [c_void_p, _PTR, _PTR]),
+    "cg_nufft_get_info": (c_int, [c_void_p, ctypes.POINTER(c_int), _PTR]),
+    "cg_nufft_destroy": (c_int, [c_void_p]),
     "cg_release_cache": (c_int, []),
     "cg_last_error": (ctypes.c_char_p, []),
     "cg_kernel_launches": (ctypes.c_longlong, []),

@@ -421,6 +421,52 @@ static int bin_impl(const double* d_uvw, int64_t M, const Geom& g, void* d_ws, i
   return CG_OK;
 }
 
+__global__ void k_iota(int* __restrict__ v, int64_t M) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < M;
+       i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = (int)i;
+}
+
+// Stable sort of 32-bit keys (only the low `bits` bits are significant):
+// d_perm gets the original index of each sorted key and d_sorted its key.
+// d_keys is overwritten; workspace: bin_workspace_bytes(M, 4).
+int launch_sort_u32(uint32_t* d_keys, int64_t M, int bits, void* d_ws, size_t ws_bytes,
+                    int* d_perm, uint32_t* d_sorted, cudaStream_t st) {
+  if (ws_bytes < bin_workspace_bytes(M, 4)) return CG_ERR_ARG;
+  if (M == 0) return CG_OK;
+  using K = uint32_t;
+  const int64_t ntiles = (M + kRsTile - 1) / kRsTile, ncount = 256 * ntiles;
+  char* p = (char*)d_ws;
+  K* kb = (K*)p; p += align256((size_t)M * 4);
+  p += align256((size_t)M * 4);  // (second key buffer of the plan layout, unused here)
+  int* vb = (int*)p; p += align256((size_t)M * 4);
+  int* counts = (int*)p; p += align256((size_t)ncount * 4);
+  int* offs = (int*)p; p += align256((size_t)ncount * 4);
+  int* sums = (int*)p;
+  const int blocks = (int)std::min<int64_t>((M + 255) / 256, 148 * 32);
+  k_iota<<<blocks, 256, 0, st>>>(d_perm, M);
+  count_launches(1);
+  CG_CUDA(cudaFuncSetAttribute(k_rs_downsweep<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)rs_down_smem<K>()));
+  K* kin = d_keys; int* vin = d_perm; K* kout = kb; int* vout = vb;
+  const int passes = std::max(1, (bits + 7) / 8);
+  for (int ps = 0; ps < passes; ps++) {
+    const int shift = 8 * ps;
+    k_rs_upsweep<K><<<(int)ntiles, kRsThreads, 0, st>>>(kin, M, shift, (int)ntiles, counts);
+    count_launches(1);
+    CG_TRY(scan_exclusive(counts, ncount, offs, sums, st));
+    k_rs_downsweep<K><<<(int)ntiles, kRsThreads, rs_down_smem<K>(), st>>>(
+        kin, vin, kout, vout, M, shift, (int)ntiles, offs);
+    count_launches(1);
+    CG_CUDA(cudaGetLastError());
+    K* tk = kin; kin = kout; kout = tk;
+    int* tv = vin; vin = vout; vout = tv;
+  }
+  if (vin != d_perm) CG_CUDA(cudaMemcpyAsync(d_perm, vin, (size_t)M * 4, cudaMemcpyDeviceToDevice, st));
+  CG_CUDA(cudaMemcpyAsync(d_sorted, kin, (size_t)M * 4, cudaMemcpyDeviceToDevice, st));
+  return CG_OK;
+}
+
 int launch_bin(const double* d_uvw, int64_t M, const Geom& g, int key_bytes, void* d_ws,
                size_t ws_bytes, int* d_perm, void* d_sorted_keys, int* d_hive_start,
                cudaStream_t st, int* d_hs_sums) {

@@ -19,6 +19,8 @@ int launch_bin(const double* d_uvw, int64_t M, const Geom& g, int key_bytes, voi
                size_t ws_bytes, int* d_perm, void* d_sorted_keys, int* d_hive_start,
                cudaStream_t st, int* d_hs_sums = nullptr);
 inline int64_t hive_sums_ints(int64_t nh) { return (nh + 1 + 4095) / 4096; }
+int launch_sort_u32(uint32_t* d_keys, int64_t M, int bits, void* d_ws, size_t ws_bytes,
+                    int* d_perm, uint32_t* d_sorted, cudaStream_t st);
 
 template <typename T>
 int launch_build_stream(const int* d_perm, int64_t M, const double* d_uvw, const T* d_vis,

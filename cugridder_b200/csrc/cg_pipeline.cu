@@ -137,7 +137,7 @@ static double poly_phi(const double* poly, int kw, double d) {
 
 // quadrature of the kernel Fourier series (deconv.cu:80-93): ES, or the
 // piecewise-polynomial kernel when poly is given
-static void make_quad(int kw, double beta, double c, const double* poly, Quad& q) {
+void make_quad(int kw, double beta, double c, const double* poly, Quad& q) {
   double alpha = kw / 2.0;
   int p = (int)(2 + 3.0 * alpha);
   double x[2 * kMaxQuad], w[2 * kMaxQuad];
@@ -153,7 +153,7 @@ static void make_quad(int kw, double beta, double c, const double* poly, Quad& q
 }
 
 // fwkerhalf{1,2} (deconv.cu:12-26): (-1)^k folded into the cosine
-static void fseries_uv(const Quad& q, int nf, double* out) {
+void fseries_uv(const Quad& q, int nf, double* out) {
   int N = nf / 2 + 1;
   for (int k = 0; k < N; k++) {
     double s = 0;

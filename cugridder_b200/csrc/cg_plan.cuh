@@ -75,6 +75,8 @@ namespace cg {
 int setup_conv_opts(double eps, double sigma, double eps_floor, int& kw, double& beta, double& c);
 int get_num_cells(int ms, double sigma, int kw);
 void set_nhg_w(double S, double X, int kw, double sigma, int& nf, double& h, double& gam);
+void make_quad(int kw, double beta, double c, const double* poly, Quad& q);
+void fseries_uv(const Quad& q, int nf, double* out);
 int plan_configure(cg_plan_s* P, int nx, int ny, double fov, double eps, double sigma, int sign,
                    int precision);
 int ensure(cg_dev_buf& b, size_t bytes);

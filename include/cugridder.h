@@ -279,6 +279,26 @@ int cg_explicit_dirty2ms(int64_t nrow, int nxdirty, int nydirty, double fov, dou
                          const double *d_uvw, const cg_c128 *d_dirty, const double *d_wgt, int sign,
                          int64_t nvis, const int64_t *d_rows, cg_c128 *d_out, void *stream);
 
+/* ---------------- generic NUFFT, type 1 and 2, 1-3 dimensions ----------------
+ * The reference's generic front end (cunufft_setting, cuft.cu:327-504, and
+ * the flow of test/nufft_{1d,2d_1,2d_2,3d_1,3d_2}_test.cu) on this library's
+ * ES kernel, Gauss-Legendre deconvolution, sorting and cuFFT.
+ *   type 1: fk[k3][k2][k1] = sum_j c_j exp(i iflag ((k1 - N1/2) x_j +
+ *           (k2 - N2/2) y_j + (k3 - N3/2) z_j)), k1 fastest;
+ *   type 2: c_j = sum_k fk[k3][k2][k1] exp(i iflag (...)).
+ * nmodes: dim entries N1 (, N2 (, N3)).  Coordinates: DEVICE FP64 arrays in
+ * radians (period 2 pi); c / fk: DEVICE complex arrays of the plan precision.
+ * setpts sorts the points (keep the coordinate arrays alive until then
+ * only); execute may be called many times per setpts. */
+typedef struct cg_nufft_s cg_nufft;
+int cg_nufft_create(cg_nufft **plan, int type, int dim, const int64_t *nmodes, int iflag,
+                    double epsilon, double sigma, int precision, void *stream);
+int cg_nufft_setpts(cg_nufft *plan, int64_t M, const double *d_x, const double *d_y,
+                    const double *d_z);
+int cg_nufft_execute(cg_nufft *plan, void *d_c, void *d_fk);
+int cg_nufft_get_info(const cg_nufft *plan, int *kw, int64_t *nf);
+int cg_nufft_destroy(cg_nufft *plan);
+
 /* Host-pointer calls above keep one cached plan per precision so that
  * repeated calls reuse device workspace; this frees it. */
 int cg_release_cache(void);

@@ -1,0 +1,57 @@
+"""The shared-memory column FFT (FP32, power-of-two columns) against cuFFT's
+strided column transforms, through the whole pipeline in both directions."""
+import os
+
+import numpy as np
+import pytest
+
+from cugridder_b200 import Plan, synth
+from cugridder_b200.synth import rel_l2
+
+from tests.gpu_helpers import to_dev
+
+pytestmark = pytest.mark.gpu
+
+
+def _narrow_band_case(N, nrow, seed):
+    """uv confined to about 30% of the grid rows, so the band-pruned FFT runs."""
+    fov = 1.0
+    pix = np.deg2rad(fov) / N
+    freq = 1.5e8
+    u_max = 0.15 / pix * 299792458.0 / freq
+    rng = np.random.Generator(np.random.PCG64(seed))
+    uvw = np.empty((nrow, 3))
+    uvw[:, :2] = rng.uniform(-u_max, u_max, (nrow, 2))
+    uvw[:, 2] = rng.uniform(-300.0, 300.0, nrow)
+    vis = (rng.standard_normal(nrow) + 1j * rng.standard_normal(nrow)).astype(np.complex64)
+    wgt = rng.uniform(0.5, 1.5, nrow).astype(np.float32)
+    return dict(uvw=uvw, vis=vis, wgt=wgt, nx=N, ny=N, fov=fov, freq=freq)
+
+
+def _run(torch, d, img, col_fft):
+    os.environ["CG_COL_FFT"] = "1" if col_fft else "0"
+    try:
+        plan = Plan(d["nx"], d["ny"], d["fov"], 1e-5, precision="fp32")
+    finally:
+        del os.environ["CG_COL_FFT"]
+    uvw = to_dev(torch, d["uvw"], np.float64)
+    wgt = to_dev(torch, d["wgt"])
+    dirty = torch.zeros((d["nx"], d["ny"]), dtype=torch.complex64, device="cuda")
+    plan.ms2dirty(uvw, d["freq"], to_dev(torch, d["vis"]), wgt, dirty)
+    vis = torch.zeros(d["uvw"].shape[0], dtype=torch.complex64, device="cuda")
+    plan.dirty2ms(uvw, d["freq"], to_dev(torch, img, np.complex64), wgt, vis)
+    torch.cuda.synchronize()
+    info = plan.info()
+    plan.close()
+    return dirty.cpu().numpy(), vis.cpu().numpy(), info
+
+
+@pytest.mark.parametrize("N", [512, 1024, 2048, 4096])
+def test_column_fft_matches_cufft(torch_cuda, N):
+    d = _narrow_band_case(N, 100_000, seed=N)
+    img = synth.random_image(N, N, seed=2)
+    a = _run(torch_cuda, d, img, True)
+    b = _run(torch_cuda, d, img, False)
+    assert a[2]["nf2"] == 2 * N
+    assert rel_l2(a[0], b[0]) < 2e-6
+    assert rel_l2(a[1], b[1]) < 2e-6
