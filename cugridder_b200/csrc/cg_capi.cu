@@ -75,10 +75,11 @@ void destroy_plan(cg_plan_s* P) {
   if (P->fft_valid) cufftDestroy(P->fft);
   if (P->rows_valid) cufftDestroy(P->fft_rows);
   if (P->cols_valid) cufftDestroy(P->fft_cols);
+  if (P->fft1_valid) cufftDestroy(P->fft1);
   cg_dev_buf* bs[] = {&P->mm,   &P->K1,    &P->K2,     &P->K3q,    &P->zq,     &P->grid,
                       &P->recs, &P->perm,  &P->skeys,  &P->hive_start, &P->binws, &P->fftwork,
                       &P->io_uvw, &P->io_vis, &P->io_wgt, &P->io_dirty, &P->polyf, &P->polyd, &P->recs_tmp,
-                      &P->chan_uvw, &P->chan_scale, &P->coltw};
+                      &P->chan_uvw, &P->chan_scale, &P->coltw, &P->acc};
   for (auto b : bs) cg::release(*b);
   if (P->h_mm) cudaFreeHost(P->h_mm);
   if (P->timer.created)
@@ -424,6 +425,13 @@ int cg_set_host_kernel(int kind, int W, const double* coef) {
   g_host_kernel.kind = kind;
   g_host_kernel.w = W;
   if (kind == CG_KERNEL_POLY) memcpy(g_host_kernel.poly, coef, sizeof(double) * W * cg::kPolyCoef);
+  return CG_OK;
+}
+
+int cg_plan_set_grid_budget(cg_plan* plan, size_t bytes) {
+  if (!plan) return CG_ERR_ARG;
+  std::lock_guard<std::mutex> lock(plan->mu);
+  plan->grid_budget = bytes;
   return CG_OK;
 }
 

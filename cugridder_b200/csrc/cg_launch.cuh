@@ -52,6 +52,24 @@ int make_col_fft_twiddles(int L, float2* d_tw, cudaStream_t st);
 int launch_col_fft(float2* grid, int L, int nf1, size_t plane, int nplanes, int c0a, int na,
                    int c0b, int nb, int sign, const float2* d_tw, cudaStream_t st);
 
+// ---- memory-limited mode: plane windows [p0, p1) (cg_spread.cu, cg_wstage.cu) ----
+template <typename T>
+int launch_grid_window(const Rec<T>* d_recs, int64_t M, const Geom& g, int p0, int p1, T* d_fwb,
+                       cudaStream_t st);
+template <typename T>
+int launch_degrid_window(const Rec<T>* d_recs, const int* d_perm, int64_t M, const Geom& g,
+                         int p0, int p1, const T* d_fwb, T* d_vis, cudaStream_t st);
+template <typename T>
+int launch_wdft_window(const T* d_fwb, const Geom& g, int p0, int p1, const double* d_zq,
+                       double* d_acc, cudaStream_t st);
+template <typename T>
+int launch_wdft_finish(const double* d_acc, const Geom& g, const double* d_K1, const double* d_K2,
+                       const double* d_K3q, const double* d_zq, T* d_dirty, cudaStream_t st);
+template <typename T>
+int launch_plane_fill_window(const T* d_dirty, const Geom& g, int p0, int p1, const double* d_K1,
+                             const double* d_K2, const double* d_K3q, const double* d_zq, T* d_fwb,
+                             cudaStream_t st);
+
 // ---- w stage (cg_wstage.cu) ----
 int launch_quarter(const Geom& g, const Quad& q, double* d_K3q, double* d_zq, cudaStream_t st);
 template <typename T>

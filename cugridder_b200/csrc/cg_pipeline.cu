@@ -394,7 +394,20 @@ static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw)
   P->key_bytes = ((unsigned long long)nh * 64ULL <= 0xFFFFFFFFULL) ? 4 : 8;
   size_t tsz = (P->precision == CG_PREC_FP64) ? 8 : 4;
   size_t G = (size_t)g.nf1 * g.nf2 * g.nw;
-  CG_TRY(ensure(P->grid, G * 2 * tsz));
+  P->plane_batch = 0;
+  if (P->grid_budget > 0 && G * 2 * tsz > P->grid_budget) {
+    // memory-limited mode: as many whole planes as the budget holds
+    const size_t plane_bytes = (size_t)g.nf1 * g.nf2 * 2 * tsz;
+    const size_t pb = P->grid_budget / plane_bytes;
+    if (pb < 1) {
+      set_last_error("grid budget smaller than one w plane");
+      return CG_ERR_NOMEM;
+    }
+    P->plane_batch = (int)std::min<size_t>(pb, (size_t)g.nw);
+    CG_TRY(ensure(P->grid, (size_t)P->plane_batch * plane_bytes));
+  } else {
+    CG_TRY(ensure(P->grid, G * 2 * tsz));
+  }
   // hive offsets followed by the scan scratch of the counting path
   CG_TRY(ensure(P->hive_start, (size_t)(nh + 1 + hive_sums_ints(nh)) * 4));
   CG_TRY(ensure(P->perm, (size_t)nrow * 4));
@@ -556,6 +569,65 @@ static int fft_exec_pruned(cg_plan_s* P, void* d_grid, int direction) {
 
 static int64_t nh_of(const Geom& g) { return (int64_t)g.nhx * g.nhy * g.nhz; }
 
+// one-plane 2-D transform used by the memory-limited mode
+static int fft_one_plane(cg_plan_s* P, void* d_plane, int direction) {
+  const Geom& g = P->geom;
+  if (!P->fft1_valid || P->fft1_nf1 != g.nf1 || P->fft1_nf2 != g.nf2) {
+    if (P->fft1_valid) cufftDestroy(P->fft1);
+    P->fft1_valid = false;
+    CG_CUFFT(cufftPlan2d(&P->fft1, g.nf2, g.nf1,
+                         P->precision == CG_PREC_FP64 ? CUFFT_Z2Z : CUFFT_C2C));
+    P->fft1_valid = true;
+    P->fft1_nf1 = g.nf1;
+    P->fft1_nf2 = g.nf2;
+  }
+  return exec_c2c(P, P->fft1, d_plane, direction);
+}
+
+// Memory-limited ms2dirty after the sorted stream: per plane window, spread
+// the window's taps, transform its planes and add its share of the w-DFT to
+// an FP64 accumulator image; the per-pixel corrections come last.
+template <typename T>
+static int ms2dirty_windows(cg_plan_s* P, T* d_dirty) {
+  const Geom& g = P->geom;
+  cudaStream_t st = P->stream;
+  const size_t plane = (size_t)g.nf1 * g.nf2;
+  const size_t npix = (size_t)g.N1 * g.N2;
+  CG_TRY(ensure(P->acc, npix * 16));
+  CG_CUDA(cudaMemsetAsync(P->acc.p, 0, npix * 16, st));
+  T* fwb = (T*)P->grid.p;
+  for (int p0 = 0; p0 < g.nw; p0 += P->plane_batch) {
+    const int p1 = std::min(g.nw, p0 + P->plane_batch);
+    CG_TRY(launch_grid_window<T>((const Rec<T>*)P->recs.p, P->nrow, g, p0, p1, fwb, st));
+    for (int p = p0; p < p1; p++) CG_TRY(fft_one_plane(P, fwb + 2 * (p - p0) * plane, CUFFT_INVERSE));
+    CG_TRY(launch_wdft_window<T>(fwb, g, p0, p1, (const double*)P->zq.p, (double*)P->acc.p, st));
+  }
+  return launch_wdft_finish<T>((const double*)P->acc.p, g, (const double*)P->K1.p,
+                               (const double*)P->K2.p, (const double*)P->K3q.p,
+                               (const double*)P->zq.p, d_dirty, st);
+}
+
+// Memory-limited dirty2ms after the sorted stream: per plane window, fill,
+// transform and add each row's window share into vis (zeroed first).
+template <typename T>
+static int dirty2ms_windows(cg_plan_s* P, const T* d_dirty, T* d_vis) {
+  const Geom& g = P->geom;
+  cudaStream_t st = P->stream;
+  const size_t plane = (size_t)g.nf1 * g.nf2;
+  CG_CUDA(cudaMemsetAsync(d_vis, 0, (size_t)P->nrow * 2 * sizeof(T), st));
+  T* fwb = (T*)P->grid.p;
+  for (int p0 = 0; p0 < g.nw; p0 += P->plane_batch) {
+    const int p1 = std::min(g.nw, p0 + P->plane_batch);
+    CG_TRY(launch_plane_fill_window<T>(d_dirty, g, p0, p1, (const double*)P->K1.p,
+                                       (const double*)P->K2.p, (const double*)P->K3q.p,
+                                       (const double*)P->zq.p, fwb, st));
+    for (int p = p0; p < p1; p++) CG_TRY(fft_one_plane(P, fwb + 2 * (p - p0) * plane, CUFFT_FORWARD));
+    CG_TRY(launch_degrid_window<T>((const Rec<T>*)P->recs.p, (const int*)P->perm.p, P->nrow, g,
+                                   p0, p1, fwb, d_vis, st));
+  }
+  return CG_OK;
+}
+
 template <typename T>
 static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T* d_wgt,
                       T* d_dirty) {
@@ -573,6 +645,13 @@ static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T
   CG_TRY(launch_build_stream<T>((const int*)P->perm.p, M, d_uvw, d_vis, d_wgt, g, true,
                                 (Rec<T>*)P->recs_tmp.p, (Rec<T>*)P->recs.p, st));
   timer_mark(P);  // 3: sorted stream
+  if (P->plane_batch) {  // memory-limited mode: gridding, FFT and w-DFT per plane window
+    CG_TRY(ms2dirty_windows<T>(P, d_dirty));
+    timer_mark(P);  // 4: gridding (all windows)
+    timer_mark(P);  // 5: FFT (inside the windows)
+    timer_mark(P);  // 6
+    return CG_OK;
+  }
   CG_TRY(launch_grid<T>((const Rec<T>*)P->recs.p, (const int*)P->hive_start.p, M, g,
                         (T*)P->grid.p, P->grid_method, queue_counter(P), st));
   timer_mark(P);  // 4: gridding
@@ -601,6 +680,13 @@ static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const
                     (int*)P->hive_start.p + (nh_of(g) + 1)));
   timer_mark(P);  // 2: binning
   if (P->stop_stage == 1) return CG_OK;
+  if (P->plane_batch) {  // memory-limited mode: fill, FFT and degridding per plane window
+    CG_TRY(launch_build_stream<T>((const int*)P->perm.p, M, d_uvw, (const T*)nullptr, d_wgt, g,
+                                  false, (Rec<T>*)P->recs_tmp.p, (Rec<T>*)P->recs.p, st));
+    CG_TRY(dirty2ms_windows<T>(P, d_dirty, d_vis));
+    for (int i = 0; i < 4; i++) timer_mark(P);  // stages 3-6 are inside the windows
+    return CG_OK;
+  }
   CG_TRY(launch_plane_fill<T>(d_dirty, g, (const double*)P->K1.p, (const double*)P->K2.p,
                               (const double*)P->K3q.p, (const double*)P->zq.p, (T*)P->grid.p, st));
   timer_mark(P);  // 3: plane fill

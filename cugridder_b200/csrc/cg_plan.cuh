@@ -54,7 +54,7 @@ struct cg_plan_s {
   double poly[cg::kMaxW * cg::kPolyCoef] = {};
   // device buffers
   cg_dev_buf mm, K1, K2, K3q, zq, grid, recs, perm, skeys, hive_start, binws, fftwork, io_uvw,
-      io_vis, io_wgt, io_dirty, polyf, polyd, recs_tmp, chan_uvw, chan_scale, coltw;
+      io_vis, io_wgt, io_dirty, polyf, polyd, recs_tmp, chan_uvw, chan_scale, coltw, acc;
   unsigned long long* h_mm = nullptr;  // pinned, 2 words + flag
   // cuFFT: full 2-D batched plan, and the 1-D plans of the band-pruned path
   cufftHandle fft = 0;
@@ -67,6 +67,13 @@ struct cg_plan_s {
   int fft_pruning = 1;  // 0: always the full 2-D transform (CG_FFT_PRUNE=0)
   int col_fft = 1;      // 0: cuFFT for the column transforms too (CG_COL_FFT=0)
   int coltw_n = 0;      // length of the twiddle table in coltw
+  // memory-limited mode (cg_plan_set_grid_budget): the grid holds plane_batch
+  // planes at a time when the whole grid exceeds grid_budget bytes
+  size_t grid_budget = 0;
+  int plane_batch = 0;  // 0: the whole grid is resident
+  cufftHandle fft1 = 0; // one-plane 2-D transform of the memory-limited mode
+  bool fft1_valid = false;
+  int fft1_nf1 = 0, fft1_nf2 = 0;
   cg_stage_timer timer;
   std::mutex mu;
 };

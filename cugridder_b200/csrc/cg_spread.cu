@@ -822,6 +822,143 @@ int launch_degrid(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_sta
 #undef CG_DEGRID_CALL
 }
 
+// ================================================================ plane windows
+// Memory-limited mode: the grid holds only planes [p0, p1) (plane p at
+// fwb + (p - p0) * plane).  Spreading skips taps outside the window; the
+// interpolation adds each window's share of a row into vis, so a call
+// visits every window once.  Sorted-stream order, one row per thread.
+template <typename T, int W>
+__global__ void __launch_bounds__(256) k_grid_window(const Rec<T>* __restrict__ recs, int64_t M,
+                                                     Geom g, int p0, int p1, T* __restrict__ fwb) {
+  const T beta = (T)g.beta, c = (T)g.es_c;
+  const T* __restrict__ poly = geom_poly<T>(g);
+  const int nf1 = g.nf1, nf2 = g.nf2, nw = g.nw;
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < M;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    const Rec<T> r = recs[s];
+    T kx[W], ky[W], kz[W];
+    const int bx = (int)(r.bxy & 0xFFFFu), by = (int)(r.bxy >> 16), bz = (int)r.bz;
+    if (bx >= nf1 || by >= nf2 || bz >= nw) continue;
+    const int oz = bz + taps<T, W>(r.f[2], beta, c, poly, kz);
+    bool any = false;
+#pragma unroll
+    for (int a = 0; a < W; a++) {
+      const int zz = wrapi(oz + a, nw);
+      any |= zz >= p0 && zz < p1;
+    }
+    if (!any) continue;
+    const int ox = bx + taps<T, W>(r.f[0], beta, c, poly, kx);
+    const int oy = by + taps<T, W>(r.f[1], beta, c, poly, ky);
+#pragma unroll 1
+    for (int a = 0; a < W; a++) {
+      const int zz = wrapi(oz + a, nw);
+      if (zz < p0 || zz >= p1) continue;
+      const T cr = r.c[0] * kz[a], ci = r.c[1] * kz[a];
+#pragma unroll 1
+      for (int b = 0; b < W; b++) {
+        const int yy = wrapi(oy + b, nf2);
+        const T vr = cr * ky[b], vi = ci * ky[b];
+        T* row = fwb + 2 * (((size_t)(zz - p0) * nf2 + yy) * nf1);
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+          const int xx = wrapi(ox + e, nf1);
+          atomicAdd(row + 2 * xx, vr * kx[e]);
+          atomicAdd(row + 2 * xx + 1, vi * kx[e]);
+        }
+      }
+    }
+  }
+}
+
+template <typename T, int W>
+__global__ void __launch_bounds__(256) k_degrid_window(const Rec<T>* __restrict__ recs,
+                                                       const int* __restrict__ perm, int64_t M,
+                                                       Geom g, int p0, int p1,
+                                                       const T* __restrict__ fwb,
+                                                       T* __restrict__ vis) {
+  const T beta = (T)g.beta, c = (T)g.es_c;
+  const T* __restrict__ poly = geom_poly<T>(g);
+  const int nf1 = g.nf1, nf2 = g.nf2, nw = g.nw;
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < M;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    const Rec<T> r = recs[s];
+    T kx[W], ky[W], kz[W];
+    const int bx = (int)(r.bxy & 0xFFFFu), by = (int)(r.bxy >> 16), bz = (int)r.bz;
+    if (bx >= nf1 || by >= nf2 || bz >= nw) continue;
+    const int oz = bz + taps<T, W>(r.f[2], beta, c, poly, kz);
+    bool any = false;
+#pragma unroll
+    for (int a = 0; a < W; a++) {
+      const int zz = wrapi(oz + a, nw);
+      any |= zz >= p0 && zz < p1;
+    }
+    if (!any) continue;
+    const int ox = bx + taps<T, W>(r.f[0], beta, c, poly, kx);
+    const int oy = by + taps<T, W>(r.f[1], beta, c, poly, ky);
+    T sr = 0, si = 0;
+#pragma unroll 1
+    for (int a = 0; a < W; a++) {
+      const int zz = wrapi(oz + a, nw);
+      if (zz < p0 || zz >= p1) continue;
+      T pr = 0, pi = 0;
+#pragma unroll 1
+      for (int b = 0; b < W; b++) {
+        const int yy = wrapi(oy + b, nf2);
+        const T* row = fwb + 2 * (((size_t)(zz - p0) * nf2 + yy) * nf1);
+        T qr = 0, qi = 0;
+#pragma unroll
+        for (int e = 0; e < W; e++) {
+          const int xx = wrapi(ox + e, nf1);
+          qr += row[2 * xx] * kx[e];
+          qi += row[2 * xx + 1] * kx[e];
+        }
+        pr += qr * ky[b];
+        pi += qi * ky[b];
+      }
+      sr += pr * kz[a];
+      si += pi * kz[a];
+    }
+    const int64_t i = perm[s];
+    if (i < 0 || i >= M) continue;
+    vis[2 * i] += sr * r.c[0] - si * r.c[1];
+    vis[2 * i + 1] += sr * r.c[1] + si * r.c[0];
+  }
+}
+
+template <typename T>
+int launch_grid_window(const Rec<T>* d_recs, int64_t M, const Geom& g, int p0, int p1, T* d_fwb,
+                       cudaStream_t st) {
+  CG_CUDA(cudaMemsetAsync(d_fwb, 0, (size_t)(p1 - p0) * g.nf1 * g.nf2 * 2 * sizeof(T), st));
+  if (M == 0) return CG_OK;
+  const int blocks = (int)std::min<int64_t>((M + 255) / 256, 148 * 64);
+#define CG_GW_CALL(w)                                                              \
+  (k_grid_window<T, w><<<blocks, 256, 0, st>>>(d_recs, M, g, p0, p1, d_fwb),     \
+   count_launches(1), cudaGetLastError() == cudaSuccess ? CG_OK : CG_ERR_CUDA)
+  CG_W_SWITCH(g.kw, CG_GW_CALL)
+#undef CG_GW_CALL
+}
+
+template <typename T>
+int launch_degrid_window(const Rec<T>* d_recs, const int* d_perm, int64_t M, const Geom& g,
+                         int p0, int p1, const T* d_fwb, T* d_vis, cudaStream_t st) {
+  if (M == 0) return CG_OK;
+  const int blocks = (int)std::min<int64_t>((M + 255) / 256, 148 * 64);
+#define CG_DW_CALL(w)                                                                         \
+  (k_degrid_window<T, w><<<blocks, 256, 0, st>>>(d_recs, d_perm, M, g, p0, p1, d_fwb, d_vis), \
+   count_launches(1), cudaGetLastError() == cudaSuccess ? CG_OK : CG_ERR_CUDA)
+  CG_W_SWITCH(g.kw, CG_DW_CALL)
+#undef CG_DW_CALL
+}
+
+template int launch_grid_window<float>(const Rec<float>*, int64_t, const Geom&, int, int, float*,
+                                       cudaStream_t);
+template int launch_grid_window<double>(const Rec<double>*, int64_t, const Geom&, int, int,
+                                        double*, cudaStream_t);
+template int launch_degrid_window<float>(const Rec<float>*, const int*, int64_t, const Geom&, int,
+                                         int, const float*, float*, cudaStream_t);
+template int launch_degrid_window<double>(const Rec<double>*, const int*, int64_t, const Geom&,
+                                          int, int, const double*, double*, cudaStream_t);
+
 template TileCfg grid_tiling<float>(const Geom&, bool);
 template TileCfg grid_tiling<double>(const Geom&, bool);
 template int launch_grid<float>(const Rec<float>*, const int*, int64_t, const Geom&, float*, int,

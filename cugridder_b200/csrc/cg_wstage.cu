@@ -173,6 +173,140 @@ int launch_plane_fill(const T* d_dirty, const Geom& g, const double* d_K1, const
   return CG_OK;
 }
 
+// Memory-limited mode: the w-DFT of k_wdft_deconv split over plane windows.
+// acc[pixel] (FP64) += sum_{p in [p0, p1)} fwb[p - p0] exp(i zp (p - nw/2));
+// k_wdft_finish then applies the per-pixel correction.
+template <typename T>
+__global__ void k_wdft_accum(const T* __restrict__ fwb, Geom g, int p0, int p1,
+                             const double* __restrict__ zq, double2* __restrict__ acc) {
+  using V = typename Vec2<T>::type;
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = blockIdx.y;
+  if (col >= g.N1) return;
+  const size_t plane = (size_t)g.nf1 * g.nf2;
+  const size_t idx = (size_t)cmcl(row, g.N2, g.nf2) * g.nf1 + cmcl(col, g.N1, g.nf1);
+  const int dr = abs(row - g.N2 / 2), dc = abs(col - g.N1 / 2);
+  const double zp = (zq[dr * (g.N1 / 2 + 1) + dc] - g.o_center) * g.gamma * g.h;
+  double sn, cs, pr, pi;
+  sincos(zp, &sn, &cs);
+  sincos(zp * (double)(p0 - g.nw / 2), &pi, &pr);
+  double sr = 0.0, si = 0.0;
+  const V* f = reinterpret_cast<const V*>(fwb) + idx;
+  for (int p = p0; p < p1; p++) {
+    const V v = f[(size_t)(p - p0) * plane];
+    sr += (double)v.x * pr - (double)v.y * pi;
+    si += (double)v.x * pi + (double)v.y * pr;
+    const double t = pr * cs - pi * sn;
+    pi = pr * sn + pi * cs;
+    pr = t;
+  }
+  double2& a = acc[(size_t)row * g.N1 + col];
+  a.x += sr;
+  a.y += si;
+}
+
+template <typename T>
+__global__ void k_wdft_finish(const double2* __restrict__ acc, Geom g, const double* __restrict__ K1,
+                              const double* __restrict__ K2, const double* __restrict__ K3q,
+                              const double* __restrict__ zq, T* __restrict__ dirty) {
+  using V = typename Vec2<T>::type;
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = blockIdx.y;
+  if (col >= g.N1) return;
+  double fr, fi, zp;
+  pixel_factor(g, row, col, K1, K2, K3q, zq, 1.0, fr, fi, zp);
+  const double2 a = acc[(size_t)row * g.N1 + col];
+  V out;
+  out.x = (T)(a.x * fr - a.y * fi);
+  out.y = (T)(a.x * fi + a.y * fr);
+  reinterpret_cast<V*>(dirty)[(size_t)row * g.N1 + col] = out;
+}
+
+// planes [p0, p1) of k_plane_fill (plane p at fwb + (p - p0) * plane)
+template <typename T>
+__global__ void k_plane_fill_window(const T* __restrict__ dirty, Geom g, int p0, int p1,
+                                    const double* __restrict__ K1, const double* __restrict__ K2,
+                                    const double* __restrict__ K3q, const double* __restrict__ zq,
+                                    T* __restrict__ fwb) {
+  using V = typename Vec2<T>::type;
+  const int g0 = blockIdx.x * blockDim.x + threadIdx.x;
+  const int g1 = blockIdx.y;
+  if (g0 >= g.nf1) return;
+  const size_t plane = (size_t)g.nf1 * g.nf2;
+  V* f = reinterpret_cast<V*>(fwb) + (size_t)g1 * g.nf1 + g0;
+  const int col = inv_cmcl(g0, g.N1, g.nf1), row = inv_cmcl(g1, g.N2, g.nf2);
+  if (col < 0 || row < 0) {
+    V zero;
+    zero.x = (T)0;
+    zero.y = (T)0;
+    for (int p = p0; p < p1; p++) f[(size_t)(p - p0) * plane] = zero;
+    return;
+  }
+  double fr, fi, zp;
+  pixel_factor(g, row, col, K1, K2, K3q, zq, -1.0, fr, fi, zp);
+  const V d = reinterpret_cast<const V*>(dirty)[(size_t)row * g.N1 + col];
+  const double br = (double)d.x * fr - (double)d.y * fi;
+  const double bi = (double)d.x * fi + (double)d.y * fr;
+  double sn, cs, pr, pi;
+  sincos(-zp, &sn, &cs);
+  sincos(-zp * (double)(p0 - g.nw / 2), &pi, &pr);
+  for (int p = p0; p < p1; p++) {
+    V o;
+    o.x = (T)(br * pr - bi * pi);
+    o.y = (T)(br * pi + bi * pr);
+    f[(size_t)(p - p0) * plane] = o;
+    const double t = pr * cs - pi * sn;
+    pi = pr * sn + pi * cs;
+    pr = t;
+  }
+}
+
+template <typename T>
+int launch_wdft_window(const T* d_fwb, const Geom& g, int p0, int p1, const double* d_zq,
+                       double* d_acc, cudaStream_t st) {
+  dim3 grid((g.N1 + 127) / 128, g.N2);
+  k_wdft_accum<T><<<grid, 128, 0, st>>>(d_fwb, g, p0, p1, d_zq, (double2*)d_acc);
+  count_launches(1);
+  CG_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+template <typename T>
+int launch_wdft_finish(const double* d_acc, const Geom& g, const double* d_K1, const double* d_K2,
+                       const double* d_K3q, const double* d_zq, T* d_dirty, cudaStream_t st) {
+  dim3 grid((g.N1 + 127) / 128, g.N2);
+  k_wdft_finish<T><<<grid, 128, 0, st>>>((const double2*)d_acc, g, d_K1, d_K2, d_K3q, d_zq, d_dirty);
+  count_launches(1);
+  CG_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+template <typename T>
+int launch_plane_fill_window(const T* d_dirty, const Geom& g, int p0, int p1, const double* d_K1,
+                             const double* d_K2, const double* d_K3q, const double* d_zq, T* d_fwb,
+                             cudaStream_t st) {
+  dim3 grid((g.nf1 + 127) / 128, g.nf2);
+  k_plane_fill_window<T><<<grid, 128, 0, st>>>(d_dirty, g, p0, p1, d_K1, d_K2, d_K3q, d_zq, d_fwb);
+  count_launches(1);
+  CG_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+template int launch_wdft_window<float>(const float*, const Geom&, int, int, const double*, double*,
+                                       cudaStream_t);
+template int launch_wdft_window<double>(const double*, const Geom&, int, int, const double*,
+                                        double*, cudaStream_t);
+template int launch_wdft_finish<float>(const double*, const Geom&, const double*, const double*,
+                                       const double*, const double*, float*, cudaStream_t);
+template int launch_wdft_finish<double>(const double*, const Geom&, const double*, const double*,
+                                        const double*, const double*, double*, cudaStream_t);
+template int launch_plane_fill_window<float>(const float*, const Geom&, int, int, const double*,
+                                             const double*, const double*, const double*, float*,
+                                             cudaStream_t);
+template int launch_plane_fill_window<double>(const double*, const Geom&, int, int, const double*,
+                                              const double*, const double*, const double*,
+                                              double*, cudaStream_t);
+
 template int launch_wdft_deconv<float>(const float*, const Geom&, const double*, const double*,
                                        const double*, const double*, float*, cudaStream_t);
 template int launch_wdft_deconv<double>(const double*, const Geom&, const double*, const double*,

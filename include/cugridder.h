@@ -193,6 +193,14 @@ int cg_plan_set_kernel(cg_plan *plan, int kind, int W, const double *coef);
  * reference's behaviour.  No reference counterpart. */
 int cg_set_host_kernel(int kind, int W, const double *coef);
 
+/* Memory-limited mode (no reference counterpart; the reference's equivalent
+ * is its plane-cube loop, ra_exec.cu:292-389 / 522-613).  When the whole
+ * grid (nw planes) would exceed `bytes`, the plan keeps only as many planes
+ * as fit and runs gridding + FFT + w-DFT (ms2dirty) or plane fill + FFT +
+ * degridding (dirty2ms) window by window; results equal the resident path
+ * up to summation order.  0 (default) = no limit. */
+int cg_plan_set_grid_budget(cg_plan *plan, size_t bytes);
+
 /* Stops the next calls after a stage (testing): 0 = run to the end,
  * 1 = after binning, 2 = after gridding (ms2dirty) / plane fill (dirty2ms),
  * 3 = after the FFT. */
