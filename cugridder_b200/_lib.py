@@ -83,6 +83,7 @@ SIGNATURES = {
     "cg_plan_copy_buffer": (c_int, [c_void_p, c_int, c_void_p, c_size_t, ctypes.POINTER(c_size_t)]),
     "cg_plan_set_stop_stage": (c_int, [c_void_p, c_int]),
     "cg_plan_set_grid_budget": (c_int, [c_void_p, c_size_t]),
+    "cg_plan_set_fixed_uvw": (c_int, [c_void_p, c_int]),
     "cg_plan_set_method": (c_int, [c_void_p, c_int]),
     "cg_plan_set_timing": (c_int, [c_void_p, c_int]),
     "cg_plan_get_timing": (c_int, [c_void_p, c_int, ctypes.POINTER(c_double), c_int,
@@ -111,6 +112,11 @@ SIGNATURES = {
     "cg_nufft_execute": (c_int, [c_void_p, _PTR, _PTR]),
     "cg_nufft_get_info": (c_int, [c_void_p, ctypes.POINTER(c_int), _PTR]),
     "cg_nufft_destroy": (c_int, [c_void_p]),
+    "cg_batch_create": (c_int, [ctypes.POINTER(c_void_p), c_int, _PTR, c_double, c_double, c_int,
+                                c_int, c_void_p]),
+    "cg_batch_ms2dirty": (c_int, [c_void_p]),
+    "cg_batch_dirty2ms": (c_int, [c_void_p]),
+    "cg_batch_destroy": (c_int, [c_void_p]),
     "cg_release_cache": (c_int, []),
     "cg_last_error": (ctypes.c_char_p, []),
     "cg_kernel_launches": (ctypes.c_longlong, []),

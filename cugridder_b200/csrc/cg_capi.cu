@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -24,6 +25,42 @@ static thread_local std::string g_last_error;
 void set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
 static std::atomic<long long> g_launches{0};
 void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+cudaError_t kernel_occupancy(const void* func, int threads, size_t smem, int* per_sm) {
+  struct Key {
+    const void* f;
+    int t;
+    size_t s;
+    int dev;
+    bool operator<(const Key& o) const {
+      return f != o.f ? f < o.f : t != o.t ? t < o.t : s != o.s ? s < o.s : dev < o.dev;
+    }
+  };
+  static std::mutex mu;
+  static std::map<Key, int> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const Key k{func, threads, smem, dev};
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(k);
+    if (it != cache.end()) {
+      *per_sm = it->second;
+      return cudaSuccess;
+    }
+  }
+  if (smem > 48 * 1024) {
+    const cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  int n = 0;
+  const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, func, threads, smem);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  cache[k] = n;
+  *per_sm = n;
+  return cudaSuccess;
+}
 }  // namespace cg
 
 using cg::ensure;
@@ -428,10 +465,19 @@ int cg_set_host_kernel(int kind, int W, const double* coef) {
   return CG_OK;
 }
 
+int cg_plan_set_fixed_uvw(cg_plan* plan, int on) {
+  if (!plan) return CG_ERR_ARG;
+  std::lock_guard<std::mutex> lock(plan->mu);
+  plan->fixed_uvw = on != 0;
+  plan->bins_valid = false;
+  return CG_OK;
+}
+
 int cg_plan_set_grid_budget(cg_plan* plan, size_t bytes) {
   if (!plan) return CG_ERR_ARG;
   std::lock_guard<std::mutex> lock(plan->mu);
   plan->grid_budget = bytes;
+  plan->bins_valid = false;
   return CG_OK;
 }
 

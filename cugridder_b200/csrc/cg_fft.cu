@@ -192,14 +192,15 @@ template <int L>
 int launch_l(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, int c0b, int nb,
              int sign, const float2* tw, cudaStream_t st) {
   const size_t smem = (size_t)(pad16(L) + 16) * sizeof(float4);
-  CG_CUDA(cudaFuncSetAttribute(k_col_fft<L>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem));
   int per_sm = 0;
-  CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_col_fft<L>, kFftThreads, smem));
+  CG_CUDA(kernel_occupancy((const void*)k_col_fft<L>, kFftThreads, smem, &per_sm));
   if (per_sm < 1) return CG_ERR_ARG;
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
+  }
   const int64_t items = (int64_t)(na / 2 + nb / 2) * nplanes;
   const int blocks = (int)std::min<int64_t>(items, (int64_t)per_sm * sms);
   k_col_fft<L><<<blocks, kFftThreads, smem, st>>>(grid, nf1, plane, nplanes, c0a, na, c0b, nb,

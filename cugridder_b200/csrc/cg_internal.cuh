@@ -110,6 +110,11 @@ int dirty2ms_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw
   } while (0)
 
 namespace cg {
+// Dynamic shared-memory opt-in and blocks per SM of a kernel at a launch
+// shape, computed once and cached: later launches (including those recorded
+// while a stream is being captured into a CUDA graph) make no attribute or
+// occupancy queries.  Returns a CUDA error code.
+cudaError_t kernel_occupancy(const void* func, int threads, size_t smem, int* per_sm);
 void set_last_error(const char* msg);
 // number of kernels this library has launched (process-wide)
 void count_launches(long long n);

@@ -275,6 +275,7 @@ int plan_configure(cg_plan_s* P, int nx, int ny, double fov, double eps, double 
   P->sign = sign;
   P->precision = precision;
   P->eps_status = st;
+  P->bins_valid = false;
   P->kw = kw;
   P->beta = beta;
   P->es_c = c;
@@ -630,16 +631,17 @@ static int dirty2ms_windows(cg_plan_s* P, const T* d_dirty, T* d_vis) {
 
 template <typename T>
 static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T* d_wgt,
-                      T* d_dirty) {
+                      T* d_dirty, bool reuse) {
   const Geom& g = P->geom;
   cudaStream_t st = P->stream;
   int64_t M = P->nrow;
   timer_mark(P);  // stage 0: w range + geometry
-  CG_TRY(launch_quarter(g, P->quad, (double*)P->K3q.p, (double*)P->zq.p, st));
+  if (!reuse) CG_TRY(launch_quarter(g, P->quad, (double*)P->K3q.p, (double*)P->zq.p, st));
   timer_mark(P);  // 1: quarter tables
-  CG_TRY(launch_bin(d_uvw, M, g, P->key_bytes, P->binws.p, P->binws.cap, (int*)P->perm.p,
-                    P->skeys.p, (int*)P->hive_start.p, st,
-                    (int*)P->hive_start.p + (nh_of(g) + 1)));
+  if (!reuse)
+    CG_TRY(launch_bin(d_uvw, M, g, P->key_bytes, P->binws.p, P->binws.cap, (int*)P->perm.p,
+                      P->skeys.p, (int*)P->hive_start.p, st,
+                      (int*)P->hive_start.p + (nh_of(g) + 1)));
   timer_mark(P);  // 2: binning
   if (P->stop_stage == 1) return CG_OK;
   CG_TRY(launch_build_stream<T>((const int*)P->perm.p, M, d_uvw, d_vis, d_wgt, g, true,
@@ -668,16 +670,17 @@ static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T
 
 template <typename T>
 static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const T* d_wgt,
-                      T* d_vis) {
+                      T* d_vis, bool reuse) {
   const Geom& g = P->geom;
   cudaStream_t st = P->stream;
   int64_t M = P->nrow;
   timer_mark(P);  // stage 0: w range + geometry
-  CG_TRY(launch_quarter(g, P->quad, (double*)P->K3q.p, (double*)P->zq.p, st));
+  if (!reuse) CG_TRY(launch_quarter(g, P->quad, (double*)P->K3q.p, (double*)P->zq.p, st));
   timer_mark(P);  // 1: quarter tables
-  CG_TRY(launch_bin(d_uvw, M, g, P->key_bytes, P->binws.p, P->binws.cap, (int*)P->perm.p,
-                    P->skeys.p, (int*)P->hive_start.p, st,
-                    (int*)P->hive_start.p + (nh_of(g) + 1)));
+  if (!reuse)
+    CG_TRY(launch_bin(d_uvw, M, g, P->key_bytes, P->binws.p, P->binws.cap, (int*)P->perm.p,
+                      P->skeys.p, (int*)P->hive_start.p, st,
+                      (int*)P->hive_start.p + (nh_of(g) + 1)));
   timer_mark(P);  // 2: binning
   if (P->stop_stage == 1) return CG_OK;
   if (P->plane_batch) {  // memory-limited mode: fill, FFT and degridding per plane window
@@ -704,6 +707,18 @@ static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const
   return CG_OK;
 }
 
+// fixed-uvw mode: the last call's geometry and binning still describe this one
+static bool reuse_geometry(const cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw) {
+  return P->fixed_uvw && P->bins_valid && !P->timer.on && P->stop_stage == 0 &&
+         P->last_uvw == d_uvw && P->last_nrow == nrow && P->last_freq == freq;
+}
+static void remember_geometry(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw) {
+  P->bins_valid = P->fixed_uvw && P->stop_stage == 0;
+  P->last_uvw = d_uvw;
+  P->last_nrow = nrow;
+  P->last_freq = freq;
+}
+
 int ms2dirty_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw,
                     const void* d_vis, const void* d_wgt, void* d_dirty) {
   if (!d_dirty || (nrow > 0 && (!d_uvw || !d_vis))) {
@@ -711,16 +726,18 @@ int ms2dirty_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw
     return CG_ERR_ARG;
   }
   CG_CUDA(cudaSetDevice(P->device));
+  const bool reuse = reuse_geometry(P, nrow, freq, d_uvw);
   CG_TRY(timer_begin(P, 0));
-  CG_TRY(prepare(P, nrow, freq, d_uvw));
+  if (!reuse) CG_TRY(prepare(P, nrow, freq, d_uvw));
   size_t tsz = (P->precision == CG_PREC_FP64) ? 8 : 4;
   if (nrow == 0) {
     CG_CUDA(cudaMemsetAsync(d_dirty, 0, (size_t)P->nx * P->ny * 2 * tsz, P->stream));
     return P->eps_status;
   }
   int st = (P->precision == CG_PREC_FP64)
-               ? ms2dirty_t<double>(P, d_uvw, (const double*)d_vis, (const double*)d_wgt, (double*)d_dirty)
-               : ms2dirty_t<float>(P, d_uvw, (const float*)d_vis, (const float*)d_wgt, (float*)d_dirty);
+               ? ms2dirty_t<double>(P, d_uvw, (const double*)d_vis, (const double*)d_wgt, (double*)d_dirty, reuse)
+               : ms2dirty_t<float>(P, d_uvw, (const float*)d_vis, (const float*)d_wgt, (float*)d_dirty, reuse);
+  if (st == CG_OK) remember_geometry(P, nrow, freq, d_uvw);
   return st != CG_OK ? st : P->eps_status;
 }
 
@@ -731,12 +748,14 @@ int dirty2ms_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw
     return CG_ERR_ARG;
   }
   CG_CUDA(cudaSetDevice(P->device));
+  const bool reuse = reuse_geometry(P, nrow, freq, d_uvw);
   CG_TRY(timer_begin(P, 1));
-  CG_TRY(prepare(P, nrow, freq, d_uvw));
+  if (!reuse) CG_TRY(prepare(P, nrow, freq, d_uvw));
   if (nrow == 0) return P->eps_status;
   int st = (P->precision == CG_PREC_FP64)
-               ? dirty2ms_t<double>(P, d_uvw, (const double*)d_dirty, (const double*)d_wgt, (double*)d_vis)
-               : dirty2ms_t<float>(P, d_uvw, (const float*)d_dirty, (const float*)d_wgt, (float*)d_vis);
+               ? dirty2ms_t<double>(P, d_uvw, (const double*)d_dirty, (const double*)d_wgt, (double*)d_vis, reuse)
+               : dirty2ms_t<float>(P, d_uvw, (const float*)d_dirty, (const float*)d_wgt, (float*)d_vis, reuse);
+  if (st == CG_OK) remember_geometry(P, nrow, freq, d_uvw);
   return st != CG_OK ? st : P->eps_status;
 }
 

@@ -70,6 +70,14 @@ struct cg_plan_s {
   // memory-limited mode (cg_plan_set_grid_budget): the grid holds plane_batch
   // planes at a time when the whole grid exceeds grid_budget bytes
   size_t grid_budget = 0;
+  // fixed-uvw mode (cg_plan_set_fixed_uvw): calls with the same uvw pointer,
+  // nrow and freq as the last one reuse its geometry and binning (no host
+  // synchronisation, so such calls can be captured in a CUDA graph)
+  int fixed_uvw = 0;
+  bool bins_valid = false;
+  const double* last_uvw = nullptr;
+  int64_t last_nrow = -1;
+  double last_freq = 0;
   int plane_batch = 0;  // 0: the whole grid is resident
   cufftHandle fft1 = 0; // one-plane 2-D transform of the memory-limited mode
   bool fft1_valid = false;

@@ -728,9 +728,8 @@ static int grid_w(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, cons
   }
   WarpTile tc = warp_tiling<T>(g);
   auto* kern = geom_poly_host<T>(g) ? k_grid_warp<T, W, true> : k_grid_warp<T, W, false>;
-  CG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc.smem));
   int per_sm = 0;
-  CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, tc.warps * 32, tc.smem));
+  CG_CUDA(kernel_occupancy((const void*)kern, tc.warps * 32, tc.smem, &per_sm));
   if (per_sm < 1) {
     set_last_error("warp-tiled gridding does not fit on an SM");
     return CG_ERR_ARG;
@@ -757,11 +756,8 @@ static int degrid_w(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_s
   }
   TileCfg tc = grid_tiling<T>(g, true);
   int nslots = slots_for(tc.TY, tc.PB, W);
-  CG_CUDA(cudaFuncSetAttribute(k_degrid_tiled<T, W>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)tc.smem));
   int per_sm = 0;
-  CG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_degrid_tiled<T, W>, tc.threads,
-                                                        tc.smem));
+  CG_CUDA(kernel_occupancy((const void*)k_degrid_tiled<T, W>, tc.threads, tc.smem, &per_sm));
   if (per_sm < 1) {
     set_last_error("tiled degridding does not fit on an SM");
     return CG_ERR_ARG;

@@ -95,6 +95,10 @@ class Plan:
         a = np.ascontiguousarray(np.asarray(coef, dtype=np.float64).reshape(int(W), 8))
         _lib.check(self._lib.cg_plan_set_kernel(self._h, _lib.CG_KERNEL_POLY, int(W), a.ctypes.data))
 
+    def set_fixed_uvw(self, on=True):
+        """Reuse geometry and binning while uvw (same array), nrow and freq stay fixed."""
+        _lib.check(self._lib.cg_plan_set_fixed_uvw(self._h, 1 if on else 0))
+
     def set_grid_budget(self, nbytes):
         """Memory-limited mode: keep at most nbytes of w planes resident (0: no limit)."""
         _lib.check(self._lib.cg_plan_set_grid_budget(self._h, int(nbytes)))

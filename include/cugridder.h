@@ -201,6 +201,15 @@ int cg_set_host_kernel(int kind, int W, const double *coef);
  * up to summation order.  0 (default) = no limit. */
 int cg_plan_set_grid_budget(cg_plan *plan, size_t bytes);
 
+/* Fixed-uvw mode (no reference counterpart): the caller promises that the
+ * uvw array behind d_uvw does not change between calls.  A call whose d_uvw,
+ * nrow and freq equal the previous call's (either direction) then reuses its
+ * w range, geometry, quarter tables and binning: no host synchronisation and
+ * no allocation, so after one warm call the plan's calls can be captured in
+ * a CUDA graph on the plan's stream.  Off by default; per-stage timing
+ * disables the reuse. */
+int cg_plan_set_fixed_uvw(cg_plan *plan, int on);
+
 /* Stops the next calls after a stage (testing): 0 = run to the end,
  * 1 = after binning, 2 = after gridding (ms2dirty) / plane fill (dirty2ms),
  * 3 = after the FFT. */
@@ -306,6 +315,35 @@ int cg_nufft_setpts(cg_nufft *plan, int64_t M, const double *d_x, const double *
 int cg_nufft_execute(cg_nufft *plan, void *d_c, void *d_fk);
 int cg_nufft_get_info(const cg_nufft *plan, int *kw, int64_t *nf);
 int cg_nufft_destroy(cg_nufft *plan);
+
+/* ---------------- batched solves ----------------
+ * No reference counterpart (its C API images one dataset per call).  A batch
+ * images n independent datasets -- each with its own image size, field of
+ * view, rows and channels -- in one call.  All pointers of a dataset are
+ * DEVICE pointers that must stay valid (and uvw unchanged) for the life of
+ * the batch; vis / wgt are [nrow][nchan] (wgt may be NULL), freqs a HOST array
+ * of nchan frequencies (copied at creation).  ms2dirty sums a dataset's
+ * channels into its image; dirty2ms fills every (row, channel).  The first
+ * call per direction runs eagerly; the second is captured into a CUDA graph
+ * over the batch's streams and later calls replay it (CG_BATCH_GRAPH=0
+ * disables the graph).  Calls are ordered on `stream`. */
+typedef struct {
+    int64_t nrow;
+    int nchan;
+    const double *freqs;
+    int nxdirty, nydirty;
+    double fov;
+    const double *d_uvw;
+    void *d_vis;
+    const void *d_wgt;
+    void *d_dirty;
+} cg_dataset;
+typedef struct cg_batch_s cg_batch;
+int cg_batch_create(cg_batch **batch, int n, const cg_dataset *datasets, double epsilon,
+                    double sigma, int sign, int precision, void *stream);
+int cg_batch_ms2dirty(cg_batch *batch);
+int cg_batch_dirty2ms(cg_batch *batch);
+int cg_batch_destroy(cg_batch *batch);
 
 /* Host-pointer calls above keep one cached plan per precision so that
  * repeated calls reuse device workspace; this frees it. */
