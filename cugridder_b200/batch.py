@@ -1,6 +1,7 @@
 """Batched solves on device tensors: many datasets (own image size, fov,
-rows, channels) per call; the second call per direction is captured into a
-CUDA graph and later calls replay it.
+rows, channels) per call, all spread / interpolated by one persistent
+launch whose tiling is autotuned on the first call; the second call per
+direction is captured into a CUDA graph and later calls replay it.
 
     b = Batch([dict(uvw=uvw, freqs=[f0, f1], vis=vis, wgt=wgt, dirty=dirty, fov=2.0), ...],
               epsilon=1e-4, precision="fp32")
@@ -57,6 +58,15 @@ class Batch:
 
     def dirty2ms(self):
         _lib.check(self._lib.cg_batch_dirty2ms(self._h))
+
+    def tiling(self):
+        """Autotuned tiling: (gridding x, y, planes, warps), (degridding x,
+        y, planes, threads) and the winning launch times in ms (0 = default
+        / not tuned yet)."""
+        t = (ctypes.c_int * 8)()
+        ms = (ctypes.c_float * 2)()
+        _lib.check(self._lib.cg_batch_get_tiling(self._h, ctypes.addressof(t), ctypes.addressof(ms)))
+        return tuple(t[:4]), tuple(t[4:]), (ms[0], ms[1])
 
     def close(self):
         if getattr(self, "_h", None):

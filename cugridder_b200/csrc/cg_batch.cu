@@ -1,14 +1,25 @@
 // Batched solves: many independent datasets (each with its own image size,
-// field of view, row count and channels) imaged by one call.  Each dataset
-// gets a plan in fixed-uvw mode; the datasets are spread over a few
-// streams forked from the caller's stream, so small datasets overlap.  The
-// first call per direction runs eagerly (w ranges, geometry, binning,
-// allocation, cuFFT plans); the second is captured into a CUDA graph over
-// all streams and every later call replays that graph -- one launch for the
-// whole batch.  The reference has no batched entry point (its C API images
-// one dataset per call, cugridder.cu:541-571).
+// field of view, row count and channels) imaged by one call.  The reference
+// has no batched entry point (its C API images one dataset per call,
+// cugridder.cu:541-571).
+//
+// Each dataset gets a plan in fixed-uvw mode.  A call runs in three phases:
+//   1. per dataset, forked over a few streams: the stages before the
+//      spreading step (binning on the first call, the sorted stream; for
+//      dirty2ms also the plane fill and the FFT);
+//   2. ONE persistent launch that spreads (ms2dirty) or interpolates
+//      (dirty2ms) every dataset: CTAs / warps take (dataset, tile) items from
+//      a global work queue, so small datasets fill the gaps of large ones;
+//   3. ms2dirty only, per dataset: the FFT and the w-DFT with corrections.
+// Datasets whose call cannot be split (no rows, memory-limited windows) run
+// whole in phase 1.  The first call per direction runs eagerly and autotunes
+// the tiling of the phase-2 launch (tile size, plane batch, threads per
+// tile) by timing candidates on the batch's own data; the second call is
+// captured into a CUDA graph and every later call replays it.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <numeric>
 #include <vector>
 
 #include "cg_launch.cuh"
@@ -30,6 +41,14 @@ __global__ void k_chan_scale(const double* __restrict__ uvw, int64_t nrow, int n
   }
 }
 
+// autotuner candidates: gridding warp tiles (wx, wy, planes, warps) and
+// degridding tiles (dx, dy, planes, threads); the first of each is the default
+const int kGridCand[][4] = {{16, 16, 0, 0}, {16, 8, 0, 0},  {32, 16, 0, 0}, {16, 32, 0, 0},
+                            {32, 8, 0, 0},  {16, 16, 4, 0}, {16, 16, 12, 0}, {16, 16, 0, 4}};
+const int kDegridCand[][4] = {{32, 16, 0, 512}, {32, 32, 0, 512}, {32, 8, 0, 512},
+                              {16, 16, 0, 512}, {64, 16, 0, 512}, {32, 16, 0, 256},
+                              {16, 16, 0, 256}, {32, 16, 8, 512}};
+
 }  // namespace
 
 struct cg_batch_s {
@@ -45,9 +64,20 @@ struct cg_batch_s {
   cudaStream_t origin = nullptr;      // capture origin (the caller's stream may be the NULL stream)
   cudaEvent_t fork = nullptr;
   std::vector<cudaEvent_t> joins;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;  // autotuner timing
   cudaGraphExec_t exec[2] = {nullptr, nullptr};
   int calls[2] = {0, 0};
   int use_graph = 1;
+  int autotune = 1;
+  // phase 2: which datasets were split, their jobs (device array) and shape
+  std::vector<char> split[2];
+  std::vector<int> job_of[2];         // dataset index of each job
+  std::vector<unsigned char> host_jobs[2];
+  cg_dev_buf jobs[2], counter[2];
+  cg::MultiShape shape[2] = {};
+  bool jobs_ready[2] = {false, false};
+  cg::TileTune tune{};
+  float tuned_ms[2] = {0.f, 0.f};
 };
 
 namespace {
@@ -55,14 +85,19 @@ namespace {
 void destroy_batch(cg_batch_s* B) {
   if (!B) return;
   cudaSetDevice(B->device);
-  for (int d = 0; d < 2; d++)
+  for (int d = 0; d < 2; d++) {
     if (B->exec[d]) cudaGraphExecDestroy(B->exec[d]);
+    cg::release(B->jobs[d]);
+    cg::release(B->counter[d]);
+  }
   for (auto P : B->plans) cg_plan_destroy(P);
   for (auto& b : B->uvw_chan) cg::release(b);
   for (auto& b : B->scales) cg::release(b);
   for (auto s : B->streams) cudaStreamDestroy(s);
   if (B->origin) cudaStreamDestroy(B->origin);
   if (B->fork) cudaEventDestroy(B->fork);
+  if (B->t0) cudaEventDestroy(B->t0);
+  if (B->t1) cudaEventDestroy(B->t1);
   for (auto e : B->joins) cudaEventDestroy(e);
   delete B;
 }
@@ -70,24 +105,166 @@ void destroy_batch(cg_batch_s* B) {
 const double* rows_uvw(const cg_batch_s* B, size_t i) {
   return B->ds[i].nchan > 1 ? (const double*)B->uvw_chan[i].p : B->ds[i].d_uvw;
 }
+int64_t rows_of(const cg_dataset& d) { return d.nrow * (int64_t)std::max(1, d.nchan); }
 
-// every dataset's call, forked from `origin` over the batch streams and
-// joined back into it
-int run_all(cg_batch_s* B, int dir, cudaStream_t origin) {
+int fork_streams(cg_batch_s* B, cudaStream_t origin) {
   CG_CUDA(cudaEventRecord(B->fork, origin));
   for (auto s : B->streams) CG_CUDA(cudaStreamWaitEvent(s, B->fork, 0));
-  for (size_t i = 0; i < B->ds.size(); i++) {
-    const cg_dataset& d = B->ds[i];
-    cg_plan_s* P = B->plans[i];
-    P->stream = B->streams[i % B->streams.size()];
-    const int64_t rows = d.nrow * (int64_t)std::max(1, d.nchan);
-    const int st = dir == 0 ? cg::ms2dirty_device(P, rows, B->f0[i], rows_uvw(B, i), d.d_vis, d.d_wgt, d.d_dirty)
-                            : cg::dirty2ms_device(P, rows, B->f0[i], rows_uvw(B, i), d.d_dirty, d.d_wgt, d.d_vis);
-    if (st > 1) return st;
-  }
+  return CG_OK;
+}
+int join_streams(cg_batch_s* B, cudaStream_t origin) {
   for (size_t k = 0; k < B->streams.size(); k++) {
     CG_CUDA(cudaEventRecord(B->joins[k], B->streams[k]));
     CG_CUDA(cudaStreamWaitEvent(origin, B->joins[k], 0));
+  }
+  return CG_OK;
+}
+
+// Jobs of the split datasets for tiling tt, heaviest rows-per-item first so
+// that the queue ends on light items; fills the shape.
+template <typename T>
+int build_jobs(cg_batch_s* B, int dir, const cg::TileTune& tt, std::vector<cg::GridJob<T>>& jobs,
+               std::vector<int>& order, cg::MultiShape* shape) {
+  jobs.clear();
+  order.clear();
+  for (size_t i = 0; i < B->ds.size(); i++) {
+    if (!B->split[dir][i]) continue;
+    cg::GridJob<T> J{};
+    CG_TRY(cg::plan_grid_job<T>(B->plans[i], tt, (T*)B->ds[i].d_vis, &J));
+    jobs.push_back(J);
+    order.push_back((int)i);
+  }
+  if (jobs.empty()) return CG_OK;
+  std::vector<size_t> idx(jobs.size());
+  std::iota(idx.begin(), idx.end(), 0);
+  auto density = [&](size_t k) {
+    const int items = dir == 0 ? jobs[k].wt.nitems : jobs[k].dt.nitems;
+    return (double)jobs[k].M / std::max(1, items);
+  };
+  std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return density(a) > density(b); });
+  std::vector<cg::GridJob<T>> sorted;
+  std::vector<int> sorted_order;
+  for (size_t k : idx) {
+    sorted.push_back(jobs[k]);
+    sorted_order.push_back(order[k]);
+  }
+  jobs.swap(sorted);
+  order.swap(sorted_order);
+  return cg::multi_shape<T>(jobs.data(), (int)jobs.size(), shape);
+}
+
+template <typename T>
+int upload_jobs(cg_batch_s* B, int dir, const std::vector<cg::GridJob<T>>& jobs, cudaStream_t st) {
+  const size_t bytes = sizeof(cg::GridJob<T>) * std::max<size_t>(1, jobs.size());
+  // the host copy stays alive until the batch is destroyed
+  B->host_jobs[dir].resize(bytes);
+  if (!jobs.empty()) std::memcpy(B->host_jobs[dir].data(), jobs.data(), sizeof(cg::GridJob<T>) * jobs.size());
+  CG_TRY(cg::ensure(B->jobs[dir], bytes));
+  CG_TRY(cg::ensure(B->counter[dir], 256));
+  if (!jobs.empty())
+    CG_CUDA(cudaMemcpyAsync(B->jobs[dir].p, B->host_jobs[dir].data(),
+                            sizeof(cg::GridJob<T>) * jobs.size(), cudaMemcpyHostToDevice, st));
+  return CG_OK;
+}
+
+template <typename T>
+int launch_phase2(cg_batch_s* B, int dir, int njobs, const cg::MultiShape& sh, cudaStream_t st) {
+  const auto* d_jobs = (const cg::GridJob<T>*)B->jobs[dir].p;
+  int* counter = (int*)B->counter[dir].p;
+  return dir == 0 ? cg::launch_grid_multi<T>(d_jobs, njobs, sh, counter, st)
+                  : cg::launch_degrid_multi<T>(d_jobs, njobs, sh, counter, st);
+}
+
+void set_tune(cg::TileTune& tt, int dir, const int* c) {
+  if (dir == 0) {
+    tt.wx = c[0]; tt.wy = c[1]; tt.wpb = c[2]; tt.warps = c[3];
+  } else {
+    tt.dx = c[0]; tt.dy = c[1]; tt.dpb = c[2]; tt.dthreads = c[3];
+  }
+}
+
+// First call of a direction (eager): time every candidate tiling of the
+// phase-2 launch on the batch's data (each launch rewrites its whole output,
+// so the repeats are harmless), keep the fastest, upload its jobs.
+template <typename T>
+int prepare_phase2(cg_batch_s* B, int dir, cudaStream_t st) {
+  std::vector<cg::GridJob<T>> jobs;
+  std::vector<int> order;
+  cg::MultiShape sh{};
+  if (B->autotune) {
+    const int ncand = dir == 0 ? (int)(sizeof(kGridCand) / sizeof(kGridCand[0]))
+                               : (int)(sizeof(kDegridCand) / sizeof(kDegridCand[0]));
+    float best = -1.f;
+    cg::TileTune best_tt = B->tune;
+    for (int c = 0; c < ncand; c++) {
+      cg::TileTune tt = B->tune;
+      set_tune(tt, dir, dir == 0 ? kGridCand[c] : kDegridCand[c]);
+      if (build_jobs<T>(B, dir, tt, jobs, order, &sh) != CG_OK || jobs.empty()) continue;
+      CG_TRY(upload_jobs<T>(B, dir, jobs, st));
+      float ms = 0.f;
+      bool ok = true;
+      for (int rep = 0; rep < 2 && ok; rep++) {  // the first launch warms up
+        CG_CUDA(cudaEventRecord(B->t0, st));
+        ok = launch_phase2<T>(B, dir, (int)jobs.size(), sh, st) == CG_OK;
+        CG_CUDA(cudaEventRecord(B->t1, st));
+        CG_CUDA(cudaEventSynchronize(B->t1));
+        CG_CUDA(cudaEventElapsedTime(&ms, B->t0, B->t1));
+      }
+      if (!ok) continue;  // a candidate that does not fit on an SM launched nothing
+      if (best < 0.f || ms < best) {
+        best = ms;
+        best_tt = tt;
+      }
+    }
+    B->tune = best_tt;
+    B->tuned_ms[dir] = std::max(best, 0.f);
+  }
+  CG_TRY(build_jobs<T>(B, dir, B->tune, jobs, order, &sh));
+  CG_TRY(upload_jobs<T>(B, dir, jobs, st));
+  B->job_of[dir] = order;
+  B->shape[dir] = sh;
+  B->jobs_ready[dir] = true;
+  return CG_OK;
+}
+
+// One call: phase 1 per dataset over the batch streams, phase 2 as one
+// launch on `origin`, phase 3 (ms2dirty) per dataset again.
+int run_all(cg_batch_s* B, int dir, cudaStream_t origin) {
+  const bool fp64 = B->precision == CG_PREC_FP64;
+  const size_t n = B->ds.size();
+  std::vector<char> split(n, 0);
+  CG_TRY(fork_streams(B, origin));
+  for (size_t i = 0; i < n; i++) {
+    const cg_dataset& d = B->ds[i];
+    cg_plan_s* P = B->plans[i];
+    P->stream = B->streams[i % B->streams.size()];
+    bool sp = false;
+    const int st = dir == 0 ? cg::ms2dirty_split(P, 1, rows_of(d), B->f0[i], rows_uvw(B, i), d.d_vis,
+                                                 d.d_wgt, d.d_dirty, &sp)
+                            : cg::dirty2ms_split(P, rows_of(d), B->f0[i], rows_uvw(B, i), d.d_dirty,
+                                                 d.d_wgt, d.d_vis, &sp);
+    if (st > 1) return st;
+    split[i] = sp;
+  }
+  CG_TRY(join_streams(B, origin));
+  if (!B->jobs_ready[dir]) {
+    B->split[dir] = split;
+    CG_TRY(fp64 ? prepare_phase2<double>(B, dir, origin) : prepare_phase2<float>(B, dir, origin));
+  } else if (split != B->split[dir]) {
+    cg::set_last_error("batch: the datasets' split pattern changed between calls");
+    return CG_ERR_ARG;
+  }
+  const int njobs = (int)B->job_of[dir].size();
+  CG_TRY(fp64 ? launch_phase2<double>(B, dir, njobs, B->shape[dir], origin)
+              : launch_phase2<float>(B, dir, njobs, B->shape[dir], origin));
+  if (dir == 0 && njobs > 0) {
+    CG_TRY(fork_streams(B, origin));
+    for (int i : B->job_of[0]) {
+      const cg_dataset& d = B->ds[i];
+      CG_TRY(cg::ms2dirty_split(B->plans[i], 2, rows_of(d), B->f0[i], rows_uvw(B, i), d.d_vis,
+                                d.d_wgt, d.d_dirty, nullptr));
+    }
+    CG_TRY(join_streams(B, origin));
   }
   return CG_OK;
 }
@@ -108,6 +285,7 @@ int cg_batch_create(cg_batch_s** batch, int n, const cg_dataset* ds, double epsi
   B->uvw_chan.resize(n);
   B->scales.resize(n);
   if (const char* e = getenv("CG_BATCH_GRAPH")) B->use_graph = atoi(e) != 0;
+  if (const char* e = getenv("CG_BATCH_AUTOTUNE")) B->autotune = atoi(e) != 0;
   int rc = CG_OK;
   for (int i = 0; i < n && rc <= 1; i++) {
     const cg_dataset& d = B->ds[i];
@@ -152,6 +330,8 @@ int cg_batch_create(cg_batch_s** batch, int n, const cg_dataset* ds, double epsi
   }
   if (rc <= 1 && cudaEventCreateWithFlags(&B->fork, cudaEventDisableTiming) != cudaSuccess)
     rc = CG_ERR_CUDA;
+  if (rc <= 1 && (cudaEventCreate(&B->t0) != cudaSuccess || cudaEventCreate(&B->t1) != cudaSuccess))
+    rc = CG_ERR_CUDA;
   if (rc <= 1 && cudaStreamCreateWithFlags(&B->origin, cudaStreamNonBlocking) != cudaSuccess)
     rc = CG_ERR_CUDA;
   if (rc > 1) {
@@ -166,7 +346,7 @@ static int batch_call(cg_batch_s* B, int dir) {
   if (!B) return CG_ERR_ARG;
   CG_CUDA(cudaSetDevice(B->device));
   const int k = B->calls[dir]++;
-  // first call: geometry, binning, plans
+  // first call: geometry, binning, plans, autotuning
   if (!B->use_graph || k == 0) return run_all(B, dir, B->stream);
   if (!B->exec[dir]) {
     // captured on the batch's own origin stream: the caller's stream may be
@@ -196,6 +376,19 @@ static int batch_call(cg_batch_s* B, int dir) {
 
 int cg_batch_ms2dirty(cg_batch_s* batch) { return batch_call(batch, 0); }
 int cg_batch_dirty2ms(cg_batch_s* batch) { return batch_call(batch, 1); }
+
+int cg_batch_get_tiling(const cg_batch_s* batch, int* tiling, float* tuned_ms) {
+  if (!batch || !tiling) return CG_ERR_ARG;
+  const cg::TileTune& t = batch->tune;
+  const int v[8] = {t.wx, t.wy, t.wpb, t.warps, t.dx, t.dy, t.dpb, t.dthreads};
+  for (int i = 0; i < 8; i++) tiling[i] = v[i];
+  if (tuned_ms) {
+    tuned_ms[0] = batch->tuned_ms[0];
+    tuned_ms[1] = batch->tuned_ms[1];
+  }
+  return CG_OK;
+}
+
 int cg_batch_destroy(cg_batch_s* batch) {
   destroy_batch(batch);
   return CG_OK;

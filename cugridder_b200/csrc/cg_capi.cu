@@ -49,14 +49,18 @@ cudaError_t kernel_occupancy(const void* func, int threads, size_t smem, int* pe
       return cudaSuccess;
     }
   }
-  if (smem > 48 * 1024) {
+  std::lock_guard<std::mutex> lk(mu);
+  // the opt-in only ever grows: every launch shape cached before stays valid
+  static std::map<std::pair<const void*, int>, size_t> opt_in;
+  size_t& cur = opt_in[{func, dev}];
+  if (smem > 48 * 1024 && smem > cur) {
     const cudaError_t e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    cur = smem;
   }
   int n = 0;
   const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, func, threads, smem);
   if (e != cudaSuccess) return e;
-  std::lock_guard<std::mutex> lk(mu);
   cache[k] = n;
   *per_sm = n;
   return cudaSuccess;

@@ -73,6 +73,23 @@ struct TileCfg {
   size_t smem;
 };
 
+// Warp-owned tiles of the gridding kernel: TX x TY cells times PB planes per
+// warp, cell (x, y, z) at z * PS + y * RS + x (complex units).
+struct WarpTile {
+  int TX, TY, PB, RS, PS, slots;
+  int ntx, nty, npb, nitems;
+  int warps;  // per CTA
+  size_t warp_bytes, smem;
+};
+
+// Tiling choices of one plan (0 = default): gridding warp tiles (wx x wy
+// cells, wpb planes, warps per CTA) and degridding tiles (dx x dy cells,
+// dpb planes, threads per CTA).
+struct TileTune {
+  int wx, wy, wpb, warps;
+  int dx, dy, dpb, dthreads;
+};
+
 // ---- pipeline entry points (cg_pipeline.cu) ----
 }  // namespace cg
 
@@ -83,6 +100,14 @@ int ms2dirty_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw
                     const void* d_vis, const void* d_wgt, void* d_dirty);
 int dirty2ms_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw,
                     const void* d_dirty, const void* d_wgt, void* d_vis);
+// Calls split at the spreading step (batched solves): ms2dirty part 1 runs
+// the stages before gridding, part 2 those after it; dirty2ms_split runs the
+// stages before degridding.  *split = false when the call ran whole (no
+// rows, memory-limited windows, a non-tiled method, timing or stop stages).
+int ms2dirty_split(cg_plan_s* P, int part, int64_t nrow, double freq, const double* d_uvw,
+                   const void* d_vis, const void* d_wgt, void* d_dirty, bool* split);
+int dirty2ms_split(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw,
+                   const void* d_dirty, const void* d_wgt, void* d_vis, bool* split);
 }  // namespace cg
 
 #define CG_CUDA(call)                                  \

@@ -36,14 +36,59 @@ constexpr int kGridMma = 2;  // tensor-core gridding (FP32, W <= 8); degridding 
 int launch_grid_mma(const Rec<float>* d_recs, const int* d_hive_start, const Geom& g, float* d_fw,
                     cudaStream_t st);
 template <typename T>
-TileCfg grid_tiling(const Geom& g, bool degrid);
+TileCfg grid_tiling(const Geom& g, bool degrid, const TileTune* tt = nullptr);
+template <typename T>
+WarpTile warp_tiling(const Geom& g, const TileTune* tt = nullptr);
+int degrid_slots(const TileCfg& tc, int W);
+
+// One grid of a multi-grid launch (batched solves): the plan's sorted stream,
+// hive offsets and grid, its tilings and its first work item in the launch.
+template <typename T>
+struct GridJob {
+  const Rec<T>* recs;
+  const int* hive_start;
+  const int* perm;
+  T* fw;
+  T* vis;  // degridding output (rows in the caller's order)
+  int64_t M;
+  Geom g;
+  WarpTile wt;
+  TileCfg dt;
+  int nslots;       // segment slots of the degridding tiles
+  int grid_item0;   // first gridding item of this job (prefix over jobs)
+  int degrid_item0; // first degridding item of this job
+};
+// Launch shape shared by all jobs of a multi-grid launch.
+struct MultiShape {
+  int kw;
+  bool poly;
+  int warps;          // gridding warps per CTA
+  size_t warp_bytes;  // gridding bytes per warp (largest of the jobs)
+  int threads;        // degridding threads per CTA
+  size_t dsmem;       // degridding bytes per CTA (largest of the jobs)
+  int grid_items, degrid_items;
+};
+// Fill the item prefixes and the shared shape of jobs (host array).
+template <typename T>
+int multi_shape(GridJob<T>* jobs, int njobs, MultiShape* shape);
+template <typename T>
+int launch_grid_multi(const GridJob<T>* d_jobs, int njobs, const MultiShape& sh, int* d_counter,
+                      cudaStream_t st);
+// the multi-grid job of a plan whose last call was split at its spreading
+// step (cg_plan.cuh's cg_plan_s; tilings from tt)
+template <typename T>
+int plan_grid_job(const cg_plan_s* P, const TileTune& tt, T* d_vis, GridJob<T>* job);
+template <typename T>
+int launch_degrid_multi(const GridJob<T>* d_jobs, int njobs, const MultiShape& sh, int* d_counter,
+                        cudaStream_t st);
+// tt: tiling choices (nullptr = defaults)
 template <typename T>
 int launch_grid(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, const Geom& g, T* d_fw,
-                int method, int* d_counter, cudaStream_t st);
+                int method, int* d_counter, cudaStream_t st, const TileTune* tt = nullptr);
 template <typename T>
 int launch_degrid(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_start, int64_t M,
                   const Geom& g, const T* d_fw, T* d_vis, int method, int* d_counter,
-                  cudaStream_t st);
+                  cudaStream_t st, const TileTune* tt = nullptr);
 
 // ---- column FFTs in shared memory (cg_fft.cu) ----
 bool col_fft_supported(int L, int na, int nb);

@@ -629,9 +629,25 @@ static int dirty2ms_windows(cg_plan_s* P, const T* d_dirty, T* d_vis) {
   return CG_OK;
 }
 
+// the stages after gridding: FFT, then w-DFT with the corrections
+template <typename T>
+static int ms2dirty_tail(cg_plan_s* P, T* d_dirty) {
+  const Geom& g = P->geom;
+  CG_TRY(fft_exec_pruned(P, P->grid.p, CUFFT_INVERSE));
+  timer_mark(P);  // 5: FFT
+  if (P->stop_stage == 3) return CG_OK;
+  CG_TRY(launch_wdft_deconv<T>((const T*)P->grid.p, g, (const double*)P->K1.p,
+                               (const double*)P->K2.p, (const double*)P->K3q.p,
+                               (const double*)P->zq.p, d_dirty, P->stream));
+  timer_mark(P);  // 6: w-DFT + corrections
+  return CG_OK;
+}
+
+// part 0: the whole call; 1: the stages before gridding; 2: those after it
 template <typename T>
 static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T* d_wgt,
-                      T* d_dirty, bool reuse) {
+                      T* d_dirty, bool reuse, int part = 0) {
+  if (part == 2) return ms2dirty_tail<T>(P, d_dirty);
   const Geom& g = P->geom;
   cudaStream_t st = P->stream;
   int64_t M = P->nrow;
@@ -654,23 +670,18 @@ static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T
     timer_mark(P);  // 6
     return CG_OK;
   }
+  if (part == 1) return CG_OK;
   CG_TRY(launch_grid<T>((const Rec<T>*)P->recs.p, (const int*)P->hive_start.p, M, g,
-                        (T*)P->grid.p, P->grid_method, queue_counter(P), st));
+                        (T*)P->grid.p, P->grid_method, queue_counter(P), st, &P->tune));
   timer_mark(P);  // 4: gridding
   if (P->stop_stage == 2) return CG_OK;
-  CG_TRY(fft_exec_pruned(P, P->grid.p, CUFFT_INVERSE));
-  timer_mark(P);  // 5: FFT
-  if (P->stop_stage == 3) return CG_OK;
-  CG_TRY(launch_wdft_deconv<T>((const T*)P->grid.p, g, (const double*)P->K1.p,
-                               (const double*)P->K2.p, (const double*)P->K3q.p,
-                               (const double*)P->zq.p, d_dirty, st));
-  timer_mark(P);  // 6: w-DFT + corrections
-  return CG_OK;
+  return ms2dirty_tail<T>(P, d_dirty);
 }
 
+// part 0: the whole call; 1: the stages before degridding
 template <typename T>
 static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const T* d_wgt,
-                      T* d_vis, bool reuse) {
+                      T* d_vis, bool reuse, int part = 0) {
   const Geom& g = P->geom;
   cudaStream_t st = P->stream;
   int64_t M = P->nrow;
@@ -700,9 +711,10 @@ static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const
   CG_TRY(launch_build_stream<T>((const int*)P->perm.p, M, d_uvw, (const T*)nullptr, d_wgt, g,
                                 false, (Rec<T>*)P->recs_tmp.p, (Rec<T>*)P->recs.p, st));
   timer_mark(P);  // 5: sorted stream
+  if (part == 1) return CG_OK;
   CG_TRY(launch_degrid<T>((const Rec<T>*)P->recs.p, (const int*)P->perm.p,
                           (const int*)P->hive_start.p, M, g, (const T*)P->grid.p, d_vis,
-                          P->grid_method, queue_counter(P), st));
+                          P->grid_method, queue_counter(P), st, &P->tune));
   timer_mark(P);  // 6: degridding
   return CG_OK;
 }
@@ -719,8 +731,22 @@ static void remember_geometry(cg_plan_s* P, int64_t nrow, double freq, const dou
   P->last_freq = freq;
 }
 
-int ms2dirty_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw,
-                    const void* d_vis, const void* d_wgt, void* d_dirty) {
+// A call can be split at its spreading step (batched solves): true when the
+// plan's mode has that step as one tiled launch over resident planes.
+static bool splittable(const cg_plan_s* P) {
+  return !P->plane_batch && P->grid_method == kGridTiled && !P->timer.on && P->stop_stage == 0;
+}
+
+static int ms2dirty_run(cg_plan_s* P, int part, int64_t nrow, double freq, const double* d_uvw,
+                        const void* d_vis, const void* d_wgt, void* d_dirty, bool* split) {
+  const bool fp64 = P->precision == CG_PREC_FP64;
+  if (part == 2) {
+    CG_CUDA(cudaSetDevice(P->device));
+    const int st = fp64 ? ms2dirty_t<double>(P, d_uvw, nullptr, nullptr, (double*)d_dirty, true, 2)
+                        : ms2dirty_t<float>(P, d_uvw, nullptr, nullptr, (float*)d_dirty, true, 2);
+    return st != CG_OK ? st : P->eps_status;
+  }
+  if (split) *split = false;
   if (!d_dirty || (nrow > 0 && (!d_uvw || !d_vis))) {
     set_last_error("null pointer");
     return CG_ERR_ARG;
@@ -729,20 +755,23 @@ int ms2dirty_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw
   const bool reuse = reuse_geometry(P, nrow, freq, d_uvw);
   CG_TRY(timer_begin(P, 0));
   if (!reuse) CG_TRY(prepare(P, nrow, freq, d_uvw));
-  size_t tsz = (P->precision == CG_PREC_FP64) ? 8 : 4;
+  size_t tsz = fp64 ? 8 : 4;
   if (nrow == 0) {
     CG_CUDA(cudaMemsetAsync(d_dirty, 0, (size_t)P->nx * P->ny * 2 * tsz, P->stream));
+    remember_geometry(P, nrow, freq, d_uvw);
     return P->eps_status;
   }
-  int st = (P->precision == CG_PREC_FP64)
-               ? ms2dirty_t<double>(P, d_uvw, (const double*)d_vis, (const double*)d_wgt, (double*)d_dirty, reuse)
-               : ms2dirty_t<float>(P, d_uvw, (const float*)d_vis, (const float*)d_wgt, (float*)d_dirty, reuse);
+  if (part == 1 && !splittable(P)) part = 0;
+  if (split) *split = part == 1;
+  int st = fp64 ? ms2dirty_t<double>(P, d_uvw, (const double*)d_vis, (const double*)d_wgt, (double*)d_dirty, reuse, part)
+                : ms2dirty_t<float>(P, d_uvw, (const float*)d_vis, (const float*)d_wgt, (float*)d_dirty, reuse, part);
   if (st == CG_OK) remember_geometry(P, nrow, freq, d_uvw);
   return st != CG_OK ? st : P->eps_status;
 }
 
-int dirty2ms_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw,
-                    const void* d_dirty, const void* d_wgt, void* d_vis) {
+static int dirty2ms_run(cg_plan_s* P, int part, int64_t nrow, double freq, const double* d_uvw,
+                        const void* d_dirty, const void* d_wgt, void* d_vis, bool* split) {
+  if (split) *split = false;
   if (!d_dirty || (nrow > 0 && (!d_uvw || !d_vis))) {
     set_last_error("null pointer");
     return CG_ERR_ARG;
@@ -751,12 +780,57 @@ int dirty2ms_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw
   const bool reuse = reuse_geometry(P, nrow, freq, d_uvw);
   CG_TRY(timer_begin(P, 1));
   if (!reuse) CG_TRY(prepare(P, nrow, freq, d_uvw));
-  if (nrow == 0) return P->eps_status;
+  if (nrow == 0) {
+    remember_geometry(P, nrow, freq, d_uvw);
+    return P->eps_status;
+  }
+  if (part == 1 && !splittable(P)) part = 0;
+  if (split) *split = part == 1;
   int st = (P->precision == CG_PREC_FP64)
-               ? dirty2ms_t<double>(P, d_uvw, (const double*)d_dirty, (const double*)d_wgt, (double*)d_vis, reuse)
-               : dirty2ms_t<float>(P, d_uvw, (const float*)d_dirty, (const float*)d_wgt, (float*)d_vis, reuse);
+               ? dirty2ms_t<double>(P, d_uvw, (const double*)d_dirty, (const double*)d_wgt, (double*)d_vis, reuse, part)
+               : dirty2ms_t<float>(P, d_uvw, (const float*)d_dirty, (const float*)d_wgt, (float*)d_vis, reuse, part);
   if (st == CG_OK) remember_geometry(P, nrow, freq, d_uvw);
   return st != CG_OK ? st : P->eps_status;
 }
+
+int ms2dirty_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw,
+                    const void* d_vis, const void* d_wgt, void* d_dirty) {
+  return ms2dirty_run(P, 0, nrow, freq, d_uvw, d_vis, d_wgt, d_dirty, nullptr);
+}
+
+int dirty2ms_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw,
+                    const void* d_dirty, const void* d_wgt, void* d_vis) {
+  return dirty2ms_run(P, 0, nrow, freq, d_uvw, d_dirty, d_wgt, d_vis, nullptr);
+}
+
+int ms2dirty_split(cg_plan_s* P, int part, int64_t nrow, double freq, const double* d_uvw,
+                   const void* d_vis, const void* d_wgt, void* d_dirty, bool* split) {
+  return ms2dirty_run(P, part, nrow, freq, d_uvw, d_vis, d_wgt, d_dirty, split);
+}
+
+int dirty2ms_split(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw,
+                   const void* d_dirty, const void* d_wgt, void* d_vis, bool* split) {
+  return dirty2ms_run(P, 1, nrow, freq, d_uvw, d_dirty, d_wgt, d_vis, split);
+}
+
+template <typename T>
+int plan_grid_job(const cg_plan_s* P, const TileTune& tt, T* d_vis, GridJob<T>* job) {
+  const Geom& g = P->geom;
+  GridJob<T> J{};
+  J.recs = (const Rec<T>*)P->recs.p;
+  J.hive_start = (const int*)P->hive_start.p;
+  J.perm = (const int*)P->perm.p;
+  J.fw = (T*)P->grid.p;
+  J.vis = d_vis;
+  J.M = P->nrow;
+  J.g = g;
+  J.wt = warp_tiling<T>(g, &tt);
+  J.dt = grid_tiling<T>(g, true, &tt);
+  J.nslots = degrid_slots(J.dt, g.kw);
+  *job = J;
+  return CG_OK;
+}
+template int plan_grid_job<float>(const cg_plan_s*, const TileTune&, float*, GridJob<float>*);
+template int plan_grid_job<double>(const cg_plan_s*, const TileTune&, double*, GridJob<double>*);
 
 }  // namespace cg

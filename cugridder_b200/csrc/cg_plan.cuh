@@ -46,6 +46,7 @@ struct cg_plan_s {
   int key_bytes = 4;
   int stop_stage = 0;
   int grid_method = 1;  // 0 direct, 1 tiled SIMT, 2 tensor-core (cg_plan_set_method, CG_GRID_METHOD)
+  cg::TileTune tune{};  // tiling of the tiled kernels (cg_plan_set_tiling; 0 = default)
   // gridding kernel: CG_KERNEL_ES (W from epsilon) or CG_KERNEL_POLY (W and
   // piecewise-polynomial coefficients given by cg_plan_set_kernel)
   int kernel_kind = CG_KERNEL_ES;

@@ -247,12 +247,6 @@ static int num_sms() {
 // along x.  Cell (x, y, z) of a warp tile lives at z*PS + y*RS + x (complex
 // units) with RS = 1 and PS = W (mod 16): the 16 lanes of a half-warp touch
 // 16 distinct 8-byte bank pairs.
-struct WarpTile {
-  int TX, TY, PB, RS, PS, slots;
-  int ntx, nty, npb, nitems;
-  int warps;  // per CTA
-  size_t warp_bytes, smem;
-};
 
 __device__ __forceinline__ int warp_excl_scan(int x, int& total) {
   const int lane = threadIdx.x & 31;
@@ -326,49 +320,62 @@ struct Cplx<float> { using type = float2; };
 template <>
 struct Cplx<double> { using type = double2; };
 
-template <typename T, int W, bool kPoly>
-__global__ void __launch_bounds__(256) k_grid_warp(const Rec<T>* __restrict__ recs,
-                                                   const int* __restrict__ hive_start, Geom g,
-                                                   WarpTile tc, T* __restrict__ fw) {
-  using C = typename Cplx<T>::type;
-  extern __shared__ __align__(16) unsigned char smem[];
-  constexpr int lo = Halo<W>::lo, hi = Halo<W>::hi;
-  constexpr int NP = W * W;                 // (dy, dz) tap pairs
-  constexpr int NR = (NP + 31) / 32;        // rounds of pairs
+// Lane layout constants of the warp-tiled spreading for support W.
+template <int W>
+struct WarpSpread {
+  static constexpr int NP = W * W;           // (dy, dz) tap pairs
+  static constexpr int NR = (NP + 31) / 32;  // rounds of pairs
   // The last, partly filled round of pairs leaves lanes idle for all W x
   // steps (W = 6: 4 of 36 pairs, 28 lanes idle).  When it is cheaper, those
   // REM pairs' REM * W taps are instead spread one tap per lane ("tail").
-  constexpr int NFULL = NP / 32, REM = NP % 32;
-  constexpr int NTAIL = (REM * W + 31) / 32;
-  constexpr bool kTail = REM > 0 && 12 * NTAIL < 12 + 5 * W;
-  constexpr int NRR = kTail ? NFULL : NR;  // rounds walked pair by pair
-  constexpr int NKV = (3 * W + 31) / 32;    // kernel-value registers per lane
-  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int TX = tc.TX, TY = tc.TY, PB = tc.PB, RS = tc.RS, PS = tc.PS;
-  C* acc = reinterpret_cast<C*>(smem + (size_t)wib * tc.warp_bytes);
-  int* tb = reinterpret_cast<int*>(reinterpret_cast<unsigned char*>(acc) + (size_t)PB * PS * sizeof(C));
-  const int ts = tc.slots + 1;
-  SegTable t{tb, tb + ts, tb + 2 * ts, tb + 3 * ts, tb + 4 * ts};
-  const T beta = (T)g.beta, c = (T)g.es_c, halfw = (T)W * (T)0.5;
-  // piecewise-polynomial kernel (kPoly): the coefficients of each lane's
-  // kernel-value slots (segment i of slot s = axis * W + i), loaded once
-  T pc[kPoly ? NKV : 1][kPolyCoef];
+  static constexpr int NFULL = NP / 32, REM = NP % 32;
+  static constexpr int NTAIL = (REM * W + 31) / 32;
+  static constexpr bool kTail = REM > 0 && 12 * NTAIL < 12 + 5 * W;
+  static constexpr int NRR = kTail ? NFULL : NR;  // rounds walked pair by pair
+  static constexpr int NKV = (3 * W + 31) / 32;   // kernel-value registers per lane
+};
+
+// piecewise-polynomial kernel (kPoly): the coefficients of each lane's
+// kernel-value slots (segment i of slot s = axis * W + i), loaded once per warp
+template <typename T, int W, bool kPoly>
+__device__ __forceinline__ void load_lane_poly(const T* __restrict__ poly,
+                                               T (&pc)[kPoly ? WarpSpread<W>::NKV : 1][kPolyCoef]) {
   if constexpr (kPoly) {
-    const T* __restrict__ poly = geom_poly<T>(g);
+    const int lane = threadIdx.x & 31;
 #pragma unroll
-    for (int k = 0; k < NKV; k++) {
+    for (int k = 0; k < WarpSpread<W>::NKV; k++) {
       const int sl = lane + 32 * k, i = sl % W;
 #pragma unroll
       for (int n = 0; n < kPolyCoef; n++) pc[k][n] = (sl < 3 * W) ? poly[i * kPolyCoef + n] : (T)0;
     }
   }
+}
+
+// One warp tile (work item `item` of tiling tc): accumulate the tile in the
+// warp's shared-memory region `wsmem` and write every cell of it to fw.
+template <typename T, int W, bool kPoly>
+__device__ __forceinline__ void grid_warp_tile(
+    const Rec<T>* __restrict__ recs, const int* __restrict__ hive_start, const Geom& g,
+    const WarpTile& tc, T* __restrict__ fw, int item, unsigned char* wsmem,
+    const T (&pc)[kPoly ? WarpSpread<W>::NKV : 1][kPolyCoef]) {
+  using C = typename Cplx<T>::type;
+  using WS = WarpSpread<W>;
+  constexpr int lo = Halo<W>::lo, hi = Halo<W>::hi;
+  constexpr int NP = WS::NP, NFULL = WS::NFULL, REM = WS::REM, NTAIL = WS::NTAIL;
+  constexpr bool kTail = WS::kTail;
+  constexpr int NRR = WS::NRR, NKV = WS::NKV;
+  const int lane = threadIdx.x & 31;
+  const int TX = tc.TX, TY = tc.TY, PB = tc.PB, RS = tc.RS, PS = tc.PS;
+  C* acc = reinterpret_cast<C*>(wsmem);
+  int* tb = reinterpret_cast<int*>(wsmem + (size_t)PB * PS * sizeof(C));
+  const int ts = tc.slots + 1;
+  SegTable t{tb, tb + ts, tb + 2 * ts, tb + 3 * ts, tb + 4 * ts};
+  const T beta = (T)g.beta, c = (T)g.es_c, halfw = (T)W * (T)0.5;
   const int nf1 = g.nf1, nf2 = g.nf2, nw = g.nw;
   const size_t plane = (size_t)nf1 * nf2;
-  const int gwarp = blockIdx.x * tc.warps + wib, nwarps = gridDim.x * tc.warps;
   C* fwc = reinterpret_cast<C*>(fw);
   const C zero = {(T)0, (T)0};
-
-  for (int item = gwarp; item < tc.nitems; item += nwarps) {
+  {
     const int tix = item % tc.ntx, tiy = (item / tc.ntx) % tc.nty, tib = item / (tc.ntx * tc.nty);
     const int tx0 = tix * TX, ty0 = tiy * TY, p0 = tib * PB;
     const int tx1 = min(tx0 + TX, nf1), ty1 = min(ty0 + TY, nf2), p1 = min(p0 + PB, nw);
@@ -383,7 +390,7 @@ __global__ void __launch_bounds__(256) k_grid_warp(const Rec<T>* __restrict__ re
         const int x = i % wx, y = (i / wx) % wy, z = i / (wx * wy);
         fwc[(size_t)(p0 + z) * plane + (size_t)(ty0 + y) * nf1 + tx0 + x] = zero;
       }
-      continue;
+      return;
     }
     for (int i = lane; i < PB * PS; i += 32) acc[i] = zero;
     __syncwarp();
@@ -549,15 +556,65 @@ __global__ void __launch_bounds__(256) k_grid_warp(const Rec<T>* __restrict__ re
   }
 }
 
-// ---------------------------------------------------------------- degridding
-template <typename T, int W>
-__global__ void __launch_bounds__(512) k_degrid_tiled(const Rec<T>* __restrict__ recs,
-                                                      const int* __restrict__ perm,
-                                                      const int* __restrict__ hive_start, int64_t M,
-                                                      Geom g, TileCfg tc, int nslots_max,
-                                                      const T* __restrict__ fw,
-                                                      T* __restrict__ vis, int* __restrict__ counter) {
+template <typename T, int W, bool kPoly>
+__global__ void __launch_bounds__(256) k_grid_warp(const Rec<T>* __restrict__ recs,
+                                                   const int* __restrict__ hive_start, Geom g,
+                                                   WarpTile tc, T* __restrict__ fw) {
   extern __shared__ __align__(16) unsigned char smem[];
+  const int wib = threadIdx.x >> 5;
+  T pc[kPoly ? WarpSpread<W>::NKV : 1][kPolyCoef];
+  load_lane_poly<T, W, kPoly>(geom_poly<T>(g), pc);
+  unsigned char* wsmem = smem + (size_t)wib * tc.warp_bytes;
+  const int gwarp = blockIdx.x * tc.warps + wib, nwarps = gridDim.x * tc.warps;
+  for (int item = gwarp; item < tc.nitems; item += nwarps)
+    grid_warp_tile<T, W, kPoly>(recs, hive_start, g, tc, fw, item, wsmem, pc);
+}
+
+// index of the job holding global work item `item` (item0 ascending, item0[0] = 0)
+template <typename J, typename F>
+__device__ __forceinline__ int find_job(const J* __restrict__ jobs, int njobs, int item, F item0) {
+  int lo = 0, hi = njobs;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (item0(jobs[mid]) <= item) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Many grids in one persistent launch: warps take (job, tile) items from a
+// global queue; every job shares W and the kernel.  warp_bytes is the largest
+// per-warp footprint of the jobs' tilings.
+template <typename T, int W, bool kPoly>
+__global__ void __launch_bounds__(256) k_grid_warp_multi(const GridJob<T>* __restrict__ jobs,
+                                                         int njobs, int nitems, size_t warp_bytes,
+                                                         int* __restrict__ counter) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  T pc[kPoly ? WarpSpread<W>::NKV : 1][kPolyCoef];
+  load_lane_poly<T, W, kPoly>(geom_poly<T>(jobs[0].g), pc);
+  unsigned char* wsmem = smem + (size_t)wib * warp_bytes;
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(counter, 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= nitems) break;
+    const int j = find_job(jobs, njobs, item, [](const GridJob<T>& x) { return x.grid_item0; });
+    const GridJob<T>& J = jobs[j];
+    grid_warp_tile<T, W, kPoly>(J.recs, J.hive_start, J.g, J.wt, J.fw, item - J.grid_item0, wsmem,
+                                pc);
+  }
+}
+
+// ---------------------------------------------------------------- degridding
+// One degridding tile (work item `item` of tiling tc), staged in `smem`.
+// Called by every thread of the block with the same item.
+template <typename T, int W>
+__device__ __forceinline__ void degrid_tile(const Rec<T>* __restrict__ recs,
+                                            const int* __restrict__ perm,
+                                            const int* __restrict__ hive_start, int64_t M,
+                                            const Geom& g, const TileCfg& tc, int nslots_max,
+                                            const T* __restrict__ fw, T* __restrict__ vis,
+                                            int item, unsigned char* smem, int* s_warp) {
   constexpr int lo = Halo<W>::lo, hi = Halo<W>::hi;
   const int TX = tc.TX, TY = tc.TY, PB = tc.PB;
   const int nw = g.nw, nf1 = g.nf1, nf2 = g.nf2;
@@ -569,17 +626,10 @@ __global__ void __launch_bounds__(512) k_degrid_tiled(const Rec<T>* __restrict__
   int* tb = (int*)(stg + 2 * (size_t)SXP * SY * SZ);
   const int ts = nslots_max + 1;
   SegTable t{tb, tb + ts, tb + 2 * ts, tb + 3 * ts, tb + 4 * ts};
-  __shared__ int s_warp[33];
-  __shared__ int s_item;
   const T beta = (T)g.beta, c = (T)g.es_c;
   const T* __restrict__ poly = geom_poly<T>(g);
   const size_t plane = (size_t)nf1 * nf2;
-
-  for (;;) {
-    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
-    __syncthreads();
-    const int item = s_item;
-    if (item >= tc.nitems) break;
+  {
     const int tix = item % tc.ntx, tiy = (item / tc.ntx) % tc.nty, tib = item / (tc.ntx * tc.nty);
     const int tx0 = tix * TX, ty0 = tiy * TY, p0 = all_planes ? 0 : tib * PB;
     const int tx1 = min(tx0 + TX, nf1), ty1 = min(ty0 + TY, nf2);
@@ -589,7 +639,7 @@ __global__ void __launch_bounds__(512) k_degrid_tiled(const Rec<T>* __restrict__
     const int nslots = build_segments(g, hive_start, tx0 >> 3, (tx1 - 1) >> 3, ty0 >> 3,
                                       (ty1 - 1) >> 3, p0, p1 - 1, t, s_warp);
     const int total = t.pref[nslots];
-    if (total == 0) continue;  // uniform across the block: nothing to interpolate here
+    if (total == 0) return;  // uniform across the block: nothing to interpolate here
     // stage the tile + halo (periodic); row stride SXP = SX + 1 complex
     using V = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
     V* stv = reinterpret_cast<V*>(stg);
@@ -638,6 +688,48 @@ __global__ void __launch_bounds__(512) k_degrid_tiled(const Rec<T>* __restrict__
   }
 }
 
+template <typename T, int W>
+__global__ void __launch_bounds__(512) k_degrid_tiled(const Rec<T>* __restrict__ recs,
+                                                      const int* __restrict__ perm,
+                                                      const int* __restrict__ hive_start, int64_t M,
+                                                      Geom g, TileCfg tc, int nslots_max,
+                                                      const T* __restrict__ fw,
+                                                      T* __restrict__ vis, int* __restrict__ counter) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_warp[33];
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= tc.nitems) break;
+    // the tile's first block-wide barrier orders this read before the next write of s_item
+    degrid_tile<T, W>(recs, perm, hive_start, M, g, tc, nslots_max, fw, vis, item, smem, s_warp);
+  }
+}
+
+// Many grids in one persistent launch: blocks take (job, tile) items from a
+// global queue; every job shares W and the kernel, smem is the largest
+// footprint of the jobs' tilings.
+template <typename T, int W>
+__global__ void __launch_bounds__(512, sizeof(T) == 4 ? 2 : 1) k_degrid_tiled_multi(const GridJob<T>* __restrict__ jobs,
+                                                            int njobs, int nitems,
+                                                            int* __restrict__ counter) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_warp[33];
+  __shared__ int s_item;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= nitems) break;
+    const int j = find_job(jobs, njobs, item, [](const GridJob<T>& x) { return x.degrid_item0; });
+    const GridJob<T>& J = jobs[j];
+    degrid_tile<T, W>(J.recs, J.perm, J.hive_start, J.M, J.g, J.dt, J.nslots, J.fw, J.vis,
+                      item - J.degrid_item0, smem, s_warp);
+  }
+}
+
 // ======================================================================= launch
 static int slots_for(int TY, int PB, int W) { return ((TY >> 3) + 2) * (PB + W + 1) * 3; }
 
@@ -645,16 +737,24 @@ static int slots_for(int TY, int PB, int W) { return ((TY >> 3) + 2) * (PB + W +
 // when the shared-memory footprint allows, otherwise halved until it fits.
 // CG_TILE_X / CG_TILE_Y / CG_TILE_PLANES / CG_TILE_THREADS override (tuning).
 template <typename T>
-TileCfg grid_tiling(const Geom& g, bool degrid) {
+TileCfg grid_tiling(const Geom& g, bool degrid, const TileTune* tt) {
   const size_t budget = 220 * 1024;
   const int W = g.kw;
   TileCfg tc{};
   // degridding: 32 x 16 tiles keep two CTAs per SM for FP32 at W <= 7 (one
   // stages its tile while the other interpolates); 32 x 32 left one CTA per SM
   int TX = env_int("CG_TILE_X", 32), TY = env_int("CG_TILE_Y", degrid ? 16 : 32);
+  int PB = env_int("CG_TILE_PLANES", 0);
+  int threads = env_int("CG_TILE_THREADS", 512);
+  if (tt && degrid) {
+    if (tt->dx > 0) TX = tt->dx;
+    if (tt->dy > 0) TY = tt->dy;
+    if (tt->dpb > 0) PB = tt->dpb;
+    if (tt->dthreads > 0) threads = tt->dthreads;
+  }
   TX = std::max(8, (TX / 8) * 8);
   TY = std::max(8, (TY / 8) * 8);
-  int PB = env_int("CG_TILE_PLANES", 0);
+  threads = std::min(512, std::max(64, (threads / 32) * 32));
   auto bytes = [&](int tx, int ty, int pb) -> size_t {
     size_t cells = degrid ? (size_t)(tx + W + 1) * (ty + W) * (pb >= g.nw ? g.nw : pb + W)
                           : (size_t)(tx + 8) * ty * pb;
@@ -677,21 +777,31 @@ TileCfg grid_tiling(const Geom& g, bool degrid) {
   tc.nty = (g.nf2 + TY - 1) / TY;
   tc.npb = (g.nw + PB - 1) / PB;
   tc.nitems = tc.ntx * tc.nty * tc.npb;
-  tc.threads = env_int("CG_TILE_THREADS", 512);
+  tc.threads = threads;
   tc.smem = bytes(TX, TY, PB);
   return tc;
 }
 
+int degrid_slots(const TileCfg& tc, int W) { return slots_for(tc.TY, tc.PB, W); }
+
 // Warp tiles: 16 x 16 cells by default (CG_WTILE_X / CG_WTILE_Y); the plane
 // batch and warps per CTA are chosen so that two CTAs fit on an SM.
 template <typename T>
-static WarpTile warp_tiling(const Geom& g) {
+WarpTile warp_tiling(const Geom& g, const TileTune* tt) {
   WarpTile tc{};
   const int W = g.kw;
-  tc.TX = std::max(16, (env_int("CG_WTILE_X", 16) / 16) * 16);
-  tc.TY = std::max(8, (env_int("CG_WTILE_Y", 16) / 8) * 8);
-  tc.RS = tc.TX + 1;
+  int tx = env_int("CG_WTILE_X", 16), ty = env_int("CG_WTILE_Y", 16);
   int PB = env_int("CG_WTILE_PLANES", 0);
+  int warps = env_int("CG_WTILE_WARPS", 0);
+  if (tt) {
+    if (tt->wx > 0) tx = tt->wx;
+    if (tt->wy > 0) ty = tt->wy;
+    if (tt->wpb > 0) PB = tt->wpb;
+    if (tt->warps > 0) warps = tt->warps;
+  }
+  tc.TX = std::max(16, (tx / 16) * 16);
+  tc.TY = std::max(8, (ty / 8) * 8);
+  tc.RS = tc.TX + 1;
   if (PB <= 0) PB = std::min(g.nw, 7);
   PB = std::min(PB, g.nw);
   tc.PB = PB;
@@ -700,8 +810,9 @@ static WarpTile warp_tiling(const Geom& g) {
   tc.PS = ps;
   tc.slots = ((tc.TY >> 3) + 2) * (PB + W) * 3;
   tc.warp_bytes = ((size_t)PB * tc.PS * 2 * sizeof(T) + (size_t)(tc.slots + 1) * 5 * 4 + 15) & ~(size_t)15;
-  int warps = env_int("CG_WTILE_WARPS", 0);
   if (warps <= 0) warps = (int)std::max<size_t>(1, std::min<size_t>(8, (110 * 1024) / tc.warp_bytes));
+  warps = std::min(warps, 8);
+  while (warps > 1 && tc.warp_bytes * warps > 220 * 1024) warps--;
   tc.warps = warps;
   tc.smem = tc.warp_bytes * warps;
   tc.ntx = (g.nf1 + tc.TX - 1) / tc.TX;
@@ -713,7 +824,7 @@ static WarpTile warp_tiling(const Geom& g) {
 
 template <typename T, int W>
 static int grid_w(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, const Geom& g, T* d_fw,
-                  int method, int* d_counter, cudaStream_t st) {
+                  int method, int* d_counter, cudaStream_t st, const TileTune* tt) {
   (void)d_counter;
   if (method == kGridDirect) {
     size_t G = (size_t)g.nf1 * g.nf2 * g.nw;
@@ -726,7 +837,7 @@ static int grid_w(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, cons
     CG_CUDA(cudaGetLastError());
     return CG_OK;
   }
-  WarpTile tc = warp_tiling<T>(g);
+  WarpTile tc = warp_tiling<T>(g, tt);
   auto* kern = geom_poly_host<T>(g) ? k_grid_warp<T, W, true> : k_grid_warp<T, W, false>;
   int per_sm = 0;
   CG_CUDA(kernel_occupancy((const void*)kern, tc.warps * 32, tc.smem, &per_sm));
@@ -744,7 +855,7 @@ static int grid_w(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, cons
 template <typename T, int W>
 static int degrid_w(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_start, int64_t M,
                     const Geom& g, const T* d_fw, T* d_vis, int method, int* d_counter,
-                    cudaStream_t st) {
+                    cudaStream_t st, const TileTune* tt) {
   if (M == 0) return CG_OK;
   if (method == kGridDirect) {
     int blocks = (int)((M + 255) / 256);
@@ -754,7 +865,7 @@ static int degrid_w(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_s
     CG_CUDA(cudaGetLastError());
     return CG_OK;
   }
-  TileCfg tc = grid_tiling<T>(g, true);
+  TileCfg tc = grid_tiling<T>(g, true, tt);
   int nslots = slots_for(tc.TY, tc.PB, W);
   int per_sm = 0;
   CG_CUDA(kernel_occupancy((const void*)k_degrid_tiled<T, W>, tc.threads, tc.smem, &per_sm));
@@ -793,7 +904,7 @@ static int degrid_w(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_s
 
 template <typename T>
 int launch_grid(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, const Geom& g, T* d_fw,
-                int method, int* d_counter, cudaStream_t st) {
+                int method, int* d_counter, cudaStream_t st, const TileTune* tt) {
   if (method == kGridMma) {
     // tensor-core path: FP32, ES kernel and W <= 8; everything else on the SIMT kernels
     if (sizeof(T) == 4 && !g.polyf) {
@@ -802,7 +913,7 @@ int launch_grid(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, const 
     }
     method = kGridTiled;
   }
-#define CG_GRID_CALL(w) grid_w<T, w>(d_recs, d_hive_start, M, g, d_fw, method, d_counter, st)
+#define CG_GRID_CALL(w) grid_w<T, w>(d_recs, d_hive_start, M, g, d_fw, method, d_counter, st, tt)
   CG_W_SWITCH(g.kw, CG_GRID_CALL)
 #undef CG_GRID_CALL
 }
@@ -810,12 +921,101 @@ int launch_grid(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, const 
 template <typename T>
 int launch_degrid(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_start, int64_t M,
                   const Geom& g, const T* d_fw, T* d_vis, int method, int* d_counter,
-                  cudaStream_t st) {
+                  cudaStream_t st, const TileTune* tt) {
   if (method == kGridMma) method = kGridTiled;
 #define CG_DEGRID_CALL(w) \
-  degrid_w<T, w>(d_recs, d_perm, d_hive_start, M, g, d_fw, d_vis, method, d_counter, st)
+  degrid_w<T, w>(d_recs, d_perm, d_hive_start, M, g, d_fw, d_vis, method, d_counter, st, tt)
   CG_W_SWITCH(g.kw, CG_DEGRID_CALL)
 #undef CG_DEGRID_CALL
+}
+
+// ================================================================== multi-grid
+template <typename T>
+int multi_shape(GridJob<T>* jobs, int njobs, MultiShape* sh) {
+  if (njobs < 1) return CG_ERR_ARG;
+  *sh = MultiShape{};
+  sh->kw = jobs[0].g.kw;
+  sh->poly = geom_poly_host<T>(jobs[0].g) != nullptr;
+  sh->threads = jobs[0].dt.threads;
+  int64_t gi = 0, di = 0;
+  int warps = 8;
+  for (int j = 0; j < njobs; j++) {
+    GridJob<T>& J = jobs[j];
+    if (J.g.kw != sh->kw || (geom_poly_host<T>(J.g) != nullptr) != sh->poly ||
+        J.dt.threads != sh->threads) {
+      set_last_error("multi-grid jobs differ in kernel width, kernel or threads");
+      return CG_ERR_ARG;
+    }
+    J.grid_item0 = (int)gi;
+    J.degrid_item0 = (int)di;
+    gi += J.wt.nitems;
+    di += J.dt.nitems;
+    sh->warp_bytes = std::max(sh->warp_bytes, J.wt.warp_bytes);
+    sh->dsmem = std::max(sh->dsmem, J.dt.smem);
+    warps = std::min(warps, J.wt.warps);
+  }
+  if (gi > 2147483647LL || di > 2147483647LL) return CG_ERR_SIZE;
+  sh->grid_items = (int)gi;
+  sh->degrid_items = (int)di;
+  sh->warps = std::max(1, warps);
+  while (sh->warps > 1 && sh->warp_bytes * sh->warps > 220 * 1024) sh->warps--;
+  return CG_OK;
+}
+
+template <typename T, int W>
+static int grid_multi_w(const GridJob<T>* d_jobs, int njobs, const MultiShape& sh, int* d_counter,
+                        cudaStream_t st) {
+  auto* kern = sh.poly ? k_grid_warp_multi<T, W, true> : k_grid_warp_multi<T, W, false>;
+  const size_t smem = sh.warp_bytes * sh.warps;
+  int per_sm = 0;
+  CG_CUDA(kernel_occupancy((const void*)kern, sh.warps * 32, smem, &per_sm));
+  if (per_sm < 1) {
+    set_last_error("multi-grid gridding does not fit on an SM");
+    return CG_ERR_ARG;
+  }
+  const int blocks = std::min((sh.grid_items + sh.warps - 1) / sh.warps, per_sm * num_sms());
+  CG_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(int), st));
+  kern<<<std::max(1, blocks), sh.warps * 32, smem, st>>>(d_jobs, njobs, sh.grid_items, sh.warp_bytes,
+                                                         d_counter);
+  count_launches(1);
+  CG_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+template <typename T, int W>
+static int degrid_multi_w(const GridJob<T>* d_jobs, int njobs, const MultiShape& sh,
+                          int* d_counter, cudaStream_t st) {
+  int per_sm = 0;
+  CG_CUDA(kernel_occupancy((const void*)k_degrid_tiled_multi<T, W>, sh.threads, sh.dsmem, &per_sm));
+  if (per_sm < 1) {
+    set_last_error("multi-grid degridding does not fit on an SM");
+    return CG_ERR_ARG;
+  }
+  const int blocks = std::min(sh.degrid_items, per_sm * num_sms());
+  CG_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(int), st));
+  k_degrid_tiled_multi<T, W><<<std::max(1, blocks), sh.threads, sh.dsmem, st>>>(
+      d_jobs, njobs, sh.degrid_items, d_counter);
+  count_launches(1);
+  CG_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+template <typename T>
+int launch_grid_multi(const GridJob<T>* d_jobs, int njobs, const MultiShape& sh, int* d_counter,
+                      cudaStream_t st) {
+  if (njobs < 1 || sh.grid_items < 1) return CG_OK;
+#define CG_GRID_MULTI_CALL(w) grid_multi_w<T, w>(d_jobs, njobs, sh, d_counter, st)
+  CG_W_SWITCH(sh.kw, CG_GRID_MULTI_CALL)
+#undef CG_GRID_MULTI_CALL
+}
+
+template <typename T>
+int launch_degrid_multi(const GridJob<T>* d_jobs, int njobs, const MultiShape& sh, int* d_counter,
+                        cudaStream_t st) {
+  if (njobs < 1 || sh.degrid_items < 1) return CG_OK;
+#define CG_DEGRID_MULTI_CALL(w) degrid_multi_w<T, w>(d_jobs, njobs, sh, d_counter, st)
+  CG_W_SWITCH(sh.kw, CG_DEGRID_MULTI_CALL)
+#undef CG_DEGRID_MULTI_CALL
 }
 
 // ================================================================ plane windows
@@ -955,15 +1155,28 @@ template int launch_degrid_window<float>(const Rec<float>*, const int*, int64_t,
 template int launch_degrid_window<double>(const Rec<double>*, const int*, int64_t, const Geom&,
                                           int, int, const double*, double*, cudaStream_t);
 
-template TileCfg grid_tiling<float>(const Geom&, bool);
-template TileCfg grid_tiling<double>(const Geom&, bool);
+template TileCfg grid_tiling<float>(const Geom&, bool, const TileTune*);
+template TileCfg grid_tiling<double>(const Geom&, bool, const TileTune*);
+template WarpTile warp_tiling<float>(const Geom&, const TileTune*);
+template WarpTile warp_tiling<double>(const Geom&, const TileTune*);
+template int multi_shape<float>(GridJob<float>*, int, MultiShape*);
+template int multi_shape<double>(GridJob<double>*, int, MultiShape*);
+template int launch_grid_multi<float>(const GridJob<float>*, int, const MultiShape&, int*,
+                                      cudaStream_t);
+template int launch_grid_multi<double>(const GridJob<double>*, int, const MultiShape&, int*,
+                                       cudaStream_t);
+template int launch_degrid_multi<float>(const GridJob<float>*, int, const MultiShape&, int*,
+                                        cudaStream_t);
+template int launch_degrid_multi<double>(const GridJob<double>*, int, const MultiShape&, int*,
+                                         cudaStream_t);
 template int launch_grid<float>(const Rec<float>*, const int*, int64_t, const Geom&, float*, int,
-                                int*, cudaStream_t);
+                                int*, cudaStream_t, const TileTune*);
 template int launch_grid<double>(const Rec<double>*, const int*, int64_t, const Geom&, double*, int,
-                                 int*, cudaStream_t);
+                                 int*, cudaStream_t, const TileTune*);
 template int launch_degrid<float>(const Rec<float>*, const int*, const int*, int64_t, const Geom&,
-                                  const float*, float*, int, int*, cudaStream_t);
+                                  const float*, float*, int, int*, cudaStream_t, const TileTune*);
 template int launch_degrid<double>(const Rec<double>*, const int*, const int*, int64_t,
-                                   const Geom&, const double*, double*, int, int*, cudaStream_t);
+                                   const Geom&, const double*, double*, int, int*, cudaStream_t,
+                                   const TileTune*);
 
 }  // namespace cg

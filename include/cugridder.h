@@ -323,10 +323,13 @@ int cg_nufft_destroy(cg_nufft *plan);
  * DEVICE pointers that must stay valid (and uvw unchanged) for the life of
  * the batch; vis / wgt are [nrow][nchan] (wgt may be NULL), freqs a HOST array
  * of nchan frequencies (copied at creation).  ms2dirty sums a dataset's
- * channels into its image; dirty2ms fills every (row, channel).  The first
- * call per direction runs eagerly; the second is captured into a CUDA graph
- * over the batch's streams and later calls replay it (CG_BATCH_GRAPH=0
- * disables the graph).  Calls are ordered on `stream`. */
+ * channels into its image; dirty2ms fills every (row, channel).  All
+ * datasets are spread (interpolated) by ONE persistent launch over a
+ * (dataset, tile) work queue; the stages before and after it run per dataset
+ * over the batch's streams.  The first call per direction runs eagerly and
+ * autotunes that launch's tiling; the second is captured into a CUDA graph
+ * and later calls replay it (CG_BATCH_GRAPH=0 disables the graph).  Calls
+ * are ordered on `stream`. */
 typedef struct {
     int64_t nrow;
     int nchan;
@@ -343,6 +346,12 @@ int cg_batch_create(cg_batch **batch, int n, const cg_dataset *datasets, double 
                     double sigma, int sign, int precision, void *stream);
 int cg_batch_ms2dirty(cg_batch *batch);
 int cg_batch_dirty2ms(cg_batch *batch);
+/* Tiling picked by the autotuner on the first call of each direction
+ * (CG_BATCH_AUTOTUNE=0 keeps the defaults): tiling[0..3] = gridding warp
+ * tile x, y, plane batch, warps per CTA; tiling[4..7] = degridding tile x,
+ * y, plane batch, threads per CTA (0 = default).  tuned_ms (may be NULL)
+ * receives the winning launch times in ms (0 = not tuned). */
+int cg_batch_get_tiling(const cg_batch *batch, int *tiling, float *tuned_ms);
 int cg_batch_destroy(cg_batch *batch);
 
 /* Host-pointer calls above keep one cached plan per precision so that

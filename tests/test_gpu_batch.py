@@ -1,6 +1,7 @@
 """Batched solves (cg_batch_*) against one plan per dataset: uneven datasets
-(image sizes, fov, rows, channels), the eager first call, the captured
-second call and graph replays with new visibilities / images."""
+(image sizes, fov, rows, channels, one without rows), the eager and
+autotuned first call, the captured second call and graph replays with new
+visibilities / images; and the untuned eager form."""
 import numpy as np
 import pytest
 
@@ -13,7 +14,7 @@ from tests.gpu_helpers import to_dev
 pytestmark = pytest.mark.gpu
 
 SPECS = [(64, 1.0, 3000, 1), (96, 2.5, 12000, 3), (128, 1.5, 20000, 2), (64, 4.0, 5000, 4),
-         (80, 3.0, 800, 1), (128, 2.0, 30000, 1)]
+         (80, 3.0, 800, 1), (128, 2.0, 30000, 1), (64, 2.0, 0, 2)]
 
 
 def _datasets(torch):
@@ -44,17 +45,53 @@ def _plan_ref(torch, d, direction):
     return out.cpu().numpy()
 
 
+def _close(out, ref):
+    if ref.size == 0 or not np.any(ref):  # a dataset without rows: an exactly zero result
+        return not np.any(out)
+    return rel_l2(out, ref) < 1e-5
+
+
+def _check_batch(torch, ds, b, ncalls):
+    for call in range(ncalls):
+        for i, d in enumerate(ds):
+            d["vis"].mul_(complex(0.5 + 0.1 * call, 0.2))
+        b.ms2dirty()
+        torch.cuda.synchronize()
+        for d in ds:
+            assert _close(d["dirty"].cpu().numpy(), _plan_ref(torch, d, 0)), call
+    for call in range(ncalls):
+        for i, d in enumerate(ds):
+            d["dirty"].copy_(torch.from_numpy(
+                synth.random_image(d["dirty"].shape[0], d["dirty"].shape[1], seed=500 + 10 * call + i,
+                                   dtype=np.complex64)).cuda())
+        b.dirty2ms()
+        torch.cuda.synchronize()
+        for d in ds:
+            assert _close(d["vis"].cpu().numpy(), _plan_ref(torch, d, 1)), call
+
+
+def test_batch_untuned_eager(torch_cuda, monkeypatch):
+    torch = torch_cuda
+    monkeypatch.setenv("CG_BATCH_AUTOTUNE", "0")
+    monkeypatch.setenv("CG_BATCH_GRAPH", "0")
+    ds = _datasets(torch)
+    b = Batch(ds, epsilon=1e-4, precision="fp32")
+    _check_batch(torch, ds, b, 2)
+    assert b.tiling()[0] == (0, 0, 0, 0) and b.tiling()[1] == (0, 0, 0, 0)
+    b.close()
+
+
 def test_batch_matches_plans_through_graph_replays(torch_cuda):
     torch = torch_cuda
     ds = _datasets(torch)
     b = Batch(ds, epsilon=1e-4, precision="fp32")
-    for call in range(4):  # eager, captured, replay, replay
+    for call in range(4):  # eager (autotuned), captured, replay, replay
         for i, d in enumerate(ds):  # new visibilities every call, same tensors
             d["vis"].mul_(complex(0.5 + 0.1 * call, 0.2))
         b.ms2dirty()
         torch.cuda.synchronize()
         for d in ds:
-            assert rel_l2(d["dirty"].cpu().numpy(), _plan_ref(torch, d, 0)) < 1e-5, call
+            assert _close(d["dirty"].cpu().numpy(), _plan_ref(torch, d, 0)), call
     for call in range(3):
         for i, d in enumerate(ds):
             d["dirty"].copy_(torch.from_numpy(
@@ -63,5 +100,9 @@ def test_batch_matches_plans_through_graph_replays(torch_cuda):
         b.dirty2ms()
         torch.cuda.synchronize()
         for d in ds:
-            assert rel_l2(d["vis"].cpu().numpy(), _plan_ref(torch, d, 1)) < 1e-5, call
+            assert _close(d["vis"].cpu().numpy(), _plan_ref(torch, d, 1)), call
+    grid_t, degrid_t, ms = b.tiling()
+    assert grid_t[0] in (16, 32) and grid_t[1] in (8, 16, 32), grid_t
+    assert degrid_t[3] in (256, 512), degrid_t
+    assert ms[0] > 0 and ms[1] > 0, ms
     b.close()
