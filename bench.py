@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--batch", action="store_true",
+                    help="the batched workload: 32 uneven datasets (synth.batch_specs), eps 1e-4")
     ap.add_argument("--kernel", default="auto", choices=["auto", "es", "learned"],
                     help="auto: the learned kernel at the smallest width that met epsilon in the "
                          "committed width search, else ES")
@@ -523,8 +525,149 @@ def run_reference(args, rank, world):
     return r
 
 
+# --------------------------------------------------------------------------- batched workload
+BATCH_METRIC = "Mvis/s batched ms2dirty+dirty2ms, 32 uneven datasets, eps 1e-4, 1 B200"
+
+
+def make_batch_data(specs, torch):
+    """Device arrays of the batched workload, seeded per dataset."""
+    out = []
+    for sp in specs:
+        g = torch.Generator(device="cuda")
+        g.manual_seed(sp["seed"])
+        n, nc = sp["nrow"], sp["nchan"]
+        uv = torch.randn((n, 2), generator=g, device="cuda", dtype=torch.float64) * sp["uv_sigma"]
+        uv.clamp_(-sp["uv_clip"], sp["uv_clip"])
+        w = (torch.rand((n, 1), generator=g, device="cuda", dtype=torch.float64) * 2 - 1) * sp["w_max"]
+        uvw = torch.cat([uv, w], 1).contiguous()
+        vis = torch.complex(torch.randn((n, nc), generator=g, device="cuda"),
+                            torch.randn((n, nc), generator=g, device="cuda")).contiguous()
+        wgt = (torch.rand((n, nc), generator=g, device="cuda") + 0.5).contiguous()
+        out.append(dict(uvw=uvw, freqs=sp["freqs"], vis=vis, wgt=wgt, fov=sp["fov"],
+                        dirty=torch.zeros((sp["nx"], sp["ny"]), dtype=torch.complex64, device="cuda")))
+    return out
+
+
+def run_batch(args):
+    """Batched uneven solves through cugridder_b200.batch.Batch (one persistent
+    spreading / interpolation launch per direction, autotuned tiling, CUDA
+    graph replay) against the same datasets through one Plan each, called in
+    sequence.  One step = ms2dirty then dirty2ms of every dataset; Mvis/s =
+    sum(nrow * nchan) / step time.  The visibilities are restored between
+    steps, outside the timed brackets."""
+    import torch
+
+    from cugridder_b200 import Plan, _lib, synth
+    from cugridder_b200.batch import Batch
+
+    args.eps = 1e-4
+    eps = 1e-4
+    torch.cuda.set_device(0)
+    lib = _lib.load()
+    kern = select_kernel(args)
+    specs = synth.batch_specs()
+    ds = make_batch_data(specs, torch)
+    nvis = sum(sp["nrow"] * sp["nchan"] for sp in specs)
+    pristine = [d["vis"].clone() for d in ds]
+    st = torch.cuda.current_stream()
+
+    def timed(step_fn, steps, restore):
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+        torch.cuda.synchronize()
+        for k in range(steps):
+            restore()
+            ev[k][0].record(st)
+            step_fn(0)
+            ev[k][1].record(st)
+            step_fn(1)
+            ev[k][2].record(st)
+        torch.cuda.synchronize()
+        m2d = [e[0].elapsed_time(e[1]) for e in ev]
+        d2m = [e[1].elapsed_time(e[2]) for e in ev]
+        return statistics.median(m2d), statistics.median(d2m)
+
+    def restore():
+        for d, v in zip(ds, pristine):
+            d["vis"].copy_(v)
+
+    out = {}
+    clocks = ClockSampler(0)
+    for label, kk, prec in (("learned_fp32", kern, "fp32"),
+                            ("es_fp32", {"kind": "es", "W": 0, "coef": None}, "fp32")):
+        b = Batch(ds, epsilon=eps, precision=prec)
+        if kk["kind"] == "poly":
+            b.set_kernel("poly", kk["W"], kk["coef"])
+        l0 = lib.cg_kernel_launches()
+        b.ms2dirty()  # eager, autotuned
+        b.dirty2ms()
+        torch.cuda.synchronize()
+        l1 = lib.cg_kernel_launches()
+        b.ms2dirty()  # captured
+        b.dirty2ms()
+        torch.cuda.synchronize()
+        launches = lib.cg_kernel_launches() - l1
+        for _ in range(max(1, args.warmup - 2)):
+            b.ms2dirty()
+            b.dirty2ms()
+        if label == "learned_fp32":
+            clocks.start()
+        m2d, d2m = timed(lambda dr: b.ms2dirty() if dr == 0 else b.dirty2ms(), args.steps, restore)
+        if label == "learned_fp32":
+            clocks.stop()
+        gt, dt, tms = b.tiling()
+        out[label] = {"value": nvis / ((m2d + d2m) * 1e-3) / 1e6, "ms_ms2dirty": m2d, "ms_dirty2ms": d2m,
+                      "kernels_per_step": launches, "eager_first_call_launches": l1 - l0,
+                      "tiling": {"grid_warp_tile": gt, "degrid_tile": dt,
+                                 "phase2_ms": [round(x, 3) for x in tms]},
+                      "W": kk["W"] or None}
+        b.close()
+        del b
+        torch.cuda.synchronize()
+
+    # the same datasets through one Plan each, called in sequence
+    seq_m2d = seq_d2m = 0.0
+    for d, v in zip(ds, pristine):
+        n = d["dirty"].shape[0]
+        p = Plan(n, n, d["fov"], eps, precision="fp32")
+        if kern["kind"] == "poly":
+            p.set_kernel("poly", kern["W"], kern["coef"])
+        out_vis = torch.empty_like(d["vis"])
+
+        def step(dr):
+            if dr == 0:
+                p.ms2dirty_chan(d["uvw"], d["freqs"], d["vis"], d["wgt"], d["dirty"])
+            else:
+                p.dirty2ms_chan(d["uvw"], d["freqs"], d["dirty"], d["wgt"], out_vis)
+
+        step(0)
+        step(1)
+        m2d, d2m = timed(step, 2, lambda: None)
+        seq_m2d += m2d
+        seq_d2m += d2m
+        p.close()
+    out["sequential_plans_learned_fp32"] = {"value": nvis / ((seq_m2d + seq_d2m) * 1e-3) / 1e6,
+                                            "ms_ms2dirty": seq_m2d, "ms_dirty2ms": seq_d2m}
+    main = out["learned_fp32"]
+    line = {"metric": BATCH_METRIC, "value": round(main["value"], 2), "unit": "Mvis/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(main["ms_ms2dirty"] + main["ms_dirty2ms"], 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 (fp64 uvw/coordinates)", "data": "synthetic",
+            "config": {"workload": "batch_32_uneven", "datasets": len(specs),
+                       "rows": sum(sp["nrow"] for sp in specs), "visibilities": nvis,
+                       "images": sorted({sp["nx"] for sp in specs}), "eps": eps,
+                       "kernel": kern.get("label", "ES"),
+                       "l2": "inputs larger than L2 (%.1f GB of visibilities)" % (nvis * 8 / 1e9)},
+            "forms": out, "clocks": clocks.summary(),
+            "batched_over_sequential": round(main["value"] / out["sequential_plans_learned_fp32"]["value"], 3)}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.batch:
+        run_batch(args)
+        return
     rank, world, local = dist_setup()
     if args.impl == "reference":
         r = run_reference(args, rank, world)

@@ -59,6 +59,14 @@ class Batch:
     def dirty2ms(self):
         _lib.check(self._lib.cg_batch_dirty2ms(self._h))
 
+    def set_kernel(self, kind="es", W=None, coef=None):
+        """Gridding kernel of every dataset (as Plan.set_kernel); before the first call."""
+        if kind == "es":
+            _lib.check(self._lib.cg_batch_set_kernel(self._h, _lib.CG_KERNEL_ES, int(W or 0), None))
+            return
+        a = np.ascontiguousarray(np.asarray(coef, dtype=np.float64).reshape(int(W), 8))
+        _lib.check(self._lib.cg_batch_set_kernel(self._h, _lib.CG_KERNEL_POLY, int(W), a.ctypes.data))
+
     def tiling(self):
         """Autotuned tiling: (gridding x, y, planes, warps), (degridding x,
         y, planes, threads) and the winning launch times in ms (0 = default

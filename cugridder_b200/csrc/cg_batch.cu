@@ -377,6 +377,16 @@ static int batch_call(cg_batch_s* B, int dir) {
 int cg_batch_ms2dirty(cg_batch_s* batch) { return batch_call(batch, 0); }
 int cg_batch_dirty2ms(cg_batch_s* batch) { return batch_call(batch, 1); }
 
+int cg_batch_set_kernel(cg_batch_s* batch, int kind, int W, const double* coef) {
+  if (!batch) return CG_ERR_ARG;
+  if (batch->calls[0] || batch->calls[1]) {
+    cg::set_last_error("batch: set the kernel before the first call");
+    return CG_ERR_ARG;
+  }
+  for (auto P : batch->plans) CG_TRY(cg_plan_set_kernel(P, kind, W, coef));
+  return CG_OK;
+}
+
 int cg_batch_get_tiling(const cg_batch_s* batch, int* tiling, float* tuned_ms) {
   if (!batch || !tiling) return CG_ERR_ARG;
   const cg::TileTune& t = batch->tune;

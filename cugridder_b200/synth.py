@@ -84,3 +84,30 @@ def rel_l2(a, b):
     a = np.asarray(a, dtype=np.complex128)
     b = np.asarray(b, dtype=np.complex128)
     return float(np.sqrt(np.sum(np.abs(a - b) ** 2) / np.sum(np.abs(b) ** 2)))
+
+
+# Batched uneven solves: 32 independent datasets with row counts log-uniform
+# in [1e4, 1e7], images from {512, 1024, 2048}, fov U(1, 4) deg and 1-16
+# channels spaced uniformly in [1e8, 2e8] Hz sharing one uvw set; epsilon
+# 1e-4.  u, v, w follow the 4096 case (u, v ~ N(0, 0.3 clip) clipped to
+# +-clip, w ~ U(-clip/10, clip/10)) scaled so that the clip sits at the same
+# fraction of each image's Nyquist limit at the highest frequency as the 4096
+# case's 20 km does at 1.5e8 Hz (10000 wavelengths of 4096 / (2 * 5 deg)).
+BATCH_NYQUIST_FRACTION = 10000.0 / (4096 / (2 * np.deg2rad(5.0)))
+
+
+def batch_specs(n=32, seed=2024, rows_lo=1e4, rows_hi=1e7, sizes=(512, 1024, 2048)):
+    """Per-dataset parameters of the batched workload (no arrays)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for i in range(n):
+        nrow = int(round(10 ** rng.uniform(np.log10(rows_lo), np.log10(rows_hi))))
+        size = int(rng.choice(sizes))
+        fov = float(rng.uniform(1.0, 4.0))
+        nchan = int(rng.integers(1, 17))
+        freqs = np.linspace(1.0e8, 2.0e8, nchan) if nchan > 1 else np.array([1.5e8])
+        nyq = size / (2 * np.deg2rad(fov))  # wavelengths
+        clip = BATCH_NYQUIST_FRACTION * nyq * C_LIGHT / freqs.max()  # metres
+        out.append(dict(nrow=nrow, nx=size, ny=size, fov=fov, nchan=nchan, freqs=freqs,
+                        uv_clip=clip, uv_sigma=0.3 * clip, w_max=0.1 * clip, seed=seed * 1000 + i))
+    return out

@@ -346,6 +346,9 @@ int cg_batch_create(cg_batch **batch, int n, const cg_dataset *datasets, double 
                     double sigma, int sign, int precision, void *stream);
 int cg_batch_ms2dirty(cg_batch *batch);
 int cg_batch_dirty2ms(cg_batch *batch);
+/* Gridding kernel of every dataset (arguments as cg_plan_set_kernel); only
+ * before the first call. */
+int cg_batch_set_kernel(cg_batch *batch, int kind, int W, const double *coef);
 /* Tiling picked by the autotuner on the first call of each direction
  * (CG_BATCH_AUTOTUNE=0 keeps the defaults): tiling[0..3] = gridding warp
  * tile x, y, plane batch, warps per CTA; tiling[4..7] = degridding tile x,

@@ -31,9 +31,11 @@ def _datasets(torch):
     return out
 
 
-def _plan_ref(torch, d, direction):
+def _plan_ref(torch, d, direction, kernel=None):
     n = d["dirty"].shape[0]
     p = Plan(n, n, d["fov"], 1e-4, precision="fp32")
+    if kernel is not None:
+        p.set_kernel("poly", kernel.W, kernel.horner)
     if direction == 0:
         out = torch.zeros_like(d["dirty"])
         p.ms2dirty_chan(d["uvw"], d["freqs"], d["vis"], d["wgt"], out)
@@ -51,14 +53,14 @@ def _close(out, ref):
     return rel_l2(out, ref) < 1e-5
 
 
-def _check_batch(torch, ds, b, ncalls):
+def _check_batch(torch, ds, b, ncalls, kernel=None):
     for call in range(ncalls):
         for i, d in enumerate(ds):
             d["vis"].mul_(complex(0.5 + 0.1 * call, 0.2))
         b.ms2dirty()
         torch.cuda.synchronize()
         for d in ds:
-            assert _close(d["dirty"].cpu().numpy(), _plan_ref(torch, d, 0)), call
+            assert _close(d["dirty"].cpu().numpy(), _plan_ref(torch, d, 0, kernel)), call
     for call in range(ncalls):
         for i, d in enumerate(ds):
             d["dirty"].copy_(torch.from_numpy(
@@ -67,7 +69,19 @@ def _check_batch(torch, ds, b, ncalls):
         b.dirty2ms()
         torch.cuda.synchronize()
         for d in ds:
-            assert _close(d["vis"].cpu().numpy(), _plan_ref(torch, d, 1)), call
+            assert _close(d["vis"].cpu().numpy(), _plan_ref(torch, d, 1, kernel)), call
+
+
+def test_batch_learned_kernel(torch_cuda):
+    from cugridder_b200.learn import load_kernel
+
+    torch = torch_cuda
+    k = load_kernel(5)
+    ds = _datasets(torch)
+    b = Batch(ds, epsilon=1e-4, precision="fp32")
+    b.set_kernel("poly", k.W, k.horner)
+    _check_batch(torch, ds, b, 3, kernel=k)
+    b.close()
 
 
 def test_batch_untuned_eager(torch_cuda, monkeypatch):
