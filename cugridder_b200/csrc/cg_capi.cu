@@ -123,6 +123,8 @@ void destroy_plan(cg_plan_s* P) {
                       &P->chan_uvw, &P->chan_scale, &P->coltw, &P->acc};
   for (auto b : bs) cg::release(*b);
   if (P->h_mm) cudaFreeHost(P->h_mm);
+  if (P->io_stream) cudaStreamDestroy(P->io_stream);
+  if (P->io_event) cudaEventDestroy(P->io_event);
   if (P->timer.created)
     for (int s = 0; s < 2; s++)
       for (int i = 0; i <= kMaxStages; i++) cudaEventDestroy(P->timer.ev[s][i]);
@@ -229,7 +231,23 @@ int host_call(bool to_dirty, int precision, int64_t nrow, int nx, int ny, double
   CG_TRY(ensure(P->io_wgt, (size_t)nrow * tsz));
   CG_TRY(ensure(P->io_dirty, (size_t)nx * ny * 2 * tsz));
   cudaStream_t s = P->stream;
+  if (!P->io_stream) {
+    CG_CUDA(cudaStreamCreateWithFlags(&P->io_stream, cudaStreamNonBlocking));
+    CG_CUDA(cudaEventCreateWithFlags(&P->io_event, cudaEventDisableTiming));
+  }
+  cudaStream_t s2 = P->io_stream;
+  // every return below leaves both streams idle (the host buffers may be
+  // reused as soon as the call returns) and the plan without the wait
+  struct Finish {
+    cg_plan_s* P;
+    ~Finish() {
+      P->inputs_ready = nullptr;
+      cudaStreamSynchronize(P->io_stream);
+      cudaStreamSynchronize(P->stream);
+    }
+  } finish{P};
   double* d_uvw = (double*)P->io_uvw.p;
+  // uvw first, on the plan's stream: the w range and the binning read it
   if (nrow > 0) {
     if (uvw_is_float) {
       float* d_f = (float*)(d_uvw + n_uvw);
@@ -240,17 +258,25 @@ int host_call(bool to_dirty, int precision, int64_t nrow, int nx, int ny, double
     } else {
       CG_CUDA(cudaMemcpyAsync(d_uvw, uvw, n_uvw * 8, cudaMemcpyHostToDevice, s));
     }
-    if (wgt) CG_CUDA(cudaMemcpyAsync(P->io_wgt.p, wgt, (size_t)nrow * tsz, cudaMemcpyHostToDevice, s));
   }
+  // vis / wgt / dirty on the second stream, overlapping the w range and binning
+  if (nrow > 0 && wgt)
+    CG_CUDA(cudaMemcpyAsync(P->io_wgt.p, wgt, (size_t)nrow * tsz, cudaMemcpyHostToDevice, s2));
+  if (to_dirty) {
+    if (nrow > 0)
+      CG_CUDA(cudaMemcpyAsync(P->io_vis.p, vis, (size_t)nrow * 2 * tsz, cudaMemcpyHostToDevice, s2));
+  } else {
+    CG_CUDA(cudaMemcpyAsync(P->io_dirty.p, dirty, (size_t)nx * ny * 2 * tsz, cudaMemcpyHostToDevice, s2));
+  }
+  CG_CUDA(cudaEventRecord(P->io_event, s2));
+  P->inputs_ready = P->io_event;
   int rs;
   if (to_dirty) {
-    if (nrow > 0) CG_CUDA(cudaMemcpyAsync(P->io_vis.p, vis, (size_t)nrow * 2 * tsz, cudaMemcpyHostToDevice, s));
     rs = cg::ms2dirty_device(P, nrow, freq, d_uvw, P->io_vis.p, wgt ? P->io_wgt.p : nullptr,
                              P->io_dirty.p);
     if (rs > 1) return rs;
     CG_CUDA(cudaMemcpyAsync(dirty, P->io_dirty.p, (size_t)nx * ny * 2 * tsz, cudaMemcpyDeviceToHost, s));
   } else {
-    CG_CUDA(cudaMemcpyAsync(P->io_dirty.p, dirty, (size_t)nx * ny * 2 * tsz, cudaMemcpyHostToDevice, s));
     rs = cg::dirty2ms_device(P, nrow, freq, d_uvw, P->io_dirty.p, wgt ? P->io_wgt.p : nullptr,
                              P->io_vis.p);
     if (rs > 1) return rs;

@@ -629,6 +629,12 @@ static int dirty2ms_windows(cg_plan_s* P, const T* d_dirty, T* d_vis) {
   return CG_OK;
 }
 
+// host entry points: wait for the inputs copied on the second stream
+static int wait_inputs(cg_plan_s* P) {
+  if (P->inputs_ready) CG_CUDA(cudaStreamWaitEvent(P->stream, P->inputs_ready, 0));
+  return CG_OK;
+}
+
 // the stages after gridding: FFT, then w-DFT with the corrections
 template <typename T>
 static int ms2dirty_tail(cg_plan_s* P, T* d_dirty) {
@@ -660,6 +666,7 @@ static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T
                       (int*)P->hive_start.p + (nh_of(g) + 1)));
   timer_mark(P);  // 2: binning
   if (P->stop_stage == 1) return CG_OK;
+  CG_TRY(wait_inputs(P));
   CG_TRY(launch_build_stream<T>((const int*)P->perm.p, M, d_uvw, d_vis, d_wgt, g, true,
                                 (Rec<T>*)P->recs_tmp.p, (Rec<T>*)P->recs.p, st));
   timer_mark(P);  // 3: sorted stream
@@ -694,6 +701,7 @@ static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const
                       (int*)P->hive_start.p + (nh_of(g) + 1)));
   timer_mark(P);  // 2: binning
   if (P->stop_stage == 1) return CG_OK;
+  CG_TRY(wait_inputs(P));
   if (P->plane_batch) {  // memory-limited mode: fill, FFT and degridding per plane window
     CG_TRY(launch_build_stream<T>((const int*)P->perm.p, M, d_uvw, (const T*)nullptr, d_wgt, g,
                                   false, (Rec<T>*)P->recs_tmp.p, (Rec<T>*)P->recs.p, st));

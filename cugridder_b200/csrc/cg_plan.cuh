@@ -84,6 +84,12 @@ struct cg_plan_s {
   bool fft1_valid = false;
   int fft1_nf1 = 0, fft1_nf2 = 0;
   cg_stage_timer timer;
+  // host entry points: inputs the first stages do not read are copied on
+  // io_stream; a call waits on inputs_ready (when set) before the first stage
+  // that reads vis, wgt or the dirty image
+  cudaStream_t io_stream = nullptr;
+  cudaEvent_t io_event = nullptr;
+  cudaEvent_t inputs_ready = nullptr;
   std::mutex mu;
 };
 
