@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default=WORKLOAD)
     ap.add_argument("--nrow", type=int, default=None, help="override the number of rows")
+    ap.add_argument("--fov", type=float, default=None,
+                    help="override the field of view in degrees (fewer w planes: small profiling cases)")
     ap.add_argument("--eps", type=float, default=1e-5)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
@@ -208,10 +210,11 @@ def ncu_traffic(kernel, workload):
 
 
 # --------------------------------------------------------------------------- workload
-def make_data(cfg_name, seed, nrow, torch):
+def make_data(cfg_name, seed, nrow, torch, fov=None):
     from cugridder_b200 import synth
 
-    d = synth.make(cfg_name, seed=seed, nrow=nrow)
+    over = {"fov": fov} if fov else {}
+    d = synth.make(cfg_name, seed=seed, nrow=nrow, **over)
     img = synth.random_image(d["nx"], d["ny"], seed=seed + 1000, dtype=np.complex64)
     return d, img
 
@@ -243,7 +246,7 @@ def run_b200(args, rank, world, local):
 
     torch.cuda.set_device(local)
     cfg = synth.CONFIGS[args.config]
-    d, img = make_data(args.config, rank, args.nrow, torch)
+    d, img = make_data(args.config, rank, args.nrow, torch, args.fov)
     M = d["uvw"].shape[0]
     nx, ny, fov, freq = d["nx"], d["ny"], d["fov"], d["freq"]
     dev = torch.device("cuda", local)
@@ -696,7 +699,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(res["ms_per_step"], 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (fp64 uvw/coordinates)", "data": "synthetic",
-            "config": {"workload": args.config, "nx": cfg["nx"], "ny": cfg["ny"], "fov_deg": cfg["fov"],
+            "config": {"workload": args.config, "nx": cfg["nx"], "ny": cfg["ny"], "fov_deg": args.fov or cfg["fov"],
                        "nrow_per_gpu": args.nrow or cfg["nrow"], "freq_hz": cfg["freq"], "eps": args.eps,
                        "kernel": res["kernel"]["label"], "W": info["kw"], "nw": info["nw"], "grid": [info["nf1"], info["nf2"]],
                        "parallelism": "independent datasets per GPU" if world > 1 else "single GPU",

@@ -10,7 +10,9 @@
 // Shared layout: row j of the column pair at float4 slot j + j / 16 (one pad
 // slot per 16 rows keeps the stride-16 stores of the first pass
 // conflict-free).
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "cg_internal.cuh"
@@ -63,14 +65,36 @@ __device__ __forceinline__ void dft_reg(float2* v, int sign) {
   }
 }
 
-// One Stockham pass of radix R over sub-transforms of size Ns, both columns
-// of the pair at once (float4 = column 0, column 1 of one row).  In place:
-// every thread reads its butterflies, the block syncs, then writes.  The
-// pass's twiddles e^{sign 2 pi i m k / (Ns R)} come from its own table
-// tw[m * Ns + k] (consecutive lanes read consecutive entries).
-template <int L, int R, bool kLast>
-__device__ __forceinline__ void stockham_pass(float4* s, int Ns, int sign,
+// Shared-memory element of one grid row of the CB columns a CTA transforms:
+// float2 (one column) or float4 (two adjacent columns).
+template <int CB>
+struct ColVec;
+template <>
+struct ColVec<1> {
+  using type = float2;
+  static __device__ __forceinline__ float2 col(const float2& v, int) { return v; }
+  static __device__ __forceinline__ float2 make(const float2* a, const float2*, int m) { return a[m]; }
+};
+template <>
+struct ColVec<2> {
+  using type = float4;
+  static __device__ __forceinline__ float2 col(const float4& v, int c) {
+    return c == 0 ? make_float2(v.x, v.y) : make_float2(v.z, v.w);
+  }
+  static __device__ __forceinline__ float4 make(const float2* a, const float2* b, int m) {
+    return make_float4(a[m].x, a[m].y, b[m].x, b[m].y);
+  }
+};
+
+// One Stockham pass of radix R over sub-transforms of size Ns, on every
+// column of the CTA at once.  In place: every thread reads its butterflies,
+// the block syncs, then writes.  The pass's twiddles
+// e^{sign 2 pi i m k / (Ns R)} come from its own table tw[m * Ns + k]
+// (consecutive lanes read consecutive entries).
+template <int L, int R, int CB, bool kLast>
+__device__ __forceinline__ void stockham_pass(typename ColVec<CB>::type* s, int Ns, int sign,
                                               const float2* __restrict__ tw) {
+  using CV = ColVec<CB>;
   constexpr int NB = L / R;  // butterflies per column
   constexpr int BPT = (NB + kFftThreads - 1) / kFftThreads;
   if constexpr (kLast) {
@@ -81,27 +105,26 @@ __device__ __forceinline__ void stockham_pass(float4* s, int Ns, int sign,
       float2 a[R], b[R];
 #pragma unroll
       for (int m = 0; m < R; m++) {
-        const float4 x = s[pad16(j + m * NB)];
-        float2 xa = make_float2(x.x, x.y), xb = make_float2(x.z, x.w);
+        const auto x = s[pad16(j + m * NB)];
+        float2 xa = CV::col(x, 0), xb = CB == 2 ? CV::col(x, 1) : xa;
         if (m > 0) {
           const float2 t = tw[m * Ns + j];
           const float2 w = make_float2(t.x, sign * t.y);
           xa = cmul(xa, w);
-          xb = cmul(xb, w);
+          if (CB == 2) xb = cmul(xb, w);
         }
         a[m] = xa;
         b[m] = xb;
       }
       dft_reg<R>(a, sign);
-      dft_reg<R>(b, sign);
+      if (CB == 2) dft_reg<R>(b, sign);
 #pragma unroll
-      for (int m = 0; m < R; m++)
-        s[pad16(j + m * Ns)] = make_float4(a[m].x, a[m].y, b[m].x, b[m].y);
+      for (int m = 0; m < R; m++) s[pad16(j + m * Ns)] = CV::make(a, b, m);
     }
     __syncthreads();
     return;
   } else {
-  float2 a[BPT][R], b[BPT][R];
+  float2 a[BPT][R], b[CB == 2 ? BPT : 1][R];
 #pragma unroll
   for (int q = 0; q < BPT; q++) {
     const int j = threadIdx.x + q * kFftThreads;
@@ -109,19 +132,20 @@ __device__ __forceinline__ void stockham_pass(float4* s, int Ns, int sign,
       const int k = j & (Ns - 1);
 #pragma unroll
       for (int m = 0; m < R; m++) {
-        const float4 x = s[pad16(j + m * NB)];
-        float2 xa = make_float2(x.x, x.y), xb = make_float2(x.z, x.w);
+        const auto x = s[pad16(j + m * NB)];
+        float2 xa = CV::col(x, 0);
+        float2 xb = CB == 2 ? CV::col(x, 1) : xa;
         if (m > 0 && Ns > 1) {
           const float2 t = tw[m * Ns + k];
           const float2 w = make_float2(t.x, sign * t.y);
           xa = cmul(xa, w);
-          xb = cmul(xb, w);
+          if (CB == 2) xb = cmul(xb, w);
         }
         a[q][m] = xa;
-        b[q][m] = xb;
+        if constexpr (CB == 2) b[q][m] = xb;
       }
       dft_reg<R>(a[q], sign);
-      dft_reg<R>(b[q], sign);
+      if constexpr (CB == 2) dft_reg<R>(b[q], sign);
     }
   }
   __syncthreads();
@@ -133,7 +157,7 @@ __device__ __forceinline__ void stockham_pass(float4* s, int Ns, int sign,
       const int base = (j - k) * R + k;
 #pragma unroll
       for (int m = 0; m < R; m++)
-        s[pad16(base + m * Ns)] = make_float4(a[q][m].x, a[q][m].y, b[q][m].x, b[q][m].y);
+        s[pad16(base + m * Ns)] = CV::make(a[q], b[CB == 2 ? q : 0], m);
     }
   }
   __syncthreads();
@@ -147,26 +171,30 @@ __host__ __device__ constexpr int last_radix(int L) {
   return L / ns;
 }
 
-template <int L>
-__global__ void __launch_bounds__(kFftThreads) k_col_fft(float2* __restrict__ grid, int nf1,
+template <int L, int CB>
+__global__ void __launch_bounds__(kFftThreads, CB == 1 ? 2 : 1) k_col_fft(float2* __restrict__ grid, int nf1,
                                                          size_t plane, int nplanes, int c0a,
                                                          int na, int c0b, int nb, int sign,
                                                          const float2* __restrict__ tw) {
-  extern __shared__ __align__(16) float4 s4[];
-  constexpr int CB = 2;
+  using V = typename ColVec<CB>::type;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V* sv = reinterpret_cast<V*>(smem_raw);
   const int groups_a = na / CB, groups = groups_a + nb / CB;
   const int64_t items = (int64_t)groups * nplanes;
   for (int64_t it = blockIdx.x; it < items; it += gridDim.x) {
     const int p = (int)(it / groups), gi = (int)(it - (int64_t)p * groups);
     const int col0 = gi < groups_a ? c0a + gi * CB : c0b + (gi - groups_a) * CB;
     float2* base = grid + (size_t)p * plane + col0;
-    // one 16-byte asynchronous copy per grid row (the two adjacent columns),
-    // all in flight before the block waits
+    // one asynchronous copy per grid row (the CB adjacent columns), all in
+    // flight before the block waits
 #pragma unroll 4
     for (int j = threadIdx.x; j < L; j += kFftThreads) {
-      const unsigned dst = (unsigned)__cvta_generic_to_shared(s4 + pad16(j));
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(sv + pad16(j));
       const float2* src = base + (size_t)j * nf1;
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+      if constexpr (CB == 2)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+      else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src) : "memory");
     }
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
@@ -174,26 +202,146 @@ __global__ void __launch_bounds__(kFftThreads) k_col_fft(float2* __restrict__ gr
 #pragma unroll 1
     for (; Ns * 16 <= L; Ns *= 16) {
       if (Ns * 16 == L)
-        stockham_pass<L, 16, true>(s4, Ns, sign, tw + toff);
+        stockham_pass<L, 16, CB, true>(sv, Ns, sign, tw + toff);
       else
-        stockham_pass<L, 16, false>(s4, Ns, sign, tw + toff);
+        stockham_pass<L, 16, CB, false>(sv, Ns, sign, tw + toff);
       if (Ns > 1) toff += 16 * Ns;
     }
     constexpr int RL = last_radix(L);
-    if constexpr (RL > 1) stockham_pass<L, RL, true>(s4, Ns, sign, tw + toff);
+    if constexpr (RL > 1) stockham_pass<L, RL, CB, true>(sv, Ns, sign, tw + toff);
 #pragma unroll 4
     for (int j = threadIdx.x; j < L; j += kFftThreads)
-      *reinterpret_cast<float4*>(base + (size_t)j * nf1) = s4[pad16(j)];
+      *reinterpret_cast<V*>(base + (size_t)j * nf1) = sv[pad16(j)];
     __syncthreads();
   }
 }
 
+// Register-resident variant: T = L / 16 threads, each holding 16 points of
+// both columns of the pair in registers for every pass.  Thread t always
+// holds positions t + m T (m < 16): they are the inputs of every radix-16
+// pass and of the last radix-RL pass, and the last pass writes its outputs
+// back to the same positions, so the item is loaded from and stored to those
+// rows directly.  Between passes the Stockham exchange goes through a
+// one-column shared buffer (column 0, then column 1).  A second shared
+// buffer receives the next item by cp.async while the current one is
+// transformed, so loads, passes and stores of consecutive items overlap in
+// one CTA.
 template <int L>
-int launch_l(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, int c0b, int nb,
-             int sign, const float2* tw, cudaStream_t st) {
-  const size_t smem = (size_t)(pad16(L) + 16) * sizeof(float4);
+__global__ void __launch_bounds__(L / 16) k_col_fft_reg(float2* __restrict__ grid, int nf1,
+                                                        size_t plane, int nplanes, int c0a,
+                                                        int na, int c0b, int nb, int sign,
+                                                        const float2* __restrict__ tw) {
+  constexpr int T = L / 16;
+  constexpr int RL = last_radix(L);  // 1: L is a power of 16
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* pre = reinterpret_cast<float4*>(smem_raw);                       // L rows x 2 columns
+  float2* xch = reinterpret_cast<float2*>(smem_raw + (size_t)L * sizeof(float4));  // padded column
+  const int t = threadIdx.x;
+  const int groups_a = na / 2, groups = groups_a + nb / 2;
+  const int64_t items = (int64_t)groups * nplanes;
+  auto base_of = [&](int64_t it) {
+    const int p = (int)(it / groups), gi = (int)(it - (int64_t)p * groups);
+    const int col0 = gi < groups_a ? c0a + gi * 2 : c0b + (gi - groups_a) * 2;
+    return grid + (size_t)p * plane + col0;
+  };
+  auto prefetch = [&](int64_t it) {
+    const float2* b = base_of(it);
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const int row = t + m * T;
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(pre + row);
+      const float2* src = b + (size_t)row * nf1;
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  // Stockham exchange of one column: outputs at o0 + m Ns, inputs back at t + m T
+  auto exchange = [&](float2 (&v)[16], int o0, int Ns) {
+#pragma unroll
+    for (int m = 0; m < 16; m++) xch[pad16(o0 + m * Ns)] = v[m];
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < 16; m++) v[m] = xch[pad16(t + m * T)];
+    __syncthreads();
+  };
+  int64_t it = blockIdx.x;
+  if (it < items) prefetch(it);
+  for (; it < items; it += gridDim.x) {
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    float2 a[16], b[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const float4 v = pre[t + m * T];
+      a[m] = make_float2(v.x, v.y);
+      b[m] = make_float2(v.z, v.w);
+    }
+    __syncthreads();  // the prefetch buffer is free again
+    if (it + gridDim.x < items) prefetch(it + gridDim.x);
+    int Ns = 1, toff = 0;
+#pragma unroll 1
+    for (; Ns * 16 <= L; Ns *= 16) {
+      const int k = t & (Ns - 1);
+      if (Ns > 1) {
+#pragma unroll
+        for (int m = 1; m < 16; m++) {
+          const float2 tv = tw[toff + m * Ns + k];
+          const float2 w = make_float2(tv.x, sign * tv.y);
+          a[m] = cmul(a[m], w);
+          b[m] = cmul(b[m], w);
+        }
+      }
+      dft_reg<16>(a, sign);
+      dft_reg<16>(b, sign);
+      if (Ns * 16 == L) break;  // last pass (L a power of 16): outputs at t + m T
+      const int o0 = (t - k) * 16 + k;
+      exchange(a, o0, Ns);
+      exchange(b, o0, Ns);
+      if (Ns > 1) toff += 16 * Ns;
+    }
+    if constexpr (RL > 1) {
+      // last pass, radix RL, Ns = L / RL: butterfly j = t + q T reads and
+      // writes positions j + m L / RL, i.e. slots q + m (16 / RL) of this thread
+      constexpr int Q = 16 / RL;
+#pragma unroll
+      for (int q = 0; q < Q; q++) {
+        const int j = t + q * T;
+        float2 va[RL], vb[RL];
+#pragma unroll
+        for (int m = 0; m < RL; m++) {
+          va[m] = a[q + m * Q];
+          vb[m] = b[q + m * Q];
+          if (m > 0) {
+            const float2 tv = tw[toff + m * (L / RL) + j];
+            const float2 w = make_float2(tv.x, sign * tv.y);
+            va[m] = cmul(va[m], w);
+            vb[m] = cmul(vb[m], w);
+          }
+        }
+        dft_reg<RL>(va, sign);
+        dft_reg<RL>(vb, sign);
+#pragma unroll
+        for (int m = 0; m < RL; m++) {
+          a[q + m * Q] = va[m];
+          b[q + m * Q] = vb[m];
+        }
+      }
+    }
+    float2* bs = base_of(it);
+#pragma unroll
+    for (int m = 0; m < 16; m++)
+      *reinterpret_cast<float4*>(bs + (size_t)(t + m * T) * nf1) =
+          make_float4(a[m].x, a[m].y, b[m].x, b[m].y);
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+template <int L>
+int launch_reg(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, int c0b, int nb,
+               int sign, const float2* tw, cudaStream_t st) {
+  const size_t smem = (size_t)L * sizeof(float4) + (size_t)(pad16(L) + 16) * sizeof(float2);
   int per_sm = 0;
-  CG_CUDA(kernel_occupancy((const void*)k_col_fft<L>, kFftThreads, smem, &per_sm));
+  CG_CUDA(kernel_occupancy((const void*)k_col_fft_reg<L>, L / 16, smem, &per_sm));
   if (per_sm < 1) return CG_ERR_ARG;
   static int sms = 0;
   if (!sms) {
@@ -203,11 +351,54 @@ int launch_l(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, 
   }
   const int64_t items = (int64_t)(na / 2 + nb / 2) * nplanes;
   const int blocks = (int)std::min<int64_t>(items, (int64_t)per_sm * sms);
-  k_col_fft<L><<<blocks, kFftThreads, smem, st>>>(grid, nf1, plane, nplanes, c0a, na, c0b, nb,
+  k_col_fft_reg<L><<<blocks, L / 16, smem, st>>>(grid, nf1, plane, nplanes, c0a, na, c0b, nb,
                                                  sign, tw);
   count_launches(1);
   CG_CUDA(cudaGetLastError());
   return CG_OK;
+}
+
+// columns per CTA of the shared-memory-resident kernel: two (16-byte rows),
+// or one with CG_COL_FFT_CB=1 (8-byte rows: slower on B200, kept for tests)
+inline int col_fft_cb(int L) {
+  (void)L;
+  const char* e = getenv("CG_COL_FFT_CB");
+  return e && atoi(e) == 1 ? 1 : 2;
+}
+
+template <int L, int CB>
+int launch_lc(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, int c0b, int nb,
+              int sign, const float2* tw, cudaStream_t st) {
+  using V = typename ColVec<CB>::type;
+  const size_t smem = (size_t)(pad16(L) + 16) * sizeof(V);
+  int per_sm = 0;
+  CG_CUDA(kernel_occupancy((const void*)k_col_fft<L, CB>, kFftThreads, smem, &per_sm));
+  if (per_sm < 1) return CG_ERR_ARG;
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
+  }
+  const int64_t items = (int64_t)(na / CB + nb / CB) * nplanes;
+  const int blocks = (int)std::min<int64_t>(items, (int64_t)per_sm * sms);
+  k_col_fft<L, CB><<<blocks, kFftThreads, smem, st>>>(grid, nf1, plane, nplanes, c0a, na, c0b, nb,
+                                                     sign, tw);
+  count_launches(1);
+  CG_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+template <int L>
+int launch_l(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, int c0b, int nb,
+             int sign, const float2* tw, cudaStream_t st) {
+  // CG_COL_FFT_REG=0: the shared-memory-resident kernel instead of the register-resident one
+  const char* e = getenv("CG_COL_FFT_REG");
+  if (!(e && atoi(e) == 0))
+    return launch_reg<L>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st);
+  return col_fft_cb(L) == 1
+             ? launch_lc<L, 1>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st)
+             : launch_lc<L, 2>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st);
 }
 
 }  // namespace

@@ -46,11 +46,24 @@ def _run(torch, d, img, col_fft):
     return dirty.cpu().numpy(), vis.cpu().numpy(), info
 
 
+VARIANTS = {"registers": {}, "shared_pair": {"CG_COL_FFT_REG": "0"},
+            "shared_single": {"CG_COL_FFT_REG": "0", "CG_COL_FFT_CB": "1"}}
+
+
+@pytest.mark.parametrize("variant", sorted(VARIANTS))
 @pytest.mark.parametrize("N", [512, 1024, 2048, 4096])
-def test_column_fft_matches_cufft(torch_cuda, N):
+def test_column_fft_matches_cufft(torch_cuda, N, variant):
+    """Every column kernel: register-resident (default), shared-memory
+    resident with two adjacent columns or one column per CTA."""
     d = _narrow_band_case(N, 100_000, seed=N)
     img = synth.random_image(N, N, seed=2)
-    a = _run(torch_cuda, d, img, True)
+    env = VARIANTS[variant]
+    os.environ.update(env)
+    try:
+        a = _run(torch_cuda, d, img, True)
+    finally:
+        for k in env:
+            del os.environ[k]
     b = _run(torch_cuda, d, img, False)
     assert a[2]["nf2"] == 2 * N
     assert rel_l2(a[0], b[0]) < 2e-6
