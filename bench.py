@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default tilings (no autotuning on the first call)")
     ap.add_argument("--batch", action="store_true",
                     help="the batched workload: 32 uneven datasets (synth.batch_specs), eps 1e-4")
     ap.add_argument("--kernel", default="auto", choices=["auto", "es", "learned"],
@@ -245,6 +247,8 @@ def run_b200(args, rank, world, local):
     from cugridder_b200 import Plan, _lib, dirty2ms_mixed, ms2dirty_mixed, synth  # noqa: F401
 
     torch.cuda.set_device(local)
+    if not args.no_autotune:  # the host entry points' cached plans too (e2e)
+        os.environ["CG_AUTOTUNE"] = "1"
     cfg = synth.CONFIGS[args.config]
     d, img = make_data(args.config, rank, args.nrow, torch, args.fov)
     M = d["uvw"].shape[0]
@@ -274,6 +278,7 @@ def run_b200(args, rank, world, local):
         plan = Plan(nx, ny, fov, args.eps, precision=prec, stream=stream.cuda_stream)
         if kernel is not None and kernel["kind"] == "poly":
             plan.set_kernel("poly", kernel["W"], kernel["coef"])
+        plan.set_autotune(not args.no_autotune)  # tuned in the first warm-up step
 
         def step():
             plan.ms2dirty(uvw, freq, vis, wgt, dirty)
@@ -301,7 +306,10 @@ def run_b200(args, rank, world, local):
         if sample_clocks:
             clocks.stop()
         ms = e0.elapsed_time(e1)
-        out = {"ms": ms, "launches": launches, "info": plan.info()}
+        gt, dt, tms = plan.tiling()
+        out = {"ms": ms, "launches": launches, "info": plan.info(),
+               "tiling": {"grid_warp_tile": list(gt), "degrid_tile": list(dt),
+                          "tuned_launch_ms": [round(x, 3) for x in tms]}}
         if timing:
             out["timing"] = plan.timing()
         if nsamp:
@@ -320,6 +328,7 @@ def run_b200(args, rank, world, local):
     res["ms_per_step"] = t_max / args.steps
     res["gpu_launches"] = int(main["launches"])
     res["info"] = main["info"]
+    res["tiling"] = main["tiling"]
 
     # per-stage timing and roofline of the dominant kernel of this library
     tm = main["timing"]
@@ -702,6 +711,7 @@ def main():
             "config": {"workload": args.config, "nx": cfg["nx"], "ny": cfg["ny"], "fov_deg": args.fov or cfg["fov"],
                        "nrow_per_gpu": args.nrow or cfg["nrow"], "freq_hz": cfg["freq"], "eps": args.eps,
                        "kernel": res["kernel"]["label"], "W": info["kw"], "nw": info["nw"], "grid": [info["nf1"], info["nf2"]],
+                       "tiling": dict(res["tiling"], autotuned=not args.no_autotune),
                        "parallelism": "independent datasets per GPU" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (uvw 480 MB, grid 7.5 GB)"},
             "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res.get("e2e"),

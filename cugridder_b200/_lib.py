@@ -119,6 +119,8 @@ SIGNATURES = {
     "cg_batch_destroy": (c_int, [c_void_p]),
     "cg_batch_get_tiling": (c_int, [c_void_p, c_void_p, c_void_p]),
     "cg_batch_set_kernel": (c_int, [c_void_p, c_int, c_int, c_void_p]),
+    "cg_plan_set_autotune": (c_int, [c_void_p, c_int]),
+    "cg_plan_get_tiling": (c_int, [c_void_p, c_void_p, c_void_p]),
     "cg_release_cache": (c_int, []),
     "cg_last_error": (ctypes.c_char_p, []),
     "cg_kernel_launches": (ctypes.c_longlong, []),

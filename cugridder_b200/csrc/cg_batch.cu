@@ -41,14 +41,6 @@ __global__ void k_chan_scale(const double* __restrict__ uvw, int64_t nrow, int n
   }
 }
 
-// autotuner candidates: gridding warp tiles (wx, wy, planes, warps) and
-// degridding tiles (dx, dy, planes, threads); the first of each is the default
-const int kGridCand[][4] = {{16, 16, 0, 0}, {16, 8, 0, 0},  {32, 16, 0, 0}, {16, 32, 0, 0},
-                            {32, 8, 0, 0},  {16, 16, 4, 0}, {16, 16, 12, 0}, {16, 16, 0, 4}};
-const int kDegridCand[][4] = {{32, 16, 0, 512}, {32, 32, 0, 512}, {32, 8, 0, 512},
-                              {16, 16, 0, 512}, {64, 16, 0, 512}, {32, 16, 0, 256},
-                              {16, 16, 0, 256}, {32, 16, 8, 512}};
-
 }  // namespace
 
 struct cg_batch_s {
@@ -175,14 +167,6 @@ int launch_phase2(cg_batch_s* B, int dir, int njobs, const cg::MultiShape& sh, c
                   : cg::launch_degrid_multi<T>(d_jobs, njobs, sh, counter, st);
 }
 
-void set_tune(cg::TileTune& tt, int dir, const int* c) {
-  if (dir == 0) {
-    tt.wx = c[0]; tt.wy = c[1]; tt.wpb = c[2]; tt.warps = c[3];
-  } else {
-    tt.dx = c[0]; tt.dy = c[1]; tt.dpb = c[2]; tt.dthreads = c[3];
-  }
-}
-
 // First call of a direction (eager): time every candidate tiling of the
 // phase-2 launch on the batch's data (each launch rewrites its whole output,
 // so the repeats are harmless), keep the fastest, upload its jobs.
@@ -192,13 +176,13 @@ int prepare_phase2(cg_batch_s* B, int dir, cudaStream_t st) {
   std::vector<int> order;
   cg::MultiShape sh{};
   if (B->autotune) {
-    const int ncand = dir == 0 ? (int)(sizeof(kGridCand) / sizeof(kGridCand[0]))
-                               : (int)(sizeof(kDegridCand) / sizeof(kDegridCand[0]));
+    const int (*cand)[4] = nullptr;
+    const int ncand = cg::tile_candidates(dir, &cand);
     float best = -1.f;
     cg::TileTune best_tt = B->tune;
     for (int c = 0; c < ncand; c++) {
       cg::TileTune tt = B->tune;
-      set_tune(tt, dir, dir == 0 ? kGridCand[c] : kDegridCand[c]);
+      cg::set_tile_candidate(tt, dir, cand[c]);
       if (build_jobs<T>(B, dir, tt, jobs, order, &sh) != CG_OK || jobs.empty()) continue;
       CG_TRY(upload_jobs<T>(B, dir, jobs, st));
       float ms = 0.f;

@@ -145,6 +145,7 @@ cg_plan_s* cached_plan(int precision, int& status) {
     P = new cg_plan_s();
     P->device = dev;
     P->stream = nullptr;
+    if (const char* m = getenv("CG_AUTOTUNE")) P->autotune = atoi(m) != 0;
   }
   return P;
 }
@@ -364,6 +365,7 @@ int cg_plan_create(cg_plan** plan, int nxdirty, int nydirty, double fov, double 
   }
   if (const char* m = getenv("CG_FFT_PRUNE")) P->fft_pruning = atoi(m) != 0;
   if (const char* m = getenv("CG_COL_FFT")) P->col_fft = atoi(m) != 0;
+  if (const char* m = getenv("CG_AUTOTUNE")) P->autotune = atoi(m) != 0;
   st = cg::plan_configure(P, nxdirty, nydirty, fov, epsilon, sigma, sign, precision);
   if (st > 1) {
     destroy_plan(P);
@@ -500,6 +502,27 @@ int cg_plan_set_fixed_uvw(cg_plan* plan, int on) {
   std::lock_guard<std::mutex> lock(plan->mu);
   plan->fixed_uvw = on != 0;
   plan->bins_valid = false;
+  return CG_OK;
+}
+
+int cg_plan_set_autotune(cg_plan* plan, int on) {
+  if (!plan) return CG_ERR_ARG;
+  std::lock_guard<std::mutex> lock(plan->mu);
+  plan->autotune = on != 0;
+  for (auto& k : plan->tuned_key) std::fill(k, k + 4, 0);
+  if (!on) plan->tune = cg::TileTune{};
+  return CG_OK;
+}
+
+int cg_plan_get_tiling(const cg_plan* plan, int* tiling, float* tuned_ms) {
+  if (!plan || !tiling) return CG_ERR_ARG;
+  const cg::TileTune& t = plan->tune;
+  const int v[8] = {t.wx, t.wy, t.wpb, t.warps, t.dx, t.dy, t.dpb, t.dthreads};
+  std::copy(v, v + 8, tiling);
+  if (tuned_ms) {
+    tuned_ms[0] = plan->tuned_ms[0];
+    tuned_ms[1] = plan->tuned_ms[1];
+  }
   return CG_OK;
 }
 

@@ -40,6 +40,10 @@ TileCfg grid_tiling(const Geom& g, bool degrid, const TileTune* tt = nullptr);
 template <typename T>
 WarpTile warp_tiling(const Geom& g, const TileTune* tt = nullptr);
 int degrid_slots(const TileCfg& tc, int W);
+// Autotuner candidates of direction dir (0 gridding, 1 degridding): rows of
+// {x, y, planes, warps or threads}; set_tile_candidate writes one into tt.
+int tile_candidates(int dir, const int (**cand)[4]);
+void set_tile_candidate(TileTune& tt, int dir, const int* c);
 
 // One grid of a multi-grid launch (batched solves): the plan's sorted stream,
 // hive offsets and grid, its tilings and its first work item in the launch.

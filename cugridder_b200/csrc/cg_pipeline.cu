@@ -629,6 +629,68 @@ static int dirty2ms_windows(cg_plan_s* P, const T* d_dirty, T* d_vis) {
   return CG_OK;
 }
 
+// Autotuning: on the first call per direction for a geometry, time every
+// candidate tiling of the spreading (dir 0) or interpolation (dir 1) launch
+// -- each launch rewrites its whole output, so the repeats are harmless --
+// and keep the fastest in P->tune.
+template <typename T>
+static int autotune_launch(cg_plan_s* P, int dir, T* d_vis) {
+  const Geom& g = P->geom;
+  const int key[4] = {g.nf1, g.nf2, g.nw, g.kw};
+  if (!P->autotune || P->grid_method != kGridTiled ||
+      std::equal(key, key + 4, P->tuned_key[dir]))
+    return CG_OK;
+  cudaStream_t st = P->stream;
+  auto launch = [&](const TileTune& tt) {
+    return dir == 0 ? launch_grid<T>((const Rec<T>*)P->recs.p, (const int*)P->hive_start.p,
+                                     P->nrow, g, (T*)P->grid.p, P->grid_method,
+                                     queue_counter(P), st, &tt)
+                    : launch_degrid<T>((const Rec<T>*)P->recs.p, (const int*)P->perm.p,
+                                       (const int*)P->hive_start.p, P->nrow, g,
+                                       (const T*)P->grid.p, d_vis, P->grid_method,
+                                       queue_counter(P), st, &tt);
+  };
+  cudaEvent_t e0, e1;
+  CG_CUDA(cudaEventCreate(&e0));
+  CG_CUDA(cudaEventCreate(&e1));
+  const int (*cand)[4] = nullptr;
+  const int ncand = tile_candidates(dir, &cand);
+  float best = -1.f;
+  TileTune best_tt = P->tune;
+  int rc = CG_OK;
+  for (int c = 0; c < ncand && rc == CG_OK; c++) {
+    TileTune tt = P->tune;
+    set_tile_candidate(tt, dir, cand[c]);
+    float ms = 0.f;
+    bool ok = true;
+    for (int rep = 0; rep < 2 && ok && rc == CG_OK; rep++) {  // the first launch warms up
+      if (cudaEventRecord(e0, st) != cudaSuccess) rc = CG_ERR_CUDA;
+      ok = launch(tt) == CG_OK;
+      if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+          cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+        rc = CG_ERR_CUDA;
+    }
+    if (!ok) {  // a tiling that does not fit on an SM launched nothing
+      cudaGetLastError();
+      continue;
+    }
+    if (best < 0.f || ms < best) {
+      best = ms;
+      best_tt = tt;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != CG_OK) {
+    set_last_error("autotuning: CUDA event failure");
+    return rc;
+  }
+  P->tune = best_tt;
+  P->tuned_ms[dir] = std::max(best, 0.f);
+  std::copy(key, key + 4, P->tuned_key[dir]);
+  return CG_OK;
+}
+
 // host entry points: wait for the inputs copied on the second stream
 static int wait_inputs(cg_plan_s* P) {
   if (P->inputs_ready) CG_CUDA(cudaStreamWaitEvent(P->stream, P->inputs_ready, 0));
@@ -678,6 +740,7 @@ static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T
     return CG_OK;
   }
   if (part == 1) return CG_OK;
+  CG_TRY(autotune_launch<T>(P, 0, (T*)nullptr));
   CG_TRY(launch_grid<T>((const Rec<T>*)P->recs.p, (const int*)P->hive_start.p, M, g,
                         (T*)P->grid.p, P->grid_method, queue_counter(P), st, &P->tune));
   timer_mark(P);  // 4: gridding
@@ -720,6 +783,7 @@ static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const
                                 false, (Rec<T>*)P->recs_tmp.p, (Rec<T>*)P->recs.p, st));
   timer_mark(P);  // 5: sorted stream
   if (part == 1) return CG_OK;
+  CG_TRY(autotune_launch<T>(P, 1, d_vis));
   CG_TRY(launch_degrid<T>((const Rec<T>*)P->recs.p, (const int*)P->perm.p,
                           (const int*)P->hive_start.p, M, g, (const T*)P->grid.p, d_vis,
                           P->grid_method, queue_counter(P), st, &P->tune));

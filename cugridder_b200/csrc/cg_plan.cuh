@@ -46,7 +46,13 @@ struct cg_plan_s {
   int key_bytes = 4;
   int stop_stage = 0;
   int grid_method = 1;  // 0 direct, 1 tiled SIMT, 2 tensor-core (cg_plan_set_method, CG_GRID_METHOD)
-  cg::TileTune tune{};  // tiling of the tiled kernels (cg_plan_set_tiling; 0 = default)
+  cg::TileTune tune{};  // tiling of the tiled kernels (0 = default)
+  // autotuning (cg_plan_set_autotune, CG_AUTOTUNE): the first call per
+  // direction times the candidate tilings of its spreading / interpolation
+  // launch; tuned_key holds the geometry (nf1, nf2, nw, W) each was tuned for
+  int autotune = 0;
+  int tuned_key[2][4] = {};
+  float tuned_ms[2] = {0.f, 0.f};
   // gridding kernel: CG_KERNEL_ES (W from epsilon) or CG_KERNEL_POLY (W and
   // piecewise-polynomial coefficients given by cg_plan_set_kernel)
   int kernel_kind = CG_KERNEL_ES;

@@ -557,7 +557,7 @@ __device__ __forceinline__ void grid_warp_tile(
 }
 
 template <typename T, int W, bool kPoly>
-__global__ void __launch_bounds__(256) k_grid_warp(const Rec<T>* __restrict__ recs,
+__global__ void __launch_bounds__(512) k_grid_warp(const Rec<T>* __restrict__ recs,
                                                    const int* __restrict__ hive_start, Geom g,
                                                    WarpTile tc, T* __restrict__ fw) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -585,7 +585,7 @@ __device__ __forceinline__ int find_job(const J* __restrict__ jobs, int njobs, i
 // global queue; every job shares W and the kernel.  warp_bytes is the largest
 // per-warp footprint of the jobs' tilings.
 template <typename T, int W, bool kPoly>
-__global__ void __launch_bounds__(256) k_grid_warp_multi(const GridJob<T>* __restrict__ jobs,
+__global__ void __launch_bounds__(512) k_grid_warp_multi(const GridJob<T>* __restrict__ jobs,
                                                          int njobs, int nitems, size_t warp_bytes,
                                                          int* __restrict__ counter) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -784,6 +784,33 @@ TileCfg grid_tiling(const Geom& g, bool degrid, const TileTune* tt) {
 
 int degrid_slots(const TileCfg& tc, int W) { return slots_for(tc.TY, tc.PB, W); }
 
+// Autotuner candidates.  Gridding warp tiles (x, y, planes, warps per CTA):
+// planes 64 = all planes of the grid; 0 = the default.  Degridding tiles
+// (x, y, planes, threads per CTA).  The first of each list is the default.
+static const int kGridCand[][4] = {{16, 16, 0, 0},  {16, 8, 0, 0},  {16, 8, 64, 0},
+                                   {16, 8, 64, 12}, {16, 16, 64, 0}, {32, 8, 0, 0},
+                                   {16, 16, 5, 16}, {16, 16, 0, 12}};
+static const int kDegridCand[][4] = {{32, 16, 0, 512}, {32, 32, 0, 512}, {32, 8, 0, 512},
+                                     {16, 16, 0, 512}, {64, 16, 0, 512}, {32, 16, 0, 256},
+                                     {16, 16, 0, 256}, {32, 16, 8, 512}};
+
+int tile_candidates(int dir, const int (**cand)[4]) {
+  if (dir == 0) {
+    *cand = kGridCand;
+    return (int)(sizeof(kGridCand) / sizeof(kGridCand[0]));
+  }
+  *cand = kDegridCand;
+  return (int)(sizeof(kDegridCand) / sizeof(kDegridCand[0]));
+}
+
+void set_tile_candidate(TileTune& tt, int dir, const int* c) {
+  if (dir == 0) {
+    tt.wx = c[0]; tt.wy = c[1]; tt.wpb = c[2]; tt.warps = c[3];
+  } else {
+    tt.dx = c[0]; tt.dy = c[1]; tt.dpb = c[2]; tt.dthreads = c[3];
+  }
+}
+
 // Warp tiles: 16 x 16 cells by default (CG_WTILE_X / CG_WTILE_Y); the plane
 // batch and warps per CTA are chosen so that two CTAs fit on an SM.
 template <typename T>
@@ -811,7 +838,7 @@ WarpTile warp_tiling(const Geom& g, const TileTune* tt) {
   tc.slots = ((tc.TY >> 3) + 2) * (PB + W) * 3;
   tc.warp_bytes = ((size_t)PB * tc.PS * 2 * sizeof(T) + (size_t)(tc.slots + 1) * 5 * 4 + 15) & ~(size_t)15;
   if (warps <= 0) warps = (int)std::max<size_t>(1, std::min<size_t>(8, (110 * 1024) / tc.warp_bytes));
-  warps = std::min(warps, 8);
+  warps = std::min(warps, 16);
   while (warps > 1 && tc.warp_bytes * warps > 220 * 1024) warps--;
   tc.warps = warps;
   tc.smem = tc.warp_bytes * warps;
@@ -938,7 +965,7 @@ int multi_shape(GridJob<T>* jobs, int njobs, MultiShape* sh) {
   sh->poly = geom_poly_host<T>(jobs[0].g) != nullptr;
   sh->threads = jobs[0].dt.threads;
   int64_t gi = 0, di = 0;
-  int warps = 8;
+  int warps = 16;
   for (int j = 0; j < njobs; j++) {
     GridJob<T>& J = jobs[j];
     if (J.g.kw != sh->kw || (geom_poly_host<T>(J.g) != nullptr) != sh->poly ||

@@ -95,6 +95,17 @@ class Plan:
         a = np.ascontiguousarray(np.asarray(coef, dtype=np.float64).reshape(int(W), 8))
         _lib.check(self._lib.cg_plan_set_kernel(self._h, _lib.CG_KERNEL_POLY, int(W), a.ctypes.data))
 
+    def set_autotune(self, on=True):
+        """Time candidate tilings on the first call per direction and keep the fastest."""
+        _lib.check(self._lib.cg_plan_set_autotune(self._h, 1 if on else 0))
+
+    def tiling(self):
+        """(gridding x, y, planes, warps), (degridding x, y, planes, threads), tuned ms."""
+        t = (ctypes.c_int * 8)()
+        ms = (ctypes.c_float * 2)()
+        _lib.check(self._lib.cg_plan_get_tiling(self._h, ctypes.addressof(t), ctypes.addressof(ms)))
+        return tuple(t[:4]), tuple(t[4:]), (ms[0], ms[1])
+
     def set_fixed_uvw(self, on=True):
         """Reuse geometry and binning while uvw (same array), nrow and freq stay fixed."""
         _lib.check(self._lib.cg_plan_set_fixed_uvw(self._h, 1 if on else 0))

@@ -210,6 +210,17 @@ int cg_plan_set_grid_budget(cg_plan *plan, size_t bytes);
  * disables the reuse. */
 int cg_plan_set_fixed_uvw(cg_plan *plan, int on);
 
+/* Autotuning (no reference counterpart): when on, the first call per
+ * direction for a grid geometry times a fixed list of candidate tilings of
+ * its spreading / interpolation launch (tile size, plane batch, warps or
+ * threads per CTA) on the call's own data and keeps the fastest for later
+ * calls.  Off by default; the environment variable CG_AUTOTUNE=1 turns it on
+ * for plans created afterwards, the host entry points' cached plans
+ * included.  cg_plan_get_tiling reports the tiling in the layout of
+ * cg_batch_get_tiling. */
+int cg_plan_set_autotune(cg_plan *plan, int on);
+int cg_plan_get_tiling(const cg_plan *plan, int *tiling, float *tuned_ms);
+
 /* Stops the next calls after a stage (testing): 0 = run to the end,
  * 1 = after binning, 2 = after gridding (ms2dirty) / plane fill (dirty2ms),
  * 3 = after the FFT. */
