@@ -1,0 +1,362 @@
+// Degridding with TMA-staged grid tiles (FP32 grids, all planes per tile).
+//
+// Same interpolation as k_degrid_tiled (interp_3d_nputsdriven,
+// interp.cu:132-210, restated tile by tile): a persistent CTA per SM takes
+// tiles of TX x TY cells (all nw planes) from a work queue, stages the tile
+// plus the kernel halo in shared memory and interpolates every row of the
+// tile's own hives from there, one row per thread.  Staging here is one
+// cp.async.bulk.tensor.3d box per tile into one of two shared-memory stages:
+// while the rows of one tile are interpolated, the next tile's box is already
+// in flight.  Tiles whose halo wraps around the grid edge are staged element
+// by element (periodic indices); empty tiles are skipped before any staging.
+//
+// TMA rules kept by construction: the box starts at an even x (16-byte
+// aligned for 8-byte elements) and is an even number of elements wide; every
+// start coordinate is >= 0 and the box lies inside the grid (interior tiles
+// only); the global strides are multiples of 16 bytes; the stages are
+// 1024-byte aligned.  Every wait on the stage barriers is bounded; a wait
+// that runs out sets *err and the CTA stops taking tiles.
+#include <cuda.h>
+
+#include <algorithm>
+#include <cstdlib>
+
+#include "cg_coords.cuh"
+#include "cg_launch.cuh"
+#include "cg_tiles.cuh"
+
+namespace cg {
+namespace {
+
+constexpr int kTmaThreads = 512;
+constexpr int kWaitTries = 1 << 20;  // bounded barrier wait (well under a second)
+
+struct TmaTile {
+  int TX, TY;        // tile cells (multiples of 8)
+  int SX, SY, SZ;    // staged box: SX even >= TX + W + 1, SY = TY + W, SZ = nw
+  int ntx, nty, nitems;
+  int nslots;        // segment slots of a tile's own hives
+  size_t stage_bytes;  // one stage, rounded up to 1024 bytes
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+
+// bounded wait for phase `parity` of the barrier; false if it ran out
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  for (int i = 0; i < kWaitTries; i++) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap* map, int x, int y,
+                                            int z, unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];\n" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+
+template <int W>
+__global__ void __launch_bounds__(kTmaThreads, 1) k_degrid_tma(
+    const __grid_constant__ CUtensorMap map, const Rec<float>* __restrict__ recs,
+    const int* __restrict__ perm, const int* __restrict__ hive_start, int64_t M, Geom g,
+    TmaTile tc, const float2* __restrict__ fw, float* __restrict__ vis, int* __restrict__ counter,
+    int* __restrict__ err) {
+  extern __shared__ unsigned char smem_raw[];
+  constexpr int lo = Halo<W>::lo;
+  unsigned char* base =
+      smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);  // 1024-byte aligned
+  float2* stage[2] = {reinterpret_cast<float2*>(base),
+                      reinterpret_cast<float2*>(base + tc.stage_bytes)};
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(base + 2 * tc.stage_bytes);
+  int* tb = reinterpret_cast<int*>(bars + 2);
+  const int ts = tc.nslots + 1;
+  SegTable t{tb, tb + ts, tb + 2 * ts, tb + 3 * ts, tb + 4 * ts};
+  __shared__ int s_warp[33];
+  __shared__ int s_next;
+  const int nw = g.nw, nf1 = g.nf1, nf2 = g.nf2;
+  const int SX = tc.SX, SY = tc.SY, SZ = tc.SZ;
+  const size_t plane = (size_t)nf1 * nf2;
+  const float beta = (float)g.beta, c = (float)g.es_c;
+  const float* __restrict__ poly = geom_poly<float>(g);
+  const unsigned box_bytes = (unsigned)((size_t)SX * SY * SZ * sizeof(float2));
+
+  if (threadIdx.x == 0) {
+    mbar_init(smem_u32(&bars[0]), 1);
+    mbar_init(smem_u32(&bars[1]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  // warp 0: the next tile that holds rows (or nitems when the queue is empty)
+  auto fetch = [&]() {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+      int item = 0;
+      if (lane == 0) item = atomicAdd(counter, 1);
+      item = __shfl_sync(0xffffffffu, item, 0);
+      if (item >= tc.nitems) return tc.nitems;
+      const int tix = item % tc.ntx, tiy = item / tc.ntx;
+      const int tx0 = tix * tc.TX, ty0 = tiy * tc.TY;
+      const int hx0 = tx0 >> 3, hx1 = (min(tx0 + tc.TX, nf1) - 1) >> 3;
+      const int hy0 = ty0 >> 3, nhyr = ((min(ty0 + tc.TY, nf2) - 1) >> 3) - hy0 + 1;
+      int any = 0;
+      for (int r = lane; r < nhyr * nw && !any; r += 32) {
+        const int hy = hy0 + r % nhyr, z = r / nhyr;
+        const int64_t rb = ((int64_t)z * g.nhy + hy) * g.nhx;
+        any = hive_start[rb + hx1 + 1] > hive_start[rb + hx0];
+      }
+      if (__any_sync(0xffffffffu, any)) return item;
+    }
+  };
+  // box origin of a tile (x rounded down to even) and whether it lies inside the grid
+  auto origin = [&](int item, int& gx0, int& gy0) {
+    const int tix = item % tc.ntx, tiy = item / tc.ntx;
+    gx0 = (tix * tc.TX - lo) & ~1;
+    gy0 = tiy * tc.TY - lo;
+    return gx0 >= 0 && gy0 >= 0 && gx0 + SX <= nf1 && gy0 + SY <= nf2;
+  };
+  // all threads: element-by-element staging with periodic indices
+  auto stage_wrapped = [&](int item, float2* dst) {
+    int gx0, gy0;
+    origin(item, gx0, gy0);
+    const int n = SX * SY * SZ;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const int sx = i % SX, sy = (i / SX) % SY, sz = i / (SX * SY);
+      dst[i] = fw[(size_t)sz * plane + (size_t)modi(gy0 + sy, nf2) * nf1 + modi(gx0 + sx, nf1)];
+    }
+  };
+  // thread 0: the box of an interior tile into stage s
+  auto issue = [&](int item, int s) {
+    int gx0, gy0;
+    origin(item, gx0, gy0);
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    const unsigned bar = smem_u32(&bars[s]);
+    mbar_expect_tx(bar, box_bytes);
+    tma_load_3d(smem_u32(stage[s]), &map, gx0, gy0, 0, bar);
+  };
+
+  if (threadIdx.x < 32) {
+    const int it = fetch();
+    if (threadIdx.x == 0) s_next = it;
+  }
+  __syncthreads();
+  int cur = s_next, s = 0;
+  unsigned phase[2] = {0u, 0u};
+  bool pending[2] = {false, false};  // a box issued into the stage and not yet waited for
+  int gx_dummy, gy_dummy;
+  bool cur_tma = cur < tc.nitems && origin(cur, gx_dummy, gy_dummy);
+  if (cur < tc.nitems) {
+    if (cur_tma) {
+      if (threadIdx.x == 0) issue(cur, 0);
+      pending[0] = true;
+    } else {
+      stage_wrapped(cur, stage[0]);
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    }
+  }
+  __syncthreads();
+  while (cur < tc.nitems) {
+    // the next tile: fetched by warp 0, its box issued into the other stage
+    if (threadIdx.x < 32) {
+      const int it = fetch();
+      if (threadIdx.x == 0) s_next = it;
+    }
+    __syncthreads();
+    const int next = s_next;
+    const bool next_tma = next < tc.nitems && origin(next, gx_dummy, gy_dummy);
+    if (next_tma) {
+      if (threadIdx.x == 0) issue(next, s ^ 1);
+      pending[s ^ 1] = true;
+    }
+    // the current tile's box
+    bool ok = true;
+    if (cur_tma) {
+      ok = mbar_wait(smem_u32(&bars[s]), phase[s]);
+      if (ok) {
+        phase[s] ^= 1u;
+        pending[s] = false;
+      }
+    }
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicExch(err, 1);
+      break;
+    }
+    // runs of the tile's own hives, all planes
+    const int tix = cur % tc.ntx, tiy = cur / tc.ntx;
+    const int tx0 = tix * tc.TX, ty0 = tiy * tc.TY;
+    const int tx1 = min(tx0 + tc.TX, nf1), ty1 = min(ty0 + tc.TY, nf2);
+    int gx0, gy0;
+    origin(cur, gx0, gy0);
+    const int nslots = build_segments(g, hive_start, tx0 >> 3, (tx1 - 1) >> 3, ty0 >> 3,
+                                      (ty1 - 1) >> 3, 0, nw - 1, t, s_warp);
+    const int total = t.pref[nslots];
+    const float2* st = stage[s];
+    for (int q = threadIdx.x; q < total; q += blockDim.x) {
+      const int sgi = find_segment(t.pref, nslots, q);
+      const int sidx = t.start[sgi] + (q - t.pref[sgi]);
+      const Rec<float> r = recs[sidx];
+      const int bx = (int)(r.bxy & 0xFFFFu), by = (int)(r.bxy >> 16), bz = (int)r.bz;
+      float kx[W], ky[W], kz[W];
+      const int lx = bx + taps<float, W>(r.f[0], beta, c, poly, kx) - gx0;
+      const int ly = by + taps<float, W>(r.f[1], beta, c, poly, ky) - gy0;
+      const int lz = bz + taps<float, W>(r.f[2], beta, c, poly, kz);
+      if (lx < 0 || ly < 0 || lx + W > SX || ly + W > SY) continue;  // cannot happen: tile rows only
+      float sr = 0.f, si = 0.f;
+      for (int a = 0; a < W; a++) {
+        const int zz = wrapi(lz + a, nw);
+        float pr = 0.f, pi = 0.f;
+        for (int b = 0; b < W; b++) {
+          const float2* row = st + ((size_t)zz * SY + (ly + b)) * SX + lx;
+          float qr = 0.f, qi = 0.f;
+#pragma unroll
+          for (int e = 0; e < W; e++) {
+            const float2 v = row[e];
+            qr += v.x * kx[e];
+            qi += v.y * kx[e];
+          }
+          pr += qr * ky[b];
+          pi += qi * ky[b];
+        }
+        sr += pr * kz[a];
+        si += pi * kz[a];
+      }
+      const int64_t i = perm[sidx];
+      if (i < 0 || i >= M) continue;
+      vis[2 * i] = sr * r.c[0] - si * r.c[1];
+      vis[2 * i + 1] = sr * r.c[1] + si * r.c[0];
+    }
+    // generic reads of stage s before the box that will overwrite it
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();  // stage s and the segment table are free again
+    s ^= 1;
+    cur = next;
+    cur_tma = next_tma;
+    if (cur < tc.nitems && !cur_tma) {
+      stage_wrapped(cur, stage[s]);
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      __syncthreads();
+    }
+  }
+  // after a timed-out wait boxes may still be in flight: wait for them
+  // (bounded) before the CTA's shared memory is released
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 2; k++)
+      if (pending[k]) mbar_wait(smem_u32(&bars[k]), phase[k]);
+}
+
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                 const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_fn() {
+  static EncodeTiled fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiled>(p);
+  }
+  return fn;
+}
+
+bool tma_tiling(const Geom& g, TmaTile& tc) {
+  const int W = g.kw;
+  const int tx = 32, ty = 16;
+  tc.TX = tx;
+  tc.TY = ty;
+  tc.SX = (tx + W + 1 + 1) & ~1;
+  tc.SY = ty + W;
+  tc.SZ = g.nw;
+  tc.ntx = (g.nf1 + tx - 1) / tx;
+  tc.nty = (g.nf2 + ty - 1) / ty;
+  tc.nitems = tc.ntx * tc.nty;
+  tc.nslots = ((ty >> 3) + 1) * g.nw * 3;
+  tc.stage_bytes = ((size_t)tc.SX * tc.SY * tc.SZ * sizeof(float2) + 1023) & ~(size_t)1023;
+  const size_t smem = 1024 + 2 * tc.stage_bytes + 16 + (size_t)(tc.nslots + 1) * 5 * 4;
+  // box dimensions <= 256, grid rows 16-byte multiples, two stages on one SM
+  return g.nw <= 256 && tc.SX <= 256 && tc.SY <= 256 && (g.nf1 % 2) == 0 &&
+         g.nf1 >= tc.SX && g.nf2 >= tc.SY && smem <= 220 * 1024;
+}
+
+template <int W>
+int launch_w(const Rec<float>* d_recs, const int* d_perm, const int* d_hive_start, int64_t M,
+             const Geom& g, const TmaTile& tc, const float* d_fw, float* d_vis, int* d_counter,
+             int* d_err, cudaStream_t st) {
+  EncodeTiled enc = encode_fn();
+  if (!enc) return CG_ERR_ARG;
+  CUtensorMap map;
+  const cuuint64_t dims[3] = {(cuuint64_t)g.nf1, (cuuint64_t)g.nf2, (cuuint64_t)g.nw};
+  const cuuint64_t strides[2] = {(cuuint64_t)g.nf1 * sizeof(float2),
+                                 (cuuint64_t)g.nf1 * g.nf2 * sizeof(float2)};
+  const cuuint32_t box[3] = {(cuuint32_t)tc.SX, (cuuint32_t)tc.SY, (cuuint32_t)tc.SZ};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, (void*)d_fw, dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return CG_ERR_ARG;
+  const size_t smem = 1024 + 2 * tc.stage_bytes + 16 + (size_t)(tc.nslots + 1) * 5 * 4;
+  int per_sm = 0;
+  CG_CUDA(kernel_occupancy((const void*)k_degrid_tma<W>, kTmaThreads, smem, &per_sm));
+  if (per_sm < 1) return CG_ERR_ARG;
+  int sms = 0, dev = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
+  const int blocks = std::min(tc.nitems, per_sm * sms);
+  CG_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(int), st));
+  k_degrid_tma<W><<<blocks, kTmaThreads, smem, st>>>(map, d_recs, d_perm, d_hive_start, M, g, tc,
+                                                     (const float2*)d_fw, d_vis, d_counter, d_err);
+  count_launches(1);
+  CG_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+}  // namespace
+
+bool degrid_tma_supported(const Geom& g) {
+  TmaTile tc{};
+  if (g.kw < 4 || g.kw > 8 || !tma_tiling(g, tc)) return false;
+  const char* e = getenv("CG_DEGRID_TMA");
+  return !(e && atoi(e) == 0) && encode_fn() != nullptr;
+}
+
+int launch_degrid_tma(const Rec<float>* d_recs, const int* d_perm, const int* d_hive_start,
+                      int64_t M, const Geom& g, const float* d_fw, float* d_vis, int* d_counter,
+                      int* d_err, cudaStream_t st) {
+  if (M == 0) return CG_OK;
+  TmaTile tc{};
+  if (!tma_tiling(g, tc)) return CG_ERR_ARG;
+  switch (g.kw) {
+    case 4: return launch_w<4>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis, d_counter, d_err, st);
+    case 5: return launch_w<5>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis, d_counter, d_err, st);
+    case 6: return launch_w<6>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis, d_counter, d_err, st);
+    case 7: return launch_w<7>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis, d_counter, d_err, st);
+    case 8: return launch_w<8>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis, d_counter, d_err, st);
+    default: return CG_ERR_ARG;
+  }
+}
+
+}  // namespace cg

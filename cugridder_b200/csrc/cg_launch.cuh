@@ -94,6 +94,13 @@ int launch_degrid(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_sta
                   const Geom& g, const T* d_fw, T* d_vis, int method, int* d_counter,
                   cudaStream_t st, const TileTune* tt = nullptr);
 
+// ---- degridding with TMA-staged tiles (cg_degrid_tma.cu; FP32, W 4..8) ----
+// d_err: a device int set to 1 when a staging wait ran out (the host checks it)
+bool degrid_tma_supported(const Geom& g);
+int launch_degrid_tma(const Rec<float>* d_recs, const int* d_perm, const int* d_hive_start,
+                      int64_t M, const Geom& g, const float* d_fw, float* d_vis, int* d_counter,
+                      int* d_err, cudaStream_t st);
+
 // ---- column FFTs in shared memory (cg_fft.cu) ----
 bool col_fft_supported(int L, int na, int nb);
 size_t col_fft_twiddle_count(int L);

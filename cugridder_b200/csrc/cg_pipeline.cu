@@ -316,13 +316,18 @@ static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw)
   }
   cudaStream_t st = P->stream;
   CG_TRY(ensure(P->mm, 128));
-  if (!P->h_mm) CG_CUDA(cudaMallocHost(&P->h_mm, 64));
+  if (!P->h_mm) CG_CUDA(cudaMallocHost(&P->h_mm, 128));
   unsigned long long* d_mm = (unsigned long long*)P->mm.p;
   int* d_bad = (int*)(d_mm + 6);
   CG_TRY(launch_wminmax(d_uvw, nrow, d_mm, d_bad, st));
-  CG_CUDA(cudaMemcpyAsync(P->h_mm, d_mm, 52, cudaMemcpyDeviceToHost, st));
+  CG_CUDA(cudaMemcpyAsync(P->h_mm, d_mm, 80, cudaMemcpyDeviceToHost, st));
   CG_CUDA(cudaStreamSynchronize(st));
   timer_flush(P, P->timer.cur ^ 1);
+  if (P->tma_armed && ((const int*)P->h_mm)[18]) {  // word 72: a TMA staging wait ran out
+    CG_CUDA(cudaMemsetAsync((char*)P->mm.p + 72, 0, sizeof(int), st));
+    set_last_error("degridding: a TMA staging wait timed out in an earlier call");
+    return CG_ERR_CUDA;
+  }
   if (((int*)(P->h_mm + 6))[0]) {
     set_last_error("non-finite uvw coordinate");
     return CG_ERR_ARG;
@@ -456,6 +461,33 @@ static int fft_exec(cg_plan_s* P, void* d_grid, int direction) {
 
 // work-queue head of the tiled kernels: a word of the small scratch buffer
 static int* queue_counter(cg_plan_s* P) { return (int*)((char*)P->mm.p + 64); }
+// error word of the TMA-staged degridding (read back by the next prepare)
+static int* tma_error_word(cg_plan_s* P) { return (int*)((char*)P->mm.p + 72); }
+
+// Degridding launch for tiling tt: threads -1 selects the TMA-staged kernel
+// (FP32 where it applies), anything else the tiled kernel.
+template <typename T>
+static int degrid_dispatch(cg_plan_s* P, const TileTune& tt, T* d_vis) {
+  const Geom& g = P->geom;
+  if (tt.dthreads < 0 || (tt.dthreads == 0 && P->tma_default)) {
+    if constexpr (sizeof(T) == 4) {
+      if (P->grid_method == kGridTiled && degrid_tma_supported(g)) {
+        if (!P->tma_armed) {
+          CG_CUDA(cudaMemsetAsync(tma_error_word(P), 0, sizeof(int), P->stream));
+          P->tma_armed = true;
+        }
+        return launch_degrid_tma((const Rec<float>*)P->recs.p, (const int*)P->perm.p,
+                                 (const int*)P->hive_start.p, P->nrow, g,
+                                 (const float*)P->grid.p, (float*)d_vis, queue_counter(P),
+                                 tma_error_word(P), P->stream);
+      }
+    }
+    if (tt.dthreads < 0) return CG_ERR_ARG;  // a tuning candidate that does not apply
+  }
+  return launch_degrid<T>((const Rec<T>*)P->recs.p, (const int*)P->perm.p,
+                          (const int*)P->hive_start.p, P->nrow, g, (const T*)P->grid.p, d_vis,
+                          P->grid_method, queue_counter(P), P->stream, &tt);
+}
 
 // 1-D cuFFT plans of the band-pruned transform (work areas shared with the
 // 2-D plan's buffer; the plans run one after another on the plan's stream).
@@ -645,10 +677,7 @@ static int autotune_launch(cg_plan_s* P, int dir, T* d_vis) {
     return dir == 0 ? launch_grid<T>((const Rec<T>*)P->recs.p, (const int*)P->hive_start.p,
                                      P->nrow, g, (T*)P->grid.p, P->grid_method,
                                      queue_counter(P), st, &tt)
-                    : launch_degrid<T>((const Rec<T>*)P->recs.p, (const int*)P->perm.p,
-                                       (const int*)P->hive_start.p, P->nrow, g,
-                                       (const T*)P->grid.p, d_vis, P->grid_method,
-                                       queue_counter(P), st, &tt);
+                    : degrid_dispatch<T>(P, tt, d_vis);
   };
   cudaEvent_t e0, e1;
   CG_CUDA(cudaEventCreate(&e0));
@@ -784,9 +813,7 @@ static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const
   timer_mark(P);  // 5: sorted stream
   if (part == 1) return CG_OK;
   CG_TRY(autotune_launch<T>(P, 1, d_vis));
-  CG_TRY(launch_degrid<T>((const Rec<T>*)P->recs.p, (const int*)P->perm.p,
-                          (const int*)P->hive_start.p, M, g, (const T*)P->grid.p, d_vis,
-                          P->grid_method, queue_counter(P), st, &P->tune));
+  CG_TRY(degrid_dispatch<T>(P, P->tune, d_vis));
   timer_mark(P);  // 6: degridding
   return CG_OK;
 }

@@ -1,0 +1,119 @@
+// Tile helpers shared by the tiled spreading / interpolation kernels: the
+// kernel halo, and the segment table that lists a tile's sorted rows as
+// contiguous runs of hives (with the periodic shift of each run).
+#pragma once
+#include "cg_internal.cuh"
+
+namespace cg {
+
+// halo of the taps: a row in cell b touches cells [b - lo, b + hi]
+template <int W>
+struct Halo {
+  static constexpr int lo = (W - 1) / 2;
+  static constexpr int hi = (W + 1) / 2;
+};
+
+__device__ __forceinline__ int floordiv8(int a) { return a >= 0 ? a >> 3 : -((7 - a) >> 3); }
+
+// Segment table of one work item: contiguous runs of sorted rows (hives that
+// are neighbours along x share one run) with the periodic shift of their cells.
+struct SegTable {
+  int* start;
+  int* pref;  // exclusive prefix of the run lengths, pref[nslots] = total
+  int* sx;
+  int* sy;
+  int* sz;
+};
+
+// Build the runs for hive rows hy in [hya, hyb], planes hz in [za, zb] (raw,
+// possibly outside the grid: wrapped with a shift of -+nf / -+nw) and hive
+// columns [hxa, hxb].  Three slots per (hz, hy) row (left wrap, inside, right
+// wrap).  Returns the number of slots.  Must be called by all threads.
+__device__ inline int build_segments(const Geom& g, const int* __restrict__ hive_start, int hxa, int hxb,
+                              int hya, int hyb, int za, int zb, SegTable t, int* s_warp) {
+  const int ny_raw = hyb - hya + 1, nz_raw = zb - za + 1;
+  const int rows = ny_raw * nz_raw;
+  const int nslots = rows * 3;
+  const int nhx = g.nhx, nhy = g.nhy, nw = g.nw;
+  for (int base = 0; base < rows; base += blockDim.x) {
+    const int r = base + threadIdx.x;
+    int cnt[3] = {0, 0, 0};
+    if (r < rows) {
+      const int hy_raw = hya + r % ny_raw, hz_raw = za + r / ny_raw;
+      int hy = hy_raw, shy = 0;
+      if (hy < 0) { hy += nhy; shy = -g.nf2; }
+      else if (hy >= nhy) { hy -= nhy; shy = g.nf2; }
+      int hz = hz_raw, shz = 0;
+      if (hz < 0) { hz += nw; shz = -nw; }
+      else if (hz >= nw) { hz -= nw; shz = nw; }
+      const int64_t rowbase = ((int64_t)hz * nhy + hy) * nhx;
+      // part k: raw hx range and actual offset
+      const int lo_k[3] = {hxa, max(hxa, 0), max(hxa, nhx)};
+      const int hi_k[3] = {min(hxb, -1), min(hxb, nhx - 1), hxb};
+      const int off_k[3] = {nhx, 0, -nhx};
+      const int shx_k[3] = {-g.nf1, 0, g.nf1};
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        const int slot = r * 3 + k;
+        int st = 0, c = 0;
+        if (lo_k[k] <= hi_k[k]) {
+          const int64_t h0 = rowbase + lo_k[k] + off_k[k];
+          const int64_t h1 = rowbase + hi_k[k] + off_k[k];
+          st = hive_start[h0];
+          c = hive_start[h1 + 1] - st;
+        }
+        t.start[slot] = st;
+        t.sx[slot] = shx_k[k];
+        t.sy[slot] = shy;
+        t.sz[slot] = shz;
+        cnt[k] = c;
+      }
+    }
+    // exclusive scan of the per-row sums across the block
+    const int sum = cnt[0] + cnt[1] + cnt[2];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int inc = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    if (lane == 31) s_warp[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+      const int nwarps = blockDim.x >> 5;
+      int v = lane < nwarps ? s_warp[lane] : 0, vi = v;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, vi, o);
+        if (lane >= o) vi += y;
+      }
+      s_warp[lane] = vi - v;
+      if (lane == 31) s_warp[32] = vi;
+    }
+    __syncthreads();
+    const int carry = (base == 0) ? 0 : t.pref[base * 3];
+    const int ex = carry + s_warp[warp] + inc - sum;
+    const int total = s_warp[32];
+    if (r < rows) {
+      t.pref[r * 3] = ex;
+      t.pref[r * 3 + 1] = ex + cnt[0];
+      t.pref[r * 3 + 2] = ex + cnt[0] + cnt[1];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) t.pref[min(base + (int)blockDim.x, rows) * 3] = carry + total;
+    __syncthreads();
+  }
+  return nslots;
+}
+
+__device__ __forceinline__ int find_segment(const int* __restrict__ pref, int nslots, int q) {
+  int lo = 0, hi = nslots;  // pref[lo] <= q < pref[hi]
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (pref[mid] <= q) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+}  // namespace cg
