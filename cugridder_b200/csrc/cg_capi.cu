@@ -146,7 +146,7 @@ cg_plan_s* cached_plan(int precision, int& status) {
     P->device = dev;
     P->stream = nullptr;
     if (const char* m = getenv("CG_AUTOTUNE")) P->autotune = atoi(m) != 0;
-    if (const char* m = getenv("CG_DEGRID_TMA")) P->tma_default = atoi(m) != 0;
+    if (const char* m = getenv("CG_DEGRID_TMA")) P->tma_default = atoi(m);
   }
   return P;
 }
@@ -367,7 +367,7 @@ int cg_plan_create(cg_plan** plan, int nxdirty, int nydirty, double fov, double 
   if (const char* m = getenv("CG_FFT_PRUNE")) P->fft_pruning = atoi(m) != 0;
   if (const char* m = getenv("CG_COL_FFT")) P->col_fft = atoi(m) != 0;
   if (const char* m = getenv("CG_AUTOTUNE")) P->autotune = atoi(m) != 0;
-  if (const char* m = getenv("CG_DEGRID_TMA")) P->tma_default = atoi(m) != 0;
+  if (const char* m = getenv("CG_DEGRID_TMA")) P->tma_default = atoi(m);
   st = cg::plan_configure(P, nxdirty, nydirty, fov, epsilon, sigma, sign, precision);
   if (st > 1) {
     destroy_plan(P);

@@ -28,7 +28,6 @@
 namespace cg {
 namespace {
 
-constexpr int kTmaThreads = 512;
 constexpr int kWaitTries = 1 << 20;  // bounded barrier wait (well under a second)
 
 struct TmaTile {
@@ -76,8 +75,11 @@ __device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap* map
       : "memory");
 }
 
-template <int W>
-__global__ void __launch_bounds__(kTmaThreads, 1) k_degrid_tma(
+// NT threads per CTA; NS stages: 2 = the next tile's box in flight while the
+// current one is interpolated (one CTA per SM), 1 = one box at a time (two
+// CTAs per SM overlap each other's staging and interpolation)
+template <int W, int NT, int NS>
+__global__ void __launch_bounds__(NT, NS == 1 ? 2 : 1) k_degrid_tma(
     const __grid_constant__ CUtensorMap map, const Rec<float>* __restrict__ recs,
     const int* __restrict__ perm, const int* __restrict__ hive_start, int64_t M, Geom g,
     TmaTile tc, const float2* __restrict__ fw, float* __restrict__ vis, int* __restrict__ counter,
@@ -87,8 +89,8 @@ __global__ void __launch_bounds__(kTmaThreads, 1) k_degrid_tma(
   unsigned char* base =
       smem_raw + ((1024 - (smem_u32(smem_raw) & 1023)) & 1023);  // 1024-byte aligned
   float2* stage[2] = {reinterpret_cast<float2*>(base),
-                      reinterpret_cast<float2*>(base + tc.stage_bytes)};
-  unsigned long long* bars = reinterpret_cast<unsigned long long*>(base + 2 * tc.stage_bytes);
+                      reinterpret_cast<float2*>(base + (NS - 1) * tc.stage_bytes)};
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(base + NS * tc.stage_bytes);
   int* tb = reinterpret_cast<int*>(bars + 2);
   const int ts = tc.nslots + 1;
   SegTable t{tb, tb + ts, tb + 2 * ts, tb + 3 * ts, tb + 4 * ts};
@@ -183,7 +185,7 @@ __global__ void __launch_bounds__(kTmaThreads, 1) k_degrid_tma(
     __syncthreads();
     const int next = s_next;
     const bool next_tma = next < tc.nitems && origin(next, gx_dummy, gy_dummy);
-    if (next_tma) {
+    if (NS == 2 && next_tma) {
       if (threadIdx.x == 0) issue(next, s ^ 1);
       pending[s ^ 1] = true;
     }
@@ -247,13 +249,18 @@ __global__ void __launch_bounds__(kTmaThreads, 1) k_degrid_tma(
     // generic reads of stage s before the box that will overwrite it
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();  // stage s and the segment table are free again
-    s ^= 1;
+    if (NS == 2) s ^= 1;
     cur = next;
     cur_tma = next_tma;
-    if (cur < tc.nitems && !cur_tma) {
-      stage_wrapped(cur, stage[s]);
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      __syncthreads();
+    if (cur < tc.nitems) {
+      if (!cur_tma) {
+        stage_wrapped(cur, stage[s]);
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncthreads();
+      } else if (NS == 1) {
+        if (threadIdx.x == 0) issue(cur, 0);
+        pending[0] = true;
+      }
     }
   }
   // after a timed-out wait boxes may still be in flight: wait for them
@@ -283,7 +290,13 @@ EncodeTiled encode_fn() {
   return fn;
 }
 
-bool tma_tiling(const Geom& g, TmaTile& tc) {
+// shared memory of one CTA with NS stages
+size_t tma_smem(const TmaTile& tc, int ns) {
+  return 1024 + ns * tc.stage_bytes + 16 + (size_t)(tc.nslots + 1) * 5 * 4;
+}
+
+// variant 1: 512 threads, two stages; variant 2: 256 threads, one stage
+bool tma_tiling(const Geom& g, TmaTile& tc, int variant) {
   const int W = g.kw;
   const int tx = 32, ty = 16;
   tc.TX = tx;
@@ -296,13 +309,15 @@ bool tma_tiling(const Geom& g, TmaTile& tc) {
   tc.nitems = tc.ntx * tc.nty;
   tc.nslots = ((ty >> 3) + 1) * g.nw * 3;
   tc.stage_bytes = ((size_t)tc.SX * tc.SY * tc.SZ * sizeof(float2) + 1023) & ~(size_t)1023;
-  const size_t smem = 1024 + 2 * tc.stage_bytes + 16 + (size_t)(tc.nslots + 1) * 5 * 4;
-  // box dimensions <= 256, grid rows 16-byte multiples, two stages on one SM
-  return g.nw <= 256 && tc.SX <= 256 && tc.SY <= 256 && (g.nf1 % 2) == 0 &&
-         g.nf1 >= tc.SX && g.nf2 >= tc.SY && smem <= 220 * 1024;
+  // box dimensions <= 256, grid rows 16-byte multiples; two stages on one
+  // SM (variant 1) or two one-stage CTAs on one SM (variant 2)
+  const size_t limit = variant == 2 ? 110 * 1024 : 220 * 1024;
+  return (variant == 1 || variant == 2) && g.nw <= 256 && tc.SX <= 256 && tc.SY <= 256 &&
+         (g.nf1 % 2) == 0 && g.nf1 >= tc.SX && g.nf2 >= tc.SY &&
+         tma_smem(tc, variant == 2 ? 1 : 2) <= limit;
 }
 
-template <int W>
+template <int W, int NT, int NS>
 int launch_w(const Rec<float>* d_recs, const int* d_perm, const int* d_hive_start, int64_t M,
              const Geom& g, const TmaTile& tc, const float* d_fw, float* d_vis, int* d_counter,
              int* d_err, cudaStream_t st) {
@@ -318,17 +333,17 @@ int launch_w(const Rec<float>* d_recs, const int* d_perm, const int* d_hive_star
           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return CG_ERR_ARG;
-  const size_t smem = 1024 + 2 * tc.stage_bytes + 16 + (size_t)(tc.nslots + 1) * 5 * 4;
+  const size_t smem = tma_smem(tc, NS);
   int per_sm = 0;
-  CG_CUDA(kernel_occupancy((const void*)k_degrid_tma<W>, kTmaThreads, smem, &per_sm));
+  CG_CUDA(kernel_occupancy((const void*)k_degrid_tma<W, NT, NS>, NT, smem, &per_sm));
   if (per_sm < 1) return CG_ERR_ARG;
   int sms = 0, dev = 0;
   cudaGetDevice(&dev);
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
   const int blocks = std::min(tc.nitems, per_sm * sms);
   CG_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(int), st));
-  k_degrid_tma<W><<<blocks, kTmaThreads, smem, st>>>(map, d_recs, d_perm, d_hive_start, M, g, tc,
-                                                     (const float2*)d_fw, d_vis, d_counter, d_err);
+  k_degrid_tma<W, NT, NS><<<blocks, NT, smem, st>>>(map, d_recs, d_perm, d_hive_start, M, g, tc,
+                                                    (const float2*)d_fw, d_vis, d_counter, d_err);
   count_launches(1);
   CG_CUDA(cudaGetLastError());
   return CG_OK;
@@ -336,27 +351,33 @@ int launch_w(const Rec<float>* d_recs, const int* d_perm, const int* d_hive_star
 
 }  // namespace
 
-bool degrid_tma_supported(const Geom& g) {
+bool degrid_tma_supported(const Geom& g, int variant) {
   TmaTile tc{};
-  if (g.kw < 4 || g.kw > 8 || !tma_tiling(g, tc)) return false;
+  if (g.kw < 4 || g.kw > 8 || !tma_tiling(g, tc, variant)) return false;
   const char* e = getenv("CG_DEGRID_TMA");
   return !(e && atoi(e) == 0) && encode_fn() != nullptr;
 }
 
 int launch_degrid_tma(const Rec<float>* d_recs, const int* d_perm, const int* d_hive_start,
                       int64_t M, const Geom& g, const float* d_fw, float* d_vis, int* d_counter,
-                      int* d_err, cudaStream_t st) {
+                      int* d_err, cudaStream_t st, int variant) {
   if (M == 0) return CG_OK;
   TmaTile tc{};
-  if (!tma_tiling(g, tc)) return CG_ERR_ARG;
+  if (!tma_tiling(g, tc, variant)) return CG_ERR_ARG;
+#define CG_TMA_CALL(w)                                                                        \
+  (variant == 2 ? launch_w<w, 256, 1>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis,    \
+                                      d_counter, d_err, st)                                 \
+                : launch_w<w, 512, 2>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis,    \
+                                      d_counter, d_err, st))
   switch (g.kw) {
-    case 4: return launch_w<4>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis, d_counter, d_err, st);
-    case 5: return launch_w<5>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis, d_counter, d_err, st);
-    case 6: return launch_w<6>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis, d_counter, d_err, st);
-    case 7: return launch_w<7>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis, d_counter, d_err, st);
-    case 8: return launch_w<8>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis, d_counter, d_err, st);
+    case 4: return CG_TMA_CALL(4);
+    case 5: return CG_TMA_CALL(5);
+    case 6: return CG_TMA_CALL(6);
+    case 7: return CG_TMA_CALL(7);
+    case 8: return CG_TMA_CALL(8);
     default: return CG_ERR_ARG;
   }
+#undef CG_TMA_CALL
 }
 
 }  // namespace cg

@@ -96,10 +96,11 @@ int launch_degrid(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_sta
 
 // ---- degridding with TMA-staged tiles (cg_degrid_tma.cu; FP32, W 4..8) ----
 // d_err: a device int set to 1 when a staging wait ran out (the host checks it)
-bool degrid_tma_supported(const Geom& g);
+// variant 1: 512 threads and two stages per CTA; 2: 256 threads and one stage, two CTAs per SM
+bool degrid_tma_supported(const Geom& g, int variant);
 int launch_degrid_tma(const Rec<float>* d_recs, const int* d_perm, const int* d_hive_start,
                       int64_t M, const Geom& g, const float* d_fw, float* d_vis, int* d_counter,
-                      int* d_err, cudaStream_t st);
+                      int* d_err, cudaStream_t st, int variant);
 
 // ---- column FFTs in shared memory (cg_fft.cu) ----
 bool col_fft_supported(int L, int na, int nb);

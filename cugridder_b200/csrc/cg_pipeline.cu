@@ -464,14 +464,16 @@ static int* queue_counter(cg_plan_s* P) { return (int*)((char*)P->mm.p + 64); }
 // error word of the TMA-staged degridding (read back by the next prepare)
 static int* tma_error_word(cg_plan_s* P) { return (int*)((char*)P->mm.p + 72); }
 
-// Degridding launch for tiling tt: threads -1 selects the TMA-staged kernel
-// (FP32 where it applies), anything else the tiled kernel.
+// Degridding launch for tiling tt: threads -1 / -2 select the TMA-staged
+// kernel's variant 1 / 2 (FP32 where it applies), anything else the tiled
+// kernel; untuned plans take variant tma_default (0: the tiled kernel).
 template <typename T>
 static int degrid_dispatch(cg_plan_s* P, const TileTune& tt, T* d_vis) {
   const Geom& g = P->geom;
-  if (tt.dthreads < 0 || (tt.dthreads == 0 && P->tma_default)) {
+  const int variant = tt.dthreads < 0 ? -tt.dthreads : (tt.dthreads == 0 ? P->tma_default : 0);
+  if (variant > 0) {
     if constexpr (sizeof(T) == 4) {
-      if (P->grid_method == kGridTiled && degrid_tma_supported(g)) {
+      if (P->grid_method == kGridTiled && degrid_tma_supported(g, variant)) {
         if (!P->tma_armed) {
           CG_CUDA(cudaMemsetAsync(tma_error_word(P), 0, sizeof(int), P->stream));
           P->tma_armed = true;
@@ -479,7 +481,7 @@ static int degrid_dispatch(cg_plan_s* P, const TileTune& tt, T* d_vis) {
         return launch_degrid_tma((const Rec<float>*)P->recs.p, (const int*)P->perm.p,
                                  (const int*)P->hive_start.p, P->nrow, g,
                                  (const float*)P->grid.p, (float*)d_vis, queue_counter(P),
-                                 tma_error_word(P), P->stream);
+                                 tma_error_word(P), P->stream, variant);
       }
     }
     if (tt.dthreads < 0) return CG_ERR_ARG;  // a tuning candidate that does not apply

@@ -52,7 +52,7 @@ struct cg_plan_s {
   // launch; tuned_key holds the geometry (nf1, nf2, nw, W) each was tuned for
   int autotune = 0;
   bool tma_armed = false;  // the TMA degridding error word has been cleared once
-  bool tma_default = true;  // untuned tiling: TMA-staged degridding where it applies (CG_DEGRID_TMA=0: off)
+  int tma_default = 2;  // untuned tiling: TMA-staged degridding variant where it applies (CG_DEGRID_TMA: 0 off, 1, 2)
   int tuned_key[2][4] = {};
   float tuned_ms[2] = {0.f, 0.f};
   // gridding kernel: CG_KERNEL_ES (W from epsilon) or CG_KERNEL_POLY (W and
