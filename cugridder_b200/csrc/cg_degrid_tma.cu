@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(NT, NS == 1 ? 2 : 1) k_degrid_tma(
   unsigned long long* bars = reinterpret_cast<unsigned long long*>(base + NS * tc.stage_bytes);
   int* tb = reinterpret_cast<int*>(bars + 2);
   const int ts = tc.nslots + 1;
-  SegTable t{tb, tb + ts, tb + 2 * ts, tb + 3 * ts, tb + 4 * ts};
+  SegTable t{tb, tb + ts, tb + 2 * ts};
   __shared__ int s_warp[33];
   __shared__ int s_next;
   const int nw = g.nw, nf1 = g.nf1, nf2 = g.nf2;
@@ -292,7 +292,7 @@ EncodeTiled encode_fn() {
 
 // shared memory of one CTA with NS stages
 size_t tma_smem(const TmaTile& tc, int ns) {
-  return 1024 + ns * tc.stage_bytes + 16 + (size_t)(tc.nslots + 1) * 5 * 4;
+  return 1024 + ns * tc.stage_bytes + 16 + (size_t)(tc.nslots + 1) * kSegInts * 4;
 }
 
 // variant 1: 512 threads, two stages; variant 2: 256 threads, one stage

@@ -183,9 +183,7 @@ __device__ int warp_build_segments(const Geom& g, const int* __restrict__ hive_s
           c = hive_start[rowbase + hi_k[k] + off_k[k] + 1] - st;
         }
         t.start[slot] = st;
-        t.sx[slot] = shx_k[k];
-        t.sy[slot] = shy;
-        t.sz[slot] = shz;
+        t.shift[slot] = pack_shift(shx_k[k], shy, shz);
         cnt[k] = c;
       }
     }
@@ -259,7 +257,7 @@ __device__ __forceinline__ void grid_warp_tile(
   C* acc = reinterpret_cast<C*>(wsmem);
   int* tb = reinterpret_cast<int*>(wsmem + (size_t)PB * PS * sizeof(C));
   const int ts = tc.slots + 1;
-  SegTable t{tb, tb + ts, tb + 2 * ts, tb + 3 * ts, tb + 4 * ts};
+  SegTable t{tb, tb + ts, tb + 2 * ts};
   const T beta = (T)g.beta, c = (T)g.es_c, halfw = (T)W * (T)0.5;
   const int nf1 = g.nf1, nf2 = g.nf2, nw = g.nw;
   const size_t plane = (size_t)nf1 * nf2;
@@ -300,9 +298,10 @@ __device__ __forceinline__ void grid_warp_tile(
         const int sgi = find_segment(t.pref, nslots, q);
         const Rec<T> r = recs[t.start[sgi] + (q - t.pref[sgi])];
         cd.f0 = r.f[0]; cd.f1 = r.f[1]; cd.f2 = r.f[2]; cd.c0 = r.c[0]; cd.c1 = r.c[1];
-        cd.bx = (int)(r.bxy & 0xFFFFu) + t.sx[sgi];
-        cd.by = (int)(r.bxy >> 16) + t.sy[sgi];
-        cd.bz = (int)r.bz + t.sz[sgi];
+        const int sc = t.shift[sgi];
+        cd.bx = (int)(r.bxy & 0xFFFFu) + unpack_shift(sc, nf1);
+        cd.by = (int)(r.bxy >> 16) + unpack_shift(sc >> 2, nf2);
+        cd.bz = (int)r.bz + unpack_shift(sc >> 4, nw);
       }
       return cd;
     };
@@ -515,7 +514,7 @@ __device__ __forceinline__ void degrid_tile(const Rec<T>* __restrict__ recs,
   T* stg = (T*)smem;
   int* tb = (int*)(stg + 2 * (size_t)SXP * SY * SZ);
   const int ts = nslots_max + 1;
-  SegTable t{tb, tb + ts, tb + 2 * ts, tb + 3 * ts, tb + 4 * ts};
+  SegTable t{tb, tb + ts, tb + 2 * ts};
   const T beta = (T)g.beta, c = (T)g.es_c;
   const T* __restrict__ poly = geom_poly<T>(g);
   const size_t plane = (size_t)nf1 * nf2;
@@ -648,7 +647,7 @@ TileCfg grid_tiling(const Geom& g, bool degrid, const TileTune* tt) {
   auto bytes = [&](int tx, int ty, int pb) -> size_t {
     size_t cells = degrid ? (size_t)(tx + W + 1) * (ty + W) * (pb >= g.nw ? g.nw : pb + W)
                           : (size_t)(tx + 8) * ty * pb;
-    return cells * 2 * sizeof(T) + (size_t)(slots_for(ty, pb, W) + 1) * 4 * 5;
+    return cells * 2 * sizeof(T) + (size_t)(slots_for(ty, pb, W) + 1) * 4 * kSegInts;
   };
   if (PB <= 0) {
     PB = g.nw;
@@ -704,6 +703,10 @@ void set_tile_candidate(TileTune& tt, int dir, const int* c) {
   }
 }
 
+// dynamic shared memory of one warp-tiled gridding CTA at most (the SM
+// offers 227 KB to one CTA)
+constexpr size_t kWarpSmemMax = 226 * 1024;
+
 // Warp tiles: 16 x 16 cells by default (CG_WTILE_X / CG_WTILE_Y); the plane
 // batch and warps per CTA are chosen so that two CTAs fit on an SM.
 template <typename T>
@@ -729,10 +732,11 @@ WarpTile warp_tiling(const Geom& g, const TileTune* tt) {
   ps += ((W % 16) - (ps % 16) + 16) % 16;  // PS = W (mod 16)
   tc.PS = ps;
   tc.slots = ((tc.TY >> 3) + 2) * (PB + W) * 3;
-  tc.warp_bytes = ((size_t)PB * tc.PS * 2 * sizeof(T) + (size_t)(tc.slots + 1) * 5 * 4 + 15) & ~(size_t)15;
+  tc.warp_bytes =
+      ((size_t)PB * tc.PS * 2 * sizeof(T) + (size_t)(tc.slots + 1) * kSegInts * 4 + 15) & ~(size_t)15;
   if (warps <= 0) warps = (int)std::max<size_t>(1, std::min<size_t>(8, (110 * 1024) / tc.warp_bytes));
   warps = std::min(warps, 16);
-  while (warps > 1 && tc.warp_bytes * warps > 220 * 1024) warps--;
+  while (warps > 1 && tc.warp_bytes * warps > kWarpSmemMax) warps--;
   tc.warps = warps;
   tc.smem = tc.warp_bytes * warps;
   tc.ntx = (g.nf1 + tc.TX - 1) / tc.TX;
@@ -878,7 +882,7 @@ int multi_shape(GridJob<T>* jobs, int njobs, MultiShape* sh) {
   sh->grid_items = (int)gi;
   sh->degrid_items = (int)di;
   sh->warps = std::max(1, warps);
-  while (sh->warps > 1 && sh->warp_bytes * sh->warps > 220 * 1024) sh->warps--;
+  while (sh->warps > 1 && sh->warp_bytes * sh->warps > kWarpSmemMax) sh->warps--;
   return CG_OK;
 }
 

@@ -19,11 +19,20 @@ __device__ __forceinline__ int floordiv8(int a) { return a >= 0 ? a >> 3 : -((7 
 // are neighbours along x share one run) with the periodic shift of their cells.
 struct SegTable {
   int* start;
-  int* pref;  // exclusive prefix of the run lengths, pref[nslots] = total
-  int* sx;
-  int* sy;
-  int* sz;
+  int* pref;   // exclusive prefix of the run lengths, pref[nslots] = total
+  int* shift;  // periodic shift of the run's cells, 2 bits per axis (see pack_shift)
 };
+constexpr int kSegInts = 3;  // ints per slot of a segment table
+
+// shift of one axis (0, -n or +n) as a 2-bit code, three axes in one int
+__device__ __forceinline__ int shift_code(int s) { return s < 0 ? 1 : (s > 0 ? 2 : 0); }
+__device__ __forceinline__ int pack_shift(int sx, int sy, int sz) {
+  return shift_code(sx) | (shift_code(sy) << 2) | (shift_code(sz) << 4);
+}
+__device__ __forceinline__ int unpack_shift(int code, int n) {
+  const int c = code & 3;
+  return c == 1 ? -n : (c == 2 ? n : 0);
+}
 
 // Build the runs for hive rows hy in [hya, hyb], planes hz in [za, zb] (raw,
 // possibly outside the grid: wrapped with a shift of -+nf / -+nw) and hive
@@ -63,9 +72,7 @@ __device__ inline int build_segments(const Geom& g, const int* __restrict__ hive
           c = hive_start[h1 + 1] - st;
         }
         t.start[slot] = st;
-        t.sx[slot] = shx_k[k];
-        t.sy[slot] = shy;
-        t.sz[slot] = shz;
+        t.shift[slot] = pack_shift(shx_k[k], shy, shz);
         cnt[k] = c;
       }
     }
