@@ -10,6 +10,8 @@
 // Shared layout: row j of the column pair at float4 slot j + j / 16 (one pad
 // slot per 16 rows keeps the stride-16 stores of the first pass
 // conflict-free).
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -336,6 +338,311 @@ __global__ void __launch_bounds__(L / 16) k_col_fft_reg(float2* __restrict__ gri
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
+// Variant of k_col_fft_reg with one shared buffer of column pairs (float4):
+// each exchange moves both columns with 128-bit accesses (half the shared
+// memory instructions), and the buffer takes the next item's rows (cp.async)
+// once the last exchange of the current item has been read, overlapping that
+// load with the last pass and the stores.
+template <int L>
+__global__ void __launch_bounds__(L / 16) k_col_fft_reg2(float2* __restrict__ grid, int nf1,
+                                                         size_t plane, int nplanes, int c0a,
+                                                         int na, int c0b, int nb, int sign,
+                                                         const float2* __restrict__ tw) {
+  constexpr int T = L / 16;
+  constexpr int RL = last_radix(L);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* sv = reinterpret_cast<float4*>(smem_raw);  // pad16(L) + 16 slots
+  const int t = threadIdx.x;
+  const int groups_a = na / 2, groups = groups_a + nb / 2;
+  const int64_t items = (int64_t)groups * nplanes;
+  auto base_of = [&](int64_t it) {
+    const int p = (int)(it / groups), gi = (int)(it - (int64_t)p * groups);
+    const int col0 = gi < groups_a ? c0a + gi * 2 : c0b + (gi - groups_a) * 2;
+    return grid + (size_t)p * plane + col0;
+  };
+  auto prefetch = [&](int64_t it) {
+    const float2* b = base_of(it);
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const int row = t + m * T;
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(sv + pad16(row));
+      const float2* src = b + (size_t)row * nf1;
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  int64_t it = blockIdx.x;
+  if (it < items) prefetch(it);
+  for (; it < items; it += gridDim.x) {
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    float2 a[16], b[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const float4 v = sv[pad16(t + m * T)];
+      a[m] = make_float2(v.x, v.y);
+      b[m] = make_float2(v.z, v.w);
+    }
+    __syncthreads();
+    const bool more = it + gridDim.x < items;
+    bool fetched = false;
+    int Ns = 1, toff = 0;
+#pragma unroll 1
+    for (; Ns * 16 <= L; Ns *= 16) {
+      const int k = t & (Ns - 1);
+      if (Ns > 1) {
+#pragma unroll
+        for (int m = 1; m < 16; m++) {
+          const float2 tv = tw[toff + m * Ns + k];
+          const float2 w = make_float2(tv.x, sign * tv.y);
+          a[m] = cmul(a[m], w);
+          b[m] = cmul(b[m], w);
+        }
+      }
+      dft_reg<16>(a, sign);
+      dft_reg<16>(b, sign);
+      if (Ns * 16 == L) break;  // last pass: outputs at t + m T
+      const int o0 = (t - k) * 16 + k;
+#pragma unroll
+      for (int m = 0; m < 16; m++)
+        sv[pad16(o0 + m * Ns)] = make_float4(a[m].x, a[m].y, b[m].x, b[m].y);
+      __syncthreads();
+#pragma unroll
+      for (int m = 0; m < 16; m++) {
+        const float4 v = sv[pad16(t + m * T)];
+        a[m] = make_float2(v.x, v.y);
+        b[m] = make_float2(v.z, v.w);
+      }
+      __syncthreads();
+      if (Ns > 1) toff += 16 * Ns;
+      // after the last exchange the buffer is free: start the next item's rows
+      const bool last_exchange = RL > 1 ? (Ns * 16 * 16 > L) : (Ns * 16 * 16 == L);
+      if (last_exchange && more) {
+        prefetch(it + gridDim.x);
+        fetched = true;
+      }
+    }
+    if constexpr (RL > 1) {
+      constexpr int Q = 16 / RL;
+#pragma unroll
+      for (int q = 0; q < Q; q++) {
+        const int j = t + q * T;
+        float2 va[RL], vb[RL];
+#pragma unroll
+        for (int m = 0; m < RL; m++) {
+          va[m] = a[q + m * Q];
+          vb[m] = b[q + m * Q];
+          if (m > 0) {
+            const float2 tv = tw[toff + m * (L / RL) + j];
+            const float2 w = make_float2(tv.x, sign * tv.y);
+            va[m] = cmul(va[m], w);
+            vb[m] = cmul(vb[m], w);
+          }
+        }
+        dft_reg<RL>(va, sign);
+        dft_reg<RL>(vb, sign);
+#pragma unroll
+        for (int m = 0; m < RL; m++) {
+          a[q + m * Q] = va[m];
+          b[q + m * Q] = vb[m];
+        }
+      }
+    }
+    float2* bs = base_of(it);
+#pragma unroll
+    for (int m = 0; m < 16; m++)
+      *reinterpret_cast<float4*>(bs + (size_t)(t + m * T) * nf1) =
+          make_float4(a[m].x, a[m].y, b[m].x, b[m].y);
+    if (more && !fetched) {  // one pass only (no exchange): fetch after the stores
+      __syncthreads();
+      prefetch(it + gridDim.x);
+    }
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+template <int L>
+int launch_reg2(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, int c0b,
+                int nb, int sign, const float2* tw, cudaStream_t st) {
+  const size_t smem = (size_t)(pad16(L) + 16) * sizeof(float4);
+  int per_sm = 0;
+  CG_CUDA(kernel_occupancy((const void*)k_col_fft_reg2<L>, L / 16, smem, &per_sm));
+  if (per_sm < 1) return CG_ERR_ARG;
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
+  }
+  const int64_t items = (int64_t)(na / 2 + nb / 2) * nplanes;
+  const int blocks = (int)std::min<int64_t>(items, (int64_t)per_sm * sms);
+  k_col_fft_reg2<L><<<blocks, L / 16, smem, st>>>(grid, nf1, plane, nplanes, c0a, na, c0b, nb,
+                                                  sign, tw);
+  count_launches(1);
+  CG_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+// Cluster variant: four CTAs (a thread-block cluster) transform 8 adjacent
+// columns together.  Each CTA loads a quarter of the rows of all 8 columns
+// (64 contiguous bytes per grid row instead of 16) into its shared buffer;
+// after a cluster barrier every CTA gathers its own column pair, all rows,
+// from the four buffers through distributed shared memory, straight into
+// the register layout of k_col_fft_reg (thread t holds rows t + m T).  A
+// second cluster barrier frees the buffers, so the next item's loads overlap
+// this item's passes and stores.  Buffer layout: local row r, 16-byte chunk c
+// (column pair c) at slot c ^ ((r >> 1) & 3) of the row's 64 bytes, which
+// keeps both the loads and the gathers free of bank conflicts.
+constexpr int kColCluster = 4;
+
+template <int L>
+__global__ void __cluster_dims__(kColCluster, 1, 1) __launch_bounds__(L / 16)
+    k_col_fft_cluster(float2* __restrict__ grid, int nf1, size_t plane, int nplanes, int c0a,
+                      int na, int c0b, int nb, int sign, const float2* __restrict__ tw) {
+  namespace cgx = cooperative_groups;
+  constexpr int T = L / 16;
+  constexpr int RL = last_radix(L);
+  constexpr int RB = L / kColCluster;  // rows per CTA in the load buffer
+  cgx::cluster_group cluster = cgx::this_cluster();
+  const int rank = (int)cluster.block_rank();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* buf = reinterpret_cast<float4*>(smem_raw);                          // RB rows x 4 chunks
+  float2* xch = reinterpret_cast<float2*>(smem_raw + (size_t)RB * 4 * sizeof(float4));  // padded column
+  const int t = threadIdx.x;
+  const int groups_a = na / 8, groups = groups_a + nb / 8;
+  const int64_t items = (int64_t)groups * nplanes;
+  const int64_t nclusters = gridDim.x / kColCluster;
+  const int64_t cid = blockIdx.x / kColCluster;
+  auto base_of = [&](int64_t it) {  // column 0 of the item's 8 columns
+    const int p = (int)(it / groups), gi = (int)(it - (int64_t)p * groups);
+    const int col0 = gi < groups_a ? c0a + gi * 8 : c0b + (gi - groups_a) * 8;
+    return grid + (size_t)p * plane + col0;
+  };
+  // this CTA's quarter of the rows, 4 chunks of 16 bytes per row
+  auto load = [&](int64_t it) {
+    const float2* b = base_of(it) + (size_t)rank * RB * nf1;
+#pragma unroll
+    for (int k = 0; k < (RB * 4) / T; k++) {
+      const int idx = t + k * T;
+      const int r = idx >> 2, c = idx & 3;
+      const unsigned dst =
+          (unsigned)__cvta_generic_to_shared(buf + r * 4 + (c ^ ((r >> 1) & 3)));
+      const float2* src = b + (size_t)r * nf1 + 2 * c;
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  auto exchange = [&](float2 (&v)[16], int o0, int Ns) {
+#pragma unroll
+    for (int m = 0; m < 16; m++) xch[pad16(o0 + m * Ns)] = v[m];
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < 16; m++) v[m] = xch[pad16(t + m * T)];
+    __syncthreads();
+  };
+  int64_t it = cid;
+  if (it < items) load(it);
+  for (; it < items; it += nclusters) {
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    cluster.sync();  // every CTA's quarter is in place
+    float2 a[16], b[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const int row = t + m * T;
+      const int q = row / RB, r = row - q * RB;
+      const float4* src = cluster.map_shared_rank(buf, q) + r * 4 + (rank ^ ((r >> 1) & 3));
+      const float4 v = *src;
+      a[m] = make_float2(v.x, v.y);
+      b[m] = make_float2(v.z, v.w);
+    }
+    cluster.sync();  // every gather is done: the buffers take the next item
+    if (it + nclusters < items) load(it + nclusters);
+    int Ns = 1, toff = 0;
+#pragma unroll 1
+    for (; Ns * 16 <= L; Ns *= 16) {
+      const int k = t & (Ns - 1);
+      if (Ns > 1) {
+#pragma unroll
+        for (int m = 1; m < 16; m++) {
+          const float2 tv = tw[toff + m * Ns + k];
+          const float2 w = make_float2(tv.x, sign * tv.y);
+          a[m] = cmul(a[m], w);
+          b[m] = cmul(b[m], w);
+        }
+      }
+      dft_reg<16>(a, sign);
+      dft_reg<16>(b, sign);
+      if (Ns * 16 == L) break;
+      const int o0 = (t - k) * 16 + k;
+      exchange(a, o0, Ns);
+      exchange(b, o0, Ns);
+      if (Ns > 1) toff += 16 * Ns;
+    }
+    if constexpr (RL > 1) {
+      constexpr int Q = 16 / RL;
+#pragma unroll
+      for (int q = 0; q < Q; q++) {
+        const int j = t + q * T;
+        float2 va[RL], vb[RL];
+#pragma unroll
+        for (int m = 0; m < RL; m++) {
+          va[m] = a[q + m * Q];
+          vb[m] = b[q + m * Q];
+          if (m > 0) {
+            const float2 tv = tw[toff + m * (L / RL) + j];
+            const float2 w = make_float2(tv.x, sign * tv.y);
+            va[m] = cmul(va[m], w);
+            vb[m] = cmul(vb[m], w);
+          }
+        }
+        dft_reg<RL>(va, sign);
+        dft_reg<RL>(vb, sign);
+#pragma unroll
+        for (int m = 0; m < RL; m++) {
+          a[q + m * Q] = va[m];
+          b[q + m * Q] = vb[m];
+        }
+      }
+    }
+    float2* bs = base_of(it) + 2 * rank;
+#pragma unroll
+    for (int m = 0; m < 16; m++)
+      *reinterpret_cast<float4*>(bs + (size_t)(t + m * T) * nf1) =
+          make_float4(a[m].x, a[m].y, b[m].x, b[m].y);
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+  cluster.sync();  // no CTA leaves while another may still read its buffer
+}
+
+template <int L>
+int launch_cluster(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, int c0b,
+                   int nb, int sign, const float2* tw, cudaStream_t st) {
+  constexpr int RB = L / kColCluster;
+  const size_t smem = (size_t)RB * 4 * sizeof(float4) + (size_t)(pad16(L) + 16) * sizeof(float2);
+  int per_sm = 0;
+  CG_CUDA(kernel_occupancy((const void*)k_col_fft_cluster<L>, L / 16, smem, &per_sm));
+  if (per_sm < 1) return CG_ERR_ARG;
+  static int max_clusters[4] = {0, 0, 0, 0};
+  const int slot = L == 1024 ? 0 : L == 2048 ? 1 : L == 4096 ? 2 : 3;
+  if (!max_clusters[slot]) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kColCluster * 148, 1, 1);
+    cfg.blockDim = dim3(L / 16, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    int n = 0;
+    CG_CUDA(cudaOccupancyMaxActiveClusters(&n, (const void*)k_col_fft_cluster<L>, &cfg));
+    if (n < 1) return CG_ERR_ARG;
+    max_clusters[slot] = n;
+  }
+  const int64_t items = (int64_t)(na / 8 + nb / 8) * nplanes;
+  const int clusters = (int)std::min<int64_t>(items, max_clusters[slot]);
+  k_col_fft_cluster<L><<<clusters * kColCluster, L / 16, smem, st>>>(grid, nf1, plane, nplanes,
+                                                                     c0a, na, c0b, nb, sign, tw);
+  count_launches(1);
+  CG_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
 template <int L>
 int launch_reg(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, int c0b, int nb,
                int sign, const float2* tw, cudaStream_t st) {
@@ -394,8 +701,11 @@ int launch_l(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, 
              int sign, const float2* tw, cudaStream_t st) {
   // CG_COL_FFT_REG=0: the shared-memory-resident kernel instead of the register-resident one
   const char* e = getenv("CG_COL_FFT_REG");
-  if (!(e && atoi(e) == 0))
-    return launch_reg<L>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st);
+  const int reg = e ? atoi(e) : 1;
+  if (reg == 3 && na % 8 == 0 && nb % 8 == 0)
+    return launch_cluster<L>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st);
+  if (reg == 2) return launch_reg2<L>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st);
+  if (reg != 0) return launch_reg<L>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st);
   return col_fft_cb(L) == 1
              ? launch_lc<L, 1>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st)
              : launch_lc<L, 2>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st);
