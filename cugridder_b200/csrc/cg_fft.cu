@@ -228,11 +228,17 @@ __global__ void __launch_bounds__(kFftThreads, CB == 1 ? 2 : 1) k_col_fft(float2
 // buffer receives the next item by cp.async while the current one is
 // transformed, so loads, passes and stores of consecutive items overlap in
 // one CTA.
+//
+// Rows [mid0, mid1) of every column are outside the image (the CMCL map
+// reaches rows [0, mid0) and [mid1, L) only): with skip = 1 they are zero on
+// input (the plane fill wrote zeros there) and are not loaded; with skip = 2
+// nothing reads them afterwards (the w-DFT) and they are not stored.
 template <int L>
 __global__ void __launch_bounds__(L / 16) k_col_fft_reg(float2* __restrict__ grid, int nf1,
                                                         size_t plane, int nplanes, int c0a,
                                                         int na, int c0b, int nb, int sign,
-                                                        const float2* __restrict__ tw) {
+                                                        const float2* __restrict__ tw, int mid0,
+                                                        int mid1, int skip) {
   constexpr int T = L / 16;
   constexpr int RL = last_radix(L);  // 1: L is a power of 16
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -246,11 +252,13 @@ __global__ void __launch_bounds__(L / 16) k_col_fft_reg(float2* __restrict__ gri
     const int col0 = gi < groups_a ? c0a + gi * 2 : c0b + (gi - groups_a) * 2;
     return grid + (size_t)p * plane + col0;
   };
+  auto outside = [&](int row) { return row >= mid0 && row < mid1; };
   auto prefetch = [&](int64_t it) {
     const float2* b = base_of(it);
 #pragma unroll
     for (int m = 0; m < 16; m++) {
       const int row = t + m * T;
+      if (skip == 1 && outside(row)) continue;  // zero rows: not loaded
       const unsigned dst = (unsigned)__cvta_generic_to_shared(pre + row);
       const float2* src = b + (size_t)row * nf1;
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
@@ -274,7 +282,8 @@ __global__ void __launch_bounds__(L / 16) k_col_fft_reg(float2* __restrict__ gri
     float2 a[16], b[16];
 #pragma unroll
     for (int m = 0; m < 16; m++) {
-      const float4 v = pre[t + m * T];
+      const int row = t + m * T;
+      const float4 v = (skip == 1 && outside(row)) ? make_float4(0.f, 0.f, 0.f, 0.f) : pre[row];
       a[m] = make_float2(v.x, v.y);
       b[m] = make_float2(v.z, v.w);
     }
@@ -331,9 +340,12 @@ __global__ void __launch_bounds__(L / 16) k_col_fft_reg(float2* __restrict__ gri
     }
     float2* bs = base_of(it);
 #pragma unroll
-    for (int m = 0; m < 16; m++)
-      *reinterpret_cast<float4*>(bs + (size_t)(t + m * T) * nf1) =
+    for (int m = 0; m < 16; m++) {
+      const int row = t + m * T;
+      if (skip == 2 && outside(row)) continue;  // rows nothing reads
+      *reinterpret_cast<float4*>(bs + (size_t)row * nf1) =
           make_float4(a[m].x, a[m].y, b[m].x, b[m].y);
+    }
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
@@ -645,7 +657,7 @@ int launch_cluster(float2* grid, int nf1, size_t plane, int nplanes, int c0a, in
 
 template <int L>
 int launch_reg(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, int c0b, int nb,
-               int sign, const float2* tw, cudaStream_t st) {
+               int sign, const float2* tw, cudaStream_t st, int mid0, int mid1, int skip) {
   const size_t smem = (size_t)L * sizeof(float4) + (size_t)(pad16(L) + 16) * sizeof(float2);
   int per_sm = 0;
   CG_CUDA(kernel_occupancy((const void*)k_col_fft_reg<L>, L / 16, smem, &per_sm));
@@ -659,7 +671,7 @@ int launch_reg(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na
   const int64_t items = (int64_t)(na / 2 + nb / 2) * nplanes;
   const int blocks = (int)std::min<int64_t>(items, (int64_t)per_sm * sms);
   k_col_fft_reg<L><<<blocks, L / 16, smem, st>>>(grid, nf1, plane, nplanes, c0a, na, c0b, nb,
-                                                 sign, tw);
+                                                 sign, tw, mid0, mid1, skip);
   count_launches(1);
   CG_CUDA(cudaGetLastError());
   return CG_OK;
@@ -698,14 +710,16 @@ int launch_lc(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na,
 
 template <int L>
 int launch_l(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, int c0b, int nb,
-             int sign, const float2* tw, cudaStream_t st) {
+             int sign, const float2* tw, cudaStream_t st, int mid0, int mid1, int skip) {
   // CG_COL_FFT_REG=0: the shared-memory-resident kernel instead of the register-resident one
   const char* e = getenv("CG_COL_FFT_REG");
   const int reg = e ? atoi(e) : 1;
   if (reg == 3 && na % 8 == 0 && nb % 8 == 0)
     return launch_cluster<L>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st);
   if (reg == 2) return launch_reg2<L>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st);
-  if (reg != 0) return launch_reg<L>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st);
+  if (reg != 0)
+    return launch_reg<L>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st, mid0, mid1,
+                         skip);
   return col_fft_cb(L) == 1
              ? launch_lc<L, 1>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st)
              : launch_lc<L, 2>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st);
@@ -750,14 +764,19 @@ int make_col_fft_twiddles(int L, float2* d_tw, cudaStream_t st) {
 // In-place column transforms of columns [c0a, c0a + na) and [c0b, c0b + nb)
 // of nplanes planes (row stride nf1, plane stride `plane` elements), length L.
 int launch_col_fft(float2* grid, int L, int nf1, size_t plane, int nplanes, int c0a, int na,
-                   int c0b, int nb, int sign, const float2* d_tw, cudaStream_t st) {
+                   int c0b, int nb, int sign, const float2* d_tw, cudaStream_t st, int mid0,
+                   int mid1, int skip) {
+  if (skip != 0 && !(0 <= mid0 && mid0 <= mid1 && mid1 <= L)) skip = 0;
+#define CG_COL_CALL(l) \
+  launch_l<l>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, d_tw, st, mid0, mid1, skip)
   switch (L) {
-    case 1024: return launch_l<1024>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, d_tw, st);
-    case 2048: return launch_l<2048>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, d_tw, st);
-    case 4096: return launch_l<4096>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, d_tw, st);
-    case 8192: return launch_l<8192>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, d_tw, st);
+    case 1024: return CG_COL_CALL(1024);
+    case 2048: return CG_COL_CALL(2048);
+    case 4096: return CG_COL_CALL(4096);
+    case 8192: return CG_COL_CALL(8192);
     default: return CG_ERR_ARG;
   }
+#undef CG_COL_CALL
 }
 
 }  // namespace cg

@@ -106,8 +106,11 @@ int launch_degrid_tma(const Rec<float>* d_recs, const int* d_perm, const int* d_
 bool col_fft_supported(int L, int na, int nb);
 size_t col_fft_twiddle_count(int L);
 int make_col_fft_twiddles(int L, float2* d_tw, cudaStream_t st);
+// Rows [mid0, mid1) of the columns: skip 1 = zero on input (not loaded),
+// 2 = unused on output (not stored), 0 = transformed like the others.
 int launch_col_fft(float2* grid, int L, int nf1, size_t plane, int nplanes, int c0a, int na,
-                   int c0b, int nb, int sign, const float2* d_tw, cudaStream_t st);
+                   int c0b, int nb, int sign, const float2* d_tw, cudaStream_t st, int mid0 = 0,
+                   int mid1 = 0, int skip = 0);
 
 // ---- memory-limited mode: plane windows [p0, p1) (cg_spread.cu, cg_wstage.cu) ----
 template <typename T>

@@ -576,10 +576,14 @@ static int fft_exec_pruned(cg_plan_s* P, void* d_grid, int direction) {
       CG_TRY(make_col_fft_twiddles(g.nf2, (float2*)P->coltw.p, P->stream));
       P->coltw_n = g.nf2;
     }
+    // image rows of a column under the CMCL map: [0, N2 - N2/2) and [nf2 - N2/2, nf2);
+    // the rows between are zero before the forward transform (plane fill)
+    // and unread after the inverse one (w-DFT)
+    const int mid0 = g.N2 - g.N2 / 2, mid1 = g.nf2 - g.N2 / 2;
     auto all_cols = [&]() {
       return launch_col_fft((float2*)d_grid, g.nf2, g.nf1, plane, g.nw, 0, half, g.nf1 - half, half,
                             direction == CUFFT_INVERSE ? 1 : -1, (const float2*)P->coltw.p,
-                            P->stream);
+                            P->stream, mid0, mid1, direction == CUFFT_INVERSE ? 2 : 1);
     };
     if (direction == CUFFT_INVERSE) {
       for (int p = 0; p < g.nw; p++) CG_TRY(rows(p));
