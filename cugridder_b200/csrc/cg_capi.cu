@@ -366,6 +366,7 @@ int cg_plan_create(cg_plan** plan, int nxdirty, int nydirty, double fov, double 
   }
   if (const char* m = getenv("CG_FFT_PRUNE")) P->fft_pruning = atoi(m) != 0;
   if (const char* m = getenv("CG_COL_FFT")) P->col_fft = atoi(m) != 0;
+  if (const char* m = getenv("CG_ROW_FFT")) P->row_fft = atoi(m) != 0;
   if (const char* m = getenv("CG_AUTOTUNE")) P->autotune = atoi(m) != 0;
   if (const char* m = getenv("CG_DEGRID_TMA")) P->tma_default = atoi(m);
   st = cg::plan_configure(P, nxdirty, nydirty, fov, epsilon, sigma, sign, precision);

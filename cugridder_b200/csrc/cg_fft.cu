@@ -218,6 +218,76 @@ __global__ void __launch_bounds__(kFftThreads, CB == 1 ? 2 : 1) k_col_fft(float2
   }
 }
 
+// All passes of a length-L transform of two vectors held in registers:
+// thread t holds elements t + m T (m < 16, T = L / 16) of each in a[], b[]
+// and gets the outputs back at the same positions.  Radix-16 Stockham passes
+// exchange through xch (one vector at a time, padded), then a last radix-RL
+// pass runs in registers.
+template <int L>
+__device__ __forceinline__ void fft_regs(float2 (&a)[16], float2 (&b)[16], int sign,
+                                         const float2* __restrict__ tw, float2* xch) {
+  constexpr int T = L / 16;
+  constexpr int RL = last_radix(L);  // 1: L is a power of 16
+  const int t = threadIdx.x;
+  auto exchange = [&](float2 (&v)[16], int o0, int Ns) {
+#pragma unroll
+    for (int m = 0; m < 16; m++) xch[pad16(o0 + m * Ns)] = v[m];
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < 16; m++) v[m] = xch[pad16(t + m * T)];
+    __syncthreads();
+  };
+  int Ns = 1, toff = 0;
+#pragma unroll 1
+  for (; Ns * 16 <= L; Ns *= 16) {
+    const int k = t & (Ns - 1);
+    if (Ns > 1) {
+#pragma unroll
+      for (int m = 1; m < 16; m++) {
+        const float2 tv = tw[toff + m * Ns + k];
+        const float2 w = make_float2(tv.x, sign * tv.y);
+        a[m] = cmul(a[m], w);
+        b[m] = cmul(b[m], w);
+      }
+    }
+    dft_reg<16>(a, sign);
+    dft_reg<16>(b, sign);
+    if (Ns * 16 == L) return;  // last pass (L a power of 16): outputs at t + m T
+    const int o0 = (t - k) * 16 + k;
+    exchange(a, o0, Ns);
+    exchange(b, o0, Ns);
+    if (Ns > 1) toff += 16 * Ns;
+  }
+  if constexpr (RL > 1) {
+    // last pass, radix RL, Ns = L / RL: butterfly j = t + q T reads and
+    // writes positions j + m L / RL, i.e. slots q + m (16 / RL) of this thread
+    constexpr int Q = 16 / RL;
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+      const int j = t + q * T;
+      float2 va[RL], vb[RL];
+#pragma unroll
+      for (int m = 0; m < RL; m++) {
+        va[m] = a[q + m * Q];
+        vb[m] = b[q + m * Q];
+        if (m > 0) {
+          const float2 tv = tw[toff + m * (L / RL) + j];
+          const float2 w = make_float2(tv.x, sign * tv.y);
+          va[m] = cmul(va[m], w);
+          vb[m] = cmul(vb[m], w);
+        }
+      }
+      dft_reg<RL>(va, sign);
+      dft_reg<RL>(vb, sign);
+#pragma unroll
+      for (int m = 0; m < RL; m++) {
+        a[q + m * Q] = va[m];
+        b[q + m * Q] = vb[m];
+      }
+    }
+  }
+}
+
 // Register-resident variant: T = L / 16 threads, each holding 16 points of
 // both columns of the pair in registers for every pass.  Thread t always
 // holds positions t + m T (m < 16): they are the inputs of every radix-16
@@ -240,7 +310,6 @@ __global__ void __launch_bounds__(L / 16) k_col_fft_reg(float2* __restrict__ gri
                                                         const float2* __restrict__ tw, int mid0,
                                                         int mid1, int skip) {
   constexpr int T = L / 16;
-  constexpr int RL = last_radix(L);  // 1: L is a power of 16
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* pre = reinterpret_cast<float4*>(smem_raw);                       // L rows x 2 columns
   float2* xch = reinterpret_cast<float2*>(smem_raw + (size_t)L * sizeof(float4));  // padded column
@@ -265,15 +334,6 @@ __global__ void __launch_bounds__(L / 16) k_col_fft_reg(float2* __restrict__ gri
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
-  // Stockham exchange of one column: outputs at o0 + m Ns, inputs back at t + m T
-  auto exchange = [&](float2 (&v)[16], int o0, int Ns) {
-#pragma unroll
-    for (int m = 0; m < 16; m++) xch[pad16(o0 + m * Ns)] = v[m];
-    __syncthreads();
-#pragma unroll
-    for (int m = 0; m < 16; m++) v[m] = xch[pad16(t + m * T)];
-    __syncthreads();
-  };
   int64_t it = blockIdx.x;
   if (it < items) prefetch(it);
   for (; it < items; it += gridDim.x) {
@@ -289,55 +349,7 @@ __global__ void __launch_bounds__(L / 16) k_col_fft_reg(float2* __restrict__ gri
     }
     __syncthreads();  // the prefetch buffer is free again
     if (it + gridDim.x < items) prefetch(it + gridDim.x);
-    int Ns = 1, toff = 0;
-#pragma unroll 1
-    for (; Ns * 16 <= L; Ns *= 16) {
-      const int k = t & (Ns - 1);
-      if (Ns > 1) {
-#pragma unroll
-        for (int m = 1; m < 16; m++) {
-          const float2 tv = tw[toff + m * Ns + k];
-          const float2 w = make_float2(tv.x, sign * tv.y);
-          a[m] = cmul(a[m], w);
-          b[m] = cmul(b[m], w);
-        }
-      }
-      dft_reg<16>(a, sign);
-      dft_reg<16>(b, sign);
-      if (Ns * 16 == L) break;  // last pass (L a power of 16): outputs at t + m T
-      const int o0 = (t - k) * 16 + k;
-      exchange(a, o0, Ns);
-      exchange(b, o0, Ns);
-      if (Ns > 1) toff += 16 * Ns;
-    }
-    if constexpr (RL > 1) {
-      // last pass, radix RL, Ns = L / RL: butterfly j = t + q T reads and
-      // writes positions j + m L / RL, i.e. slots q + m (16 / RL) of this thread
-      constexpr int Q = 16 / RL;
-#pragma unroll
-      for (int q = 0; q < Q; q++) {
-        const int j = t + q * T;
-        float2 va[RL], vb[RL];
-#pragma unroll
-        for (int m = 0; m < RL; m++) {
-          va[m] = a[q + m * Q];
-          vb[m] = b[q + m * Q];
-          if (m > 0) {
-            const float2 tv = tw[toff + m * (L / RL) + j];
-            const float2 w = make_float2(tv.x, sign * tv.y);
-            va[m] = cmul(va[m], w);
-            vb[m] = cmul(vb[m], w);
-          }
-        }
-        dft_reg<RL>(va, sign);
-        dft_reg<RL>(vb, sign);
-#pragma unroll
-        for (int m = 0; m < RL; m++) {
-          a[q + m * Q] = va[m];
-          b[q + m * Q] = vb[m];
-        }
-      }
-    }
+    fft_regs<L>(a, b, sign, tw, xch);
     float2* bs = base_of(it);
 #pragma unroll
     for (int m = 0; m < 16; m++) {
@@ -655,6 +667,93 @@ int launch_cluster(float2* grid, int nf1, size_t plane, int nplanes, int c0a, in
   return CG_OK;
 }
 
+// Row transforms of a band of grid rows, [r0, r0 + nrows) of every plane
+// (row stride L = nf1), two rows per item, in the register layout of
+// k_col_fft_reg: thread t holds elements t + m T of both rows, loaded by
+// cp.async one item ahead and stored straight from registers.  Elements
+// [mid0, mid1) (the columns outside the image) are skipped as there: with
+// skip = 1 they are zero on input and not loaded, with skip = 2 nothing
+// reads them afterwards and they are not stored.
+template <int L>
+__global__ void __launch_bounds__(L / 16) k_row_fft_reg(float2* __restrict__ grid, size_t plane,
+                                                        int nplanes, int r0, int nrows, int sign,
+                                                        const float2* __restrict__ tw, int mid0,
+                                                        int mid1, int skip) {
+  constexpr int T = L / 16;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* pre = reinterpret_cast<float4*>(smem_raw);  // element j: (row 0, row 1)
+  float2* xch = reinterpret_cast<float2*>(smem_raw + (size_t)L * sizeof(float4));
+  const int t = threadIdx.x;
+  const int pairs = nrows / 2;
+  const int64_t items = (int64_t)pairs * nplanes;
+  auto base_of = [&](int64_t it) {
+    const int p = (int)(it / pairs), rp = (int)(it - (int64_t)p * pairs);
+    return grid + (size_t)p * plane + (size_t)(r0 + 2 * rp) * L;
+  };
+  auto outside = [&](int j) { return j >= mid0 && j < mid1; };
+  auto prefetch = [&](int64_t it) {
+    const float2* b = base_of(it);
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const int j = t + m * T;
+      if (skip == 1 && outside(j)) continue;  // zero columns: not loaded
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(pre + j);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(b + j) : "memory");
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst + 8), "l"(b + L + j)
+                   : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  int64_t it = blockIdx.x;
+  if (it < items) prefetch(it);
+  for (; it < items; it += gridDim.x) {
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    float2 a[16], b[16];
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const int j = t + m * T;
+      const float4 v = (skip == 1 && outside(j)) ? make_float4(0.f, 0.f, 0.f, 0.f) : pre[j];
+      a[m] = make_float2(v.x, v.y);
+      b[m] = make_float2(v.z, v.w);
+    }
+    __syncthreads();  // the prefetch buffer is free again
+    if (it + gridDim.x < items) prefetch(it + gridDim.x);
+    fft_regs<L>(a, b, sign, tw, xch);
+    float2* bs = base_of(it);
+#pragma unroll
+    for (int m = 0; m < 16; m++) {
+      const int j = t + m * T;
+      if (skip == 2 && outside(j)) continue;  // columns nothing reads
+      bs[j] = a[m];
+      bs[L + j] = b[m];
+    }
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+template <int L>
+int launch_row(float2* grid, size_t plane, int nplanes, int r0, int nrows, int sign,
+               const float2* tw, cudaStream_t st, int mid0, int mid1, int skip) {
+  const size_t smem = (size_t)L * sizeof(float4) + (size_t)(pad16(L) + 16) * sizeof(float2);
+  int per_sm = 0;
+  CG_CUDA(kernel_occupancy((const void*)k_row_fft_reg<L>, L / 16, smem, &per_sm));
+  if (per_sm < 1) return CG_ERR_ARG;
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
+  }
+  const int64_t items = (int64_t)(nrows / 2) * nplanes;
+  const int blocks = (int)std::min<int64_t>(items, (int64_t)per_sm * sms);
+  k_row_fft_reg<L><<<blocks, L / 16, smem, st>>>(grid, plane, nplanes, r0, nrows, sign, tw, mid0,
+                                                 mid1, skip);
+  count_launches(1);
+  CG_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
 template <int L>
 int launch_reg(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, int c0b, int nb,
                int sign, const float2* tw, cudaStream_t st, int mid0, int mid1, int skip) {
@@ -726,6 +825,21 @@ int launch_l(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, 
 }
 
 }  // namespace
+
+int launch_row_fft(float2* grid, int L, size_t plane, int nplanes, int r0, int nrows, int sign,
+                   const float2* d_tw, cudaStream_t st, int mid0, int mid1, int skip) {
+  if (nrows < 2 || nrows % 2) return CG_ERR_ARG;
+  if (skip != 0 && !(0 <= mid0 && mid0 <= mid1 && mid1 <= L)) skip = 0;
+#define CG_ROW_CALL(l) launch_row<l>(grid, plane, nplanes, r0, nrows, sign, d_tw, st, mid0, mid1, skip)
+  switch (L) {
+    case 1024: return CG_ROW_CALL(1024);
+    case 2048: return CG_ROW_CALL(2048);
+    case 4096: return CG_ROW_CALL(4096);
+    case 8192: return CG_ROW_CALL(8192);
+    default: return CG_ERR_ARG;
+  }
+#undef CG_ROW_CALL
+}
 
 bool col_fft_supported(int L, int na, int nb) {
   return (L == 1024 || L == 2048 || L == 4096 || L == 8192) && na % 2 == 0 && nb % 2 == 0;

@@ -106,6 +106,11 @@ int launch_degrid_tma(const Rec<float>* d_recs, const int* d_perm, const int* d_
 bool col_fft_supported(int L, int na, int nb);
 size_t col_fft_twiddle_count(int L);
 int make_col_fft_twiddles(int L, float2* d_tw, cudaStream_t st);
+// Row transforms (FP32, power-of-two L = nf1, the columns' twiddle table
+// when nf1 = nf2) of rows [r0, r0 + nrows) (nrows even) of nplanes planes;
+// elements [mid0, mid1) skipped as for launch_col_fft.
+int launch_row_fft(float2* grid, int L, size_t plane, int nplanes, int r0, int nrows, int sign,
+                   const float2* d_tw, cudaStream_t st, int mid0 = 0, int mid1 = 0, int skip = 0);
 // Rows [mid0, mid1) of the columns: skip 1 = zero on input (not loaded),
 // 2 = unused on output (not stored), 0 = transformed like the others.
 int launch_col_fft(float2* grid, int L, int nf1, size_t plane, int nplanes, int c0a, int na,

@@ -585,12 +585,25 @@ static int fft_exec_pruned(cg_plan_s* P, void* d_grid, int direction) {
                             direction == CUFFT_INVERSE ? 1 : -1, (const float2*)P->coltw.p,
                             P->stream, mid0, mid1, direction == CUFFT_INVERSE ? 2 : 1);
     };
-    if (direction == CUFFT_INVERSE) {
+    // rows by cuFFT, or (CG_ROW_FFT=1, slower on B200) by the register-resident
+    // row kernel on square grids (the same twiddles), which skips the columns
+    // outside the image, [N1 - N1/2, nf1 - N1/2): zero before the forward row
+    // pass and unread after the inverse one
+    const bool row_kernel = g.nf1 == g.nf2 && half == g.N1 - g.N1 / 2 && P->row_fft;
+    auto all_rows = [&]() -> int {
+      if (row_kernel)
+        return launch_row_fft((float2*)d_grid, g.nf1, plane, g.nw, r0, batch,
+                              direction == CUFFT_INVERSE ? 1 : -1, (const float2*)P->coltw.p,
+                              P->stream, half, g.nf1 - half, direction == CUFFT_INVERSE ? 2 : 1);
       for (int p = 0; p < g.nw; p++) CG_TRY(rows(p));
+      return CG_OK;
+    };
+    if (direction == CUFFT_INVERSE) {
+      CG_TRY(all_rows());
       CG_TRY(all_cols());
     } else {
       CG_TRY(all_cols());
-      for (int p = 0; p < g.nw; p++) CG_TRY(rows(p));
+      CG_TRY(all_rows());
     }
     return CG_OK;
   }

@@ -75,6 +75,7 @@ struct cg_plan_s {
   int rows_n = 0, rows_batch = 0, cols_n = 0, cols_stride = 0, cols_batch = 0;
   int fft_pruning = 1;  // 0: always the full 2-D transform (CG_FFT_PRUNE=0)
   int col_fft = 1;      // 0: cuFFT for the column transforms too (CG_COL_FFT=0)
+  int row_fft = 0;      // 1: register-resident row kernel instead of cuFFT rows (CG_ROW_FFT=1; slower on B200)
   int coltw_n = 0;      // length of the twiddle table in coltw
   // memory-limited mode (cg_plan_set_grid_budget): the grid holds plane_batch
   // planes at a time when the whole grid exceeds grid_budget bytes

@@ -46,7 +46,8 @@ def _run(torch, d, img, col_fft):
     return dirty.cpu().numpy(), vis.cpu().numpy(), info
 
 
-VARIANTS = {"registers": {}, "registers_pair_exchange": {"CG_COL_FFT_REG": "2"},
+VARIANTS = {"registers": {}, "registers_row_kernel": {"CG_ROW_FFT": "1"},
+            "registers_pair_exchange": {"CG_COL_FFT_REG": "2"},
             "cluster": {"CG_COL_FFT_REG": "3"},
             "shared_pair": {"CG_COL_FFT_REG": "0"},
             "shared_single": {"CG_COL_FFT_REG": "0", "CG_COL_FFT_CB": "1"}}
@@ -55,10 +56,10 @@ VARIANTS = {"registers": {}, "registers_pair_exchange": {"CG_COL_FFT_REG": "2"},
 @pytest.mark.parametrize("variant", sorted(VARIANTS))
 @pytest.mark.parametrize("N", [512, 1024, 2048, 4096])
 def test_column_fft_matches_cufft(torch_cuda, N, variant):
-    """Every column kernel: register-resident (default, with column-pair
-    exchanges, or as a four-CTA cluster gathering through distributed shared
-    memory), shared-memory resident with two adjacent columns or one column
-    per CTA."""
+    """Every column kernel: register-resident (default, with the row pass by
+    cuFFT or by the register-resident row kernel, with column-pair exchanges,
+    or as a four-CTA cluster gathering through distributed shared memory),
+    shared-memory resident with two adjacent columns or one column per CTA."""
     d = _narrow_band_case(N, 100_000, seed=N)
     img = synth.random_image(N, N, seed=2)
     env = VARIANTS[variant]
