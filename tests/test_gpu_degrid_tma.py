@@ -64,3 +64,13 @@ def test_tma_degridding_learned_kernel(torch_cuda, variant):
     b, _ = _dirty2ms(torch_cuda, d, img, 1e-5, 0, kernel=k)
     for x in a:
         assert rel_l2(x, b[0]) < 1e-6
+
+
+@pytest.mark.parametrize("nx,ny", [(512, 1024), (1024, 512)])
+def test_tma_degridding_non_square(torch_cuda, nx, ny):
+    d = synth.make("wstack_2048_10M", seed=nx + ny, nrow=200_000, nx=nx, ny=ny, fov=1.0)
+    img = synth.random_image(nx, ny, seed=11, dtype=np.complex64)
+    a, _ = _dirty2ms(torch_cuda, d, img, 1e-5, 2)
+    b, _ = _dirty2ms(torch_cuda, d, img, 1e-5, 0)
+    for x in a:
+        assert rel_l2(x, b[0]) < 1e-6

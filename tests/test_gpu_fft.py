@@ -73,3 +73,17 @@ def test_column_fft_matches_cufft(torch_cuda, N, variant):
     assert a[2]["nf2"] == 2 * N
     assert rel_l2(a[0], b[0]) < 2e-6
     assert rel_l2(a[1], b[1]) < 2e-6
+
+
+@pytest.mark.parametrize("nx,ny", [(512, 1024), (1024, 512)])
+def test_column_fft_non_square(torch_cuda, nx, ny):
+    """Non-square images: the column length (nf2, from nx) and the image rows
+    it skips, [nx - nx/2, nf2 - nx/2), differ from the row length (nf1)."""
+    d = _narrow_band_case(max(nx, ny), 100_000, seed=nx + 3 * ny)
+    d["nx"], d["ny"] = nx, ny
+    img = synth.random_image(nx, ny, seed=5)
+    a = _run(torch_cuda, d, img, True)
+    b = _run(torch_cuda, d, img, False)
+    assert a[2]["nf2"] == 2 * nx and a[2]["nf1"] == 2 * ny
+    assert rel_l2(a[0], b[0]) < 2e-6
+    assert rel_l2(a[1], b[1]) < 2e-6
