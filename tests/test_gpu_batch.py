@@ -120,3 +120,43 @@ def test_batch_matches_plans_through_graph_replays(torch_cuda):
     assert degrid_t[3] in (256, 512), degrid_t
     assert ms[0] > 0 and ms[1] > 0, ms
     b.close()
+
+
+def test_batch_fp64_matches_plans(torch_cuda):
+    """FP64 batch (the double instantiations of the one-launch kernels)
+    against one FP64 plan per dataset."""
+    torch = torch_cuda
+    ds = []
+    for i, (n, fov, nrow, nchan) in enumerate(SPECS[:4]):
+        d = synth.make("ms2dirty_256_fp64", seed=400 + i, nrow=nrow, nx=n, ny=n, fov=fov)
+        freqs = np.linspace(1.0e8, 2.0e8, nchan) if nchan > 1 else np.array([1.0e8])
+        rng = np.random.Generator(np.random.PCG64(500 + i))
+        vis = rng.standard_normal((nrow, nchan)) + 1j * rng.standard_normal((nrow, nchan))
+        wgt = rng.uniform(0.5, 1.5, (nrow, nchan))
+        ds.append(dict(uvw=to_dev(torch, d["uvw"]), freqs=freqs, vis=to_dev(torch, vis),
+                       wgt=to_dev(torch, wgt), fov=fov,
+                       dirty=torch.zeros((n, n), dtype=torch.complex128, device="cuda")))
+    b = Batch(ds, epsilon=1e-9, precision="fp64")
+    for call in range(3):
+        b.ms2dirty()
+        torch.cuda.synchronize()
+        for d in ds:
+            n = d["dirty"].shape[0]
+            p = Plan(n, n, d["fov"], 1e-9, precision="fp64")
+            out = torch.zeros_like(d["dirty"])
+            p.ms2dirty_chan(d["uvw"], d["freqs"], d["vis"], d["wgt"], out)
+            torch.cuda.synchronize()
+            p.close()
+            assert rel_l2(d["dirty"].cpu().numpy(), out.cpu().numpy()) < 1e-12, call
+    for call in range(2):
+        b.dirty2ms()
+        torch.cuda.synchronize()
+        for d in ds:
+            n = d["dirty"].shape[0]
+            p = Plan(n, n, d["fov"], 1e-9, precision="fp64")
+            out = torch.zeros_like(d["vis"])
+            p.dirty2ms_chan(d["uvw"], d["freqs"], d["dirty"], d["wgt"], out)
+            torch.cuda.synchronize()
+            p.close()
+            assert rel_l2(d["vis"].cpu().numpy(), out.cpu().numpy()) < 1e-12, call
+    b.close()
