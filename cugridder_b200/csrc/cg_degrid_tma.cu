@@ -337,9 +337,12 @@ int launch_w(const Rec<float>* d_recs, const int* d_perm, const int* d_hive_star
   int per_sm = 0;
   CG_CUDA(kernel_occupancy((const void*)k_degrid_tma<W, NT, NS>, NT, smem, &per_sm));
   if (per_sm < 1) return CG_ERR_ARG;
-  int sms = 0, dev = 0;
-  cudaGetDevice(&dev);
-  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
+  static int sms = 0;
+  if (!sms) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
+  }
   const int blocks = std::min(tc.nitems, per_sm * sms);
   CG_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(int), st));
   k_degrid_tma<W, NT, NS><<<blocks, NT, smem, st>>>(map, d_recs, d_perm, d_hive_start, M, g, tc,
