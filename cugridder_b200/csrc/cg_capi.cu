@@ -120,7 +120,7 @@ void destroy_plan(cg_plan_s* P) {
   cg_dev_buf* bs[] = {&P->mm,   &P->K1,    &P->K2,     &P->K3q,    &P->zq,     &P->grid,
                       &P->recs, &P->perm,  &P->skeys,  &P->hive_start, &P->binws, &P->fftwork,
                       &P->io_uvw, &P->io_vis, &P->io_wgt, &P->io_dirty, &P->polyf, &P->polyd, &P->recs_tmp,
-                      &P->chan_uvw, &P->chan_scale, &P->coltw, &P->acc};
+                      &P->chan_uvw, &P->chan_scale, &P->coltw, &P->acc, &P->roots};
   for (auto b : bs) cg::release(*b);
   if (P->h_mm) cudaFreeHost(P->h_mm);
   if (P->io_stream) cudaStreamDestroy(P->io_stream);
@@ -367,6 +367,7 @@ int cg_plan_create(cg_plan** plan, int nxdirty, int nydirty, double fov, double 
   if (const char* m = getenv("CG_FFT_PRUNE")) P->fft_pruning = atoi(m) != 0;
   if (const char* m = getenv("CG_COL_FFT")) P->col_fft = atoi(m) != 0;
   if (const char* m = getenv("CG_ROW_FFT")) P->row_fft = atoi(m) != 0;
+  if (const char* m = getenv("CG_COL_FFT_REG")) P->four_step = atoi(m) == 4;
   if (const char* m = getenv("CG_AUTOTUNE")) P->autotune = atoi(m) != 0;
   if (const char* m = getenv("CG_DEGRID_TMA")) P->tma_default = atoi(m);
   st = cg::plan_configure(P, nxdirty, nydirty, fov, epsilon, sigma, sign, precision);

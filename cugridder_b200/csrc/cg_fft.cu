@@ -824,7 +824,176 @@ int launch_l(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, 
              : launch_lc<L, 2>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st);
 }
 
+// ---------------------------------------------------------------- four-step
+// Column transforms of length L = 64 * L2 in two in-place passes over 16
+// adjacent columns per CTA, so that every load and store is a 128-byte grid
+// row segment (the one-pass column kernels move 16 bytes per row).  With
+// j = j1 + L2 j2 and k = k2 + 64 k1:
+//   X[k2 + 64 k1] = sum_j1 w_L2^(j1 k1) w_L^(j1 k2) sum_j2 x[j1 + L2 j2] w_64^(j2 k2).
+// Inverse (x natural): pass 1 = 64-point DFTs over the row sets
+// {j1 + L2 j2}, times w_L^(j1 k2), in place; pass 2 = L2-point DFTs over the
+// row blocks [L2 k2, L2 k2 + L2), in place, so row k1 + L2 k2 holds
+// X[k2 + 64 k1]: index g sits at row perm(g) = g / 64 + L2 (g % 64), which the
+// w-DFT reads through.  Forward: the plane fill writes index g at row
+// perm(g); pass 1 = L2-point DFTs over the blocks, times w_L^(k2 j1), in
+// place; pass 2 = 64-point DFTs over the row sets, in place: natural output.
+//
+// One item = one row set of N rows (row s * base_mul + r * stride, r < N)
+// of 16 columns of one plane.  Thread tid holds points tc + m (N/8) (m < 8)
+// of column tid % 16, tc = tid / 16, so the 16 lanes of a half-warp touch one
+// 128-byte row segment.  Radix-8 Stockham passes exchange through shared
+// memory laid out [position][column]; roots[n] = e^{2 pi i n / L} gives every
+// twiddle (conjugated for sign -1).
+template <int N>
+__device__ __forceinline__ void small_fft8(float2 (&x)[8], int tc, int col, float2* xs, int sign,
+                                           const float2* __restrict__ roots, int L) {
+  constexpr int T = N / 8;
+  constexpr int RL = [] {
+    int ns = 1;
+    while (ns * 8 <= N) ns *= 8;
+    return N / ns;
+  }();
+  auto w = [&](int e, int den) {  // w_den^e, den divides L
+    const float2 r = roots[(int)(((int64_t)e * (L / den)) % L)];
+    return make_float2(r.x, sign * r.y);
+  };
+  int Ns = 1;
+#pragma unroll 1
+  for (; Ns * 8 <= N; Ns *= 8) {
+    const int k = tc & (Ns - 1);
+    if (Ns > 1) {
+#pragma unroll
+      for (int m = 1; m < 8; m++) x[m] = cmul(x[m], w(m * k, Ns * 8));
+    }
+    dft_reg<8>(x, sign);
+    if (Ns * 8 == N) return;  // last pass: outputs at tc + m T
+    const int o0 = (tc - k) * 8 + k;
+#pragma unroll
+    for (int m = 0; m < 8; m++) xs[(o0 + m * Ns) * 16 + col] = x[m];
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < 8; m++) x[m] = xs[(tc + m * T) * 16 + col];
+    __syncthreads();
+  }
+  if constexpr (RL > 1) {
+    constexpr int Q = 8 / RL;
+#pragma unroll
+    for (int q = 0; q < Q; q++) {
+      const int j = tc + q * T;
+      float2 v[RL];
+#pragma unroll
+      for (int m = 0; m < RL; m++) {
+        v[m] = x[q + m * Q];
+        if (m > 0) v[m] = cmul(v[m], w(m * j, N));
+      }
+      dft_reg<RL>(v, sign);
+#pragma unroll
+      for (int m = 0; m < RL; m++) x[q + m * Q] = v[m];
+    }
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(2 * N) k_col_step(float2* __restrict__ grid, int nf1,
+                                                    size_t plane, int c0a, int na, int c0b,
+                                                    int nb, int L, int nsets, int base_mul,
+                                                    int stride, int sign,
+                                                    const float2* __restrict__ roots,
+                                                    int twiddle) {
+  constexpr int T = N / 8;
+  __shared__ float2 xs[N * 16];
+  const int tid = threadIdx.x, col = tid & 15, tc = tid >> 4;
+  const int groups_a = na / 16, groups = groups_a + nb / 16;
+  const int64_t item = blockIdx.x;
+  const int sset = (int)(item % nsets);
+  const int64_t rest = item / nsets;
+  const int gi = (int)(rest % groups), p = (int)(rest / groups);
+  const int col0 = gi < groups_a ? c0a + gi * 16 : c0b + (gi - groups_a) * 16;
+  float2* base = grid + (size_t)p * plane + col0 + col;
+  const int row0 = sset * base_mul;
+  float2 x[8];
+#pragma unroll
+  for (int m = 0; m < 8; m++) x[m] = base[(size_t)(row0 + (tc + m * T) * stride) * nf1];
+  small_fft8<N>(x, tc, col, xs, sign, roots, L);
+  if (twiddle) {  // output k of set s times w_L^(s k)
+#pragma unroll
+    for (int m = 0; m < 8; m++) {
+      const int k = tc + m * T;
+      const float2 r = roots[(int)(((int64_t)sset * k) % L)];
+      x[m] = cmul(x[m], make_float2(r.x, sign * r.y));
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < 8; m++) base[(size_t)(row0 + (tc + m * T) * stride) * nf1] = x[m];
+}
+
+template <int N>
+int launch_step(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, int c0b, int nb,
+                int L, int nsets, int base_mul, int stride, int sign, const float2* roots,
+                int twiddle, cudaStream_t st) {
+  const int64_t items = (int64_t)(na / 16 + nb / 16) * nplanes * nsets;
+  if (items < 1) return CG_OK;
+  if (items > 2147483647LL) return CG_ERR_SIZE;
+  k_col_step<N><<<(unsigned)items, 2 * N, 0, st>>>(grid, nf1, plane, c0a, na, c0b, nb, L, nsets,
+                                                   base_mul, stride, sign, roots, twiddle);
+  count_launches(1);
+  CG_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+int step_n(int N, float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, int c0b,
+           int nb, int L, int nsets, int base_mul, int stride, int sign, const float2* roots,
+           int twiddle, cudaStream_t st) {
+#define CG_STEP_CALL(n) \
+  launch_step<n>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, L, nsets, base_mul, stride, sign, roots, twiddle, st)
+  switch (N) {
+    case 16: return CG_STEP_CALL(16);
+    case 32: return CG_STEP_CALL(32);
+    case 64: return CG_STEP_CALL(64);
+    case 128: return CG_STEP_CALL(128);
+    default: return CG_ERR_ARG;
+  }
+#undef CG_STEP_CALL
+}
+
 }  // namespace
+
+bool four_step_supported(int L, int na, int nb) {
+  return (L == 1024 || L == 2048 || L == 4096 || L == 8192) && na % 16 == 0 && nb % 16 == 0;
+}
+
+int make_fft_roots(int L, float2* d_roots, cudaStream_t st) {
+  std::vector<float2> h(L);
+  for (int n = 0; n < L; n++) {
+    const double a = 2.0 * kPi * (double)n / (double)L;
+    h[n] = make_float2((float)std::cos(a), (float)std::sin(a));
+  }
+  CG_CUDA(cudaMemcpyAsync(d_roots, h.data(), sizeof(float2) * L, cudaMemcpyHostToDevice, st));
+  CG_CUDA(cudaStreamSynchronize(st));
+  return CG_OK;
+}
+
+int launch_col_fft_four_step(float2* grid, int L, int nf1, size_t plane, int nplanes, int c0a,
+                             int na, int c0b, int nb, int sign, const float2* d_roots,
+                             cudaStream_t st) {
+  if (!four_step_supported(L, na, nb)) return CG_ERR_ARG;
+  const int L2 = L / 64;
+  // strided sets: 64 rows j1 + L2 j2 (s = j1); blocks: L2 rows L2 k2 + r (s = k2)
+  auto sets = [&](int twiddle) {
+    return step_n(64, grid, nf1, plane, nplanes, c0a, na, c0b, nb, L, L2, 1, L2, sign, d_roots,
+                  twiddle, st);
+  };
+  auto blocks = [&](int twiddle) {
+    return step_n(L2, grid, nf1, plane, nplanes, c0a, na, c0b, nb, L, 64, L2, 1, sign, d_roots,
+                  twiddle, st);
+  };
+  if (sign > 0) {  // inverse: natural in, permuted out
+    CG_TRY(sets(1));
+    return blocks(0);
+  }
+  CG_TRY(blocks(1));  // forward: permuted in, natural out
+  return sets(0);
+}
 
 int launch_row_fft(float2* grid, int L, size_t plane, int nplanes, int r0, int nrows, int sign,
                    const float2* d_tw, cudaStream_t st, int mid0, int mid1, int skip) {

@@ -41,7 +41,16 @@ struct Geom {
   // coefficients in the working precision; null pointers select ES
   const float* polyf;
   const double* polyd;
+  // four-step column transform active (its L2 = nf2 / 64; 0 = off): grid
+  // index g along dim 1 sits at row g / 64 + rowperm * (g % 64) between the
+  // column transform and the w stage (see row_of)
+  int rowperm;
 };
+
+// storage row of grid index g along dim 1 (identity unless rowperm)
+__host__ __device__ __forceinline__ int row_of(const Geom& g, int g1) {
+  return g.rowperm ? g1 / 64 + g.rowperm * (g1 % 64) : g1;
+}
 
 constexpr int kPolyCoef = 8;  // degree-7 Horner polynomial per segment
 

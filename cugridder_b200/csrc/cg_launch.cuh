@@ -106,6 +106,15 @@ int launch_degrid_tma(const Rec<float>* d_recs, const int* d_perm, const int* d_
 bool col_fft_supported(int L, int na, int nb);
 size_t col_fft_twiddle_count(int L);
 int make_col_fft_twiddles(int L, float2* d_tw, cudaStream_t st);
+// Four-step column transforms (FP32, L = 64 * L2, L in 1024..8192, na and nb
+// multiples of 16): inverse (sign +1) leaves index g at row
+// g / 64 + L2 (g % 64); forward (sign -1) expects its input there and
+// leaves natural order.  d_roots: e^{2 pi i n / L}, n < L (make_fft_roots).
+bool four_step_supported(int L, int na, int nb);
+int make_fft_roots(int L, float2* d_roots, cudaStream_t st);
+int launch_col_fft_four_step(float2* grid, int L, int nf1, size_t plane, int nplanes, int c0a,
+                             int na, int c0b, int nb, int sign, const float2* d_roots,
+                             cudaStream_t st);
 // Row transforms (FP32, power-of-two L = nf1, the columns' twiddle table
 // when nf1 = nf2) of rows [r0, r0 + nrows) (nrows even) of nplanes planes;
 // elements [mid0, mid1) skipped as for launch_col_fft.

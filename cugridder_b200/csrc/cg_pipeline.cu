@@ -305,6 +305,29 @@ int plan_configure(cg_plan_s* P, int nx, int ny, double fov, double eps, double 
 
 // ------------------------------------------------------------ per-call geometry
 // setup_gridder_plan (cugridder.cu:29-86) with the w range from the device.
+// the band-pruned transform pays off for this geometry (else the full 2-D one runs)
+static bool fft_is_pruned(const cg_plan_s* P, const Geom& g) {
+  const int nrows = g.band_r1 - g.band_r0 + 1;
+  const double full = 2.0 * g.nf1 * g.nf2;
+  const double pruned = (double)nrows * g.nf1 + (double)g.N1 * g.nf2;
+  return P->fft_pruning && pruned <= 0.8 * full;
+}
+
+static bool cols_all_env() {
+  static const bool v = getenv("CG_FFT_COLS_ALL") && atoi(getenv("CG_FFT_COLS_ALL")) != 0;
+  return v;
+}
+
+// L2 of the four-step column transform when it will run for this geometry
+// (FP32 plans with the column kernels, band-pruned transform, resident
+// planes, image halves in whole 16-column groups), else 0
+static int four_step_rows(const cg_plan_s* P, const Geom& g) {
+  if (!P->four_step || P->precision != CG_PREC_FP32 || !P->col_fft || P->plane_batch ||
+      cols_all_env() || !fft_is_pruned(P, g) || g.N1 % 2 != 0)
+    return 0;
+  return four_step_supported(g.nf2, g.N1 / 2, g.N1 / 2) ? g.nf2 / 64 : 0;
+}
+
 static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw) {
   if (nrow < 0 || nrow > 2147483647LL) {
     set_last_error("nrow out of range");
@@ -421,6 +444,7 @@ static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw)
   CG_TRY(ensure(P->binws, bin_workspace_bytes(nrow, P->key_bytes)));
   CG_TRY(ensure(P->recs, (size_t)nrow * (tsz == 8 ? sizeof(Rec<double>) : sizeof(Rec<float>))));
   CG_TRY(ensure(P->recs_tmp, (size_t)nrow * (tsz == 8 ? sizeof(Rec<double>) : sizeof(Rec<float>))));
+  P->geom.rowperm = four_step_rows(P, P->geom);
   return CG_OK;
 }
 
@@ -538,9 +562,7 @@ static int exec_c2c(cg_plan_s* P, cufftHandle h, void* data, int direction) {
 static int fft_exec_pruned(cg_plan_s* P, void* d_grid, int direction) {
   const Geom& g = P->geom;
   const int nrows = g.band_r1 - g.band_r0 + 1;
-  const double full = 2.0 * g.nf1 * g.nf2;
-  const double pruned = (double)nrows * g.nf1 + (double)g.N1 * g.nf2;
-  if (!P->fft_pruning || pruned > 0.8 * full) return fft_exec(P, d_grid, direction);
+  if (!fft_is_pruned(P, g)) return fft_exec(P, d_grid, direction);
   // rows plan: batch rounded up to 64 rows (extra rows are zero or unused)
   int batch = std::min(g.nf2, ((nrows + 63) / 64) * 64);
   if (!P->rows_valid || P->rows_n != g.nf1 || P->rows_batch != batch) {
@@ -549,7 +571,7 @@ static int fft_exec_pruned(cg_plan_s* P, void* d_grid, int direction) {
     P->rows_batch = batch;
   }
   // CG_FFT_COLS_ALL=1 (tuning): one column transform over every grid column
-  static const bool cols_all = getenv("CG_FFT_COLS_ALL") && atoi(getenv("CG_FFT_COLS_ALL")) != 0;
+  const bool cols_all = cols_all_env();
   const int half = cols_all ? g.nf1 : g.N1 / 2;
   if (!P->cols_valid || P->cols_n != g.nf2 || P->cols_stride != g.nf1 || P->cols_batch != half) {
     CG_TRY(make_1d_plan(P, P->fft_cols, P->cols_valid, g.nf2, g.nf1, half));
@@ -567,6 +589,28 @@ static int fft_exec_pruned(cg_plan_s* P, void* d_grid, int direction) {
     if (s1 > 1 || cols_all) return s1;
     return exec_c2c(P, P->fft_cols, base + esz * (p * plane + (size_t)(g.nf1 - half)), direction);
   };
+  // four-step column transform (two in-place passes over 16-column groups;
+  // the w stage and the plane fill address rows through row_of)
+  if (g.rowperm) {
+    if (P->roots_n != g.nf2) {
+      CG_TRY(ensure(P->roots, sizeof(float2) * g.nf2));
+      CG_TRY(make_fft_roots(g.nf2, (float2*)P->roots.p, P->stream));
+      P->roots_n = g.nf2;
+    }
+    auto cols4 = [&]() {
+      return launch_col_fft_four_step((float2*)d_grid, g.nf2, g.nf1, plane, g.nw, 0, half,
+                                      g.nf1 - half, half, direction == CUFFT_INVERSE ? 1 : -1,
+                                      (const float2*)P->roots.p, P->stream);
+    };
+    if (direction == CUFFT_INVERSE) {
+      for (int p = 0; p < g.nw; p++) CG_TRY(rows(p));
+      CG_TRY(cols4());
+    } else {
+      CG_TRY(cols4());
+      for (int p = 0; p < g.nw; p++) CG_TRY(rows(p));
+    }
+    return CG_OK;
+  }
   // FP32 power-of-two columns: the shared-memory column transform over every
   // plane in one launch (the image's two column ranges of N1/2)
   if (P->col_fft && !cols_all && P->precision == CG_PREC_FP32 &&

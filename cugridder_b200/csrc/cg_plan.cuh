@@ -63,7 +63,7 @@ struct cg_plan_s {
   double poly[cg::kMaxW * cg::kPolyCoef] = {};
   // device buffers
   cg_dev_buf mm, K1, K2, K3q, zq, grid, recs, perm, skeys, hive_start, binws, fftwork, io_uvw,
-      io_vis, io_wgt, io_dirty, polyf, polyd, recs_tmp, chan_uvw, chan_scale, coltw, acc;
+      io_vis, io_wgt, io_dirty, polyf, polyd, recs_tmp, chan_uvw, chan_scale, coltw, acc, roots;
   unsigned long long* h_mm = nullptr;  // pinned, 2 words + flag
   // cuFFT: full 2-D batched plan, and the 1-D plans of the band-pruned path
   cufftHandle fft = 0;
@@ -75,6 +75,8 @@ struct cg_plan_s {
   int rows_n = 0, rows_batch = 0, cols_n = 0, cols_stride = 0, cols_batch = 0;
   int fft_pruning = 1;  // 0: always the full 2-D transform (CG_FFT_PRUNE=0)
   int col_fft = 1;      // 0: cuFFT for the column transforms too (CG_COL_FFT=0)
+  int four_step = 0;    // four-step column transform (CG_COL_FFT_REG=4 at creation)
+  int roots_n = 0;      // length of the root table in roots
   int row_fft = 0;      // 1: register-resident row kernel instead of cuFFT rows (CG_ROW_FFT=1; slower on B200)
   int coltw_n = 0;      // length of the twiddle table in coltw
   // memory-limited mode (cg_plan_set_grid_budget): the grid holds plane_batch

@@ -90,7 +90,7 @@ __global__ void k_wdft_deconv(const T* __restrict__ fw, Geom g, const double* __
   const int row = blockIdx.y;
   if (col >= g.N1) return;
   const size_t plane = (size_t)g.nf1 * g.nf2;
-  const size_t idx = (size_t)cmcl(row, g.N2, g.nf2) * g.nf1 + cmcl(col, g.N1, g.nf1);
+  const size_t idx = (size_t)row_of(g, cmcl(row, g.N2, g.nf2)) * g.nf1 + cmcl(col, g.N1, g.nf1);
   double fr, fi, zp;
   pixel_factor(g, row, col, K1, K2, K3q, zq, 1.0, fr, fi, zp);
   // sum_p fw[p] exp(i zp (p - nw/2)), phase by rotation
@@ -133,7 +133,7 @@ __global__ void k_plane_fill(const T* __restrict__ dirty, Geom g, const double* 
   const int g1 = blockIdx.y;
   if (g0 >= g.nf1) return;
   const size_t plane = (size_t)g.nf1 * g.nf2;
-  V* f = reinterpret_cast<V*>(fw) + (size_t)g1 * g.nf1 + g0;
+  V* f = reinterpret_cast<V*>(fw) + (size_t)row_of(g, g1) * g.nf1 + g0;
   const int col = inv_cmcl(g0, g.N1, g.nf1), row = inv_cmcl(g1, g.N2, g.nf2);
   if (col < 0 || row < 0) {
     V zero;

@@ -48,7 +48,7 @@ def _run(torch, d, img, col_fft):
 
 VARIANTS = {"registers": {}, "registers_row_kernel": {"CG_ROW_FFT": "1"},
             "registers_pair_exchange": {"CG_COL_FFT_REG": "2"},
-            "cluster": {"CG_COL_FFT_REG": "3"},
+            "cluster": {"CG_COL_FFT_REG": "3"}, "four_step": {"CG_COL_FFT_REG": "4"},
             "shared_pair": {"CG_COL_FFT_REG": "0"},
             "shared_single": {"CG_COL_FFT_REG": "0", "CG_COL_FFT_CB": "1"}}
 
@@ -75,14 +75,21 @@ def test_column_fft_matches_cufft(torch_cuda, N, variant):
     assert rel_l2(a[1], b[1]) < 2e-6
 
 
+@pytest.mark.parametrize("variant", ["registers", "four_step"])
 @pytest.mark.parametrize("nx,ny", [(512, 1024), (1024, 512)])
-def test_column_fft_non_square(torch_cuda, nx, ny):
+def test_column_fft_non_square(torch_cuda, nx, ny, variant):
     """Non-square images: the column length (nf2, from nx) and the image rows
     it skips, [nx - nx/2, nf2 - nx/2), differ from the row length (nf1)."""
     d = _narrow_band_case(max(nx, ny), 100_000, seed=nx + 3 * ny)
     d["nx"], d["ny"] = nx, ny
     img = synth.random_image(nx, ny, seed=5)
-    a = _run(torch_cuda, d, img, True)
+    env = VARIANTS[variant]
+    os.environ.update(env)
+    try:
+        a = _run(torch_cuda, d, img, True)
+    finally:
+        for k in env:
+            del os.environ[k]
     b = _run(torch_cuda, d, img, False)
     assert a[2]["nf2"] == 2 * nx and a[2]["nf1"] == 2 * ny
     assert rel_l2(a[0], b[0]) < 2e-6
