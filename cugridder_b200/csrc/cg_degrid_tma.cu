@@ -79,7 +79,7 @@ __device__ __forceinline__ void tma_load_3d(unsigned dst, const CUtensorMap* map
 // current one is interpolated (one CTA per SM), 1 = one box at a time (two
 // CTAs per SM overlap each other's staging and interpolation)
 template <int W, int NT, int NS>
-__global__ void __launch_bounds__(NT, NS == 1 ? 2 : 1) k_degrid_tma(
+__global__ void __launch_bounds__(NT, NS == 1 ? (NT <= 128 ? 3 : 2) : 1) k_degrid_tma(
     const __grid_constant__ CUtensorMap map, const Rec<float>* __restrict__ recs,
     const int* __restrict__ perm, const int* __restrict__ hive_start, int64_t M, Geom g,
     TmaTile tc, const float2* __restrict__ fw, float* __restrict__ vis, int* __restrict__ counter,
@@ -295,10 +295,12 @@ size_t tma_smem(const TmaTile& tc, int ns) {
   return 1024 + ns * tc.stage_bytes + 16 + (size_t)(tc.nslots + 1) * kSegInts * 4;
 }
 
-// variant 1: 512 threads, two stages; variant 2: 256 threads, one stage
+// variant 1: 32 x 16 tiles, 512 threads, two stages; variant 2: 32 x 16
+// tiles, 256 threads, one stage; variant 3: 32 x 8 tiles, 128 threads, one
+// stage (three CTAs per SM)
 bool tma_tiling(const Geom& g, TmaTile& tc, int variant) {
   const int W = g.kw;
-  const int tx = 32, ty = 16;
+  const int tx = 32, ty = variant == 3 ? 8 : 16;
   tc.TX = tx;
   tc.TY = ty;
   tc.SX = (tx + W + 1 + 1) & ~1;
@@ -310,11 +312,11 @@ bool tma_tiling(const Geom& g, TmaTile& tc, int variant) {
   tc.nslots = ((ty >> 3) + 1) * g.nw * 3;
   tc.stage_bytes = ((size_t)tc.SX * tc.SY * tc.SZ * sizeof(float2) + 1023) & ~(size_t)1023;
   // box dimensions <= 256, grid rows 16-byte multiples; two stages on one
-  // SM (variant 1) or two one-stage CTAs on one SM (variant 2)
-  const size_t limit = variant == 2 ? 110 * 1024 : 220 * 1024;
-  return (variant == 1 || variant == 2) && g.nw <= 256 && tc.SX <= 256 && tc.SY <= 256 &&
+  // SM (variant 1), two (variant 2) or three (variant 3) one-stage CTAs per SM
+  const size_t limit = variant == 1 ? 220 * 1024 : (variant == 2 ? 110 * 1024 : 74 * 1024);
+  return variant >= 1 && variant <= 3 && g.nw <= 256 && tc.SX <= 256 && tc.SY <= 256 &&
          (g.nf1 % 2) == 0 && g.nf1 >= tc.SX && g.nf2 >= tc.SY &&
-         tma_smem(tc, variant == 2 ? 1 : 2) <= limit;
+         tma_smem(tc, variant == 1 ? 2 : 1) <= limit;
 }
 
 template <int W, int NT, int NS>
@@ -368,10 +370,12 @@ int launch_degrid_tma(const Rec<float>* d_recs, const int* d_perm, const int* d_
   TmaTile tc{};
   if (!tma_tiling(g, tc, variant)) return CG_ERR_ARG;
 #define CG_TMA_CALL(w)                                                                        \
-  (variant == 2 ? launch_w<w, 256, 1>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis,    \
-                                      d_counter, d_err, st)                                 \
-                : launch_w<w, 512, 2>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis,    \
-                                      d_counter, d_err, st))
+  (variant == 3   ? launch_w<w, 128, 1>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis,  \
+                                        d_counter, d_err, st)                               \
+   : variant == 2 ? launch_w<w, 256, 1>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis,  \
+                                        d_counter, d_err, st)                               \
+                  : launch_w<w, 512, 2>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis,  \
+                                        d_counter, d_err, st))
   switch (g.kw) {
     case 4: return CG_TMA_CALL(4);
     case 5: return CG_TMA_CALL(5);
