@@ -4,12 +4,12 @@ Runs oracle/_ref/libcurafft_ref.so -- the reference's sources compiled for
 sm_100a by oracle/ref.mk -- through its own C entry points (ms2dirty_2,
 dirty2ms_2, ms2dirtyf_2, dirty2msf_2; reference src/astro/cugridder.cu:541-571)
 on seeded inputs, and writes the outputs with the input checksums to an .npz.
-Needs a CUDA GPU; run it on the B200 box:
+Needs a CUDA GPU and the reference build:
 
-    python tests/golden/make_golden.py --out gpurun_out/golden/ref_golden.npz
+    python tests/golden/make_golden.py --out tests/golden/ref_golden.npz
 
-then copy the file to tests/golden/ref_golden.npz.  The tests regenerate the
-inputs from the seeds (cugridder_b200.synth) and check the checksums.
+The tests regenerate the inputs from the seeds (cugridder_b200.synth) and
+check the checksums.
 """
 import argparse
 import ctypes
@@ -69,7 +69,7 @@ def cases():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--lib", default=os.path.join(ROOT, "oracle", "_ref", "libcurafft_ref.so"))
-    ap.add_argument("--out", default=os.path.join(ROOT, "gpurun_out", "golden", "ref_golden.npz"))
+    ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden", "ref_golden.npz"))
     a = ap.parse_args()
     lib = ctypes.CDLL(a.lib)
     D, F, I = ctypes.c_double, ctypes.c_float, ctypes.c_int

@@ -8,7 +8,7 @@ same seeded data as bench.py, host pointers in and out as the reference's API
 takes them, and prints one JSON line per case with Mvis/s =
 nrow / (t_ms2dirty + t_dirty2ms).  Needs a CUDA GPU:
 
-    python tests/golden/time_reference_build.py --out gpurun_out/reference_gpu.json
+    python tests/golden/time_reference_build.py --out tests/golden/reference_gpu_b200.json
 """
 import argparse
 import ctypes
