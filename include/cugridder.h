@@ -216,8 +216,9 @@ int cg_plan_set_fixed_uvw(cg_plan *plan, int on);
  * threads per CTA) on the call's own data and keeps the fastest for later
  * calls.  Off by default; the environment variable CG_AUTOTUNE=1 turns it on
  * for plans created afterwards, the host entry points' cached plans
- * included.  cg_plan_get_tiling reports the tiling in the layout of
- * cg_batch_get_tiling. */
+ * included.  The tuning call synchronizes, so capture a plan's calls into a
+ * CUDA graph only after it.  cg_plan_get_tiling reports the tiling in the
+ * layout of cg_batch_get_tiling. */
 int cg_plan_set_autotune(cg_plan *plan, int on);
 int cg_plan_get_tiling(const cg_plan *plan, int *tiling, float *tuned_ms);
 
