@@ -306,8 +306,14 @@ def run_b200(args, rank, world, local):
         if sample_clocks:
             clocks.stop()
         ms = e0.elapsed_time(e1)
+        # adjointness of the last step's pair: <dirty2ms(img), vis> = <img, ms2dirty(vis)>
+        # (inner products in FP64, so that their own rounding does not enter)
+        f64 = torch.complex128
+        ip1 = complex(torch.vdot(vout.reshape(-1).to(f64), vis.reshape(-1).to(f64)).item())
+        ip2 = complex(torch.vdot(dimg.reshape(-1).to(f64), dirty.reshape(-1).to(f64)).item())
+        adjoint = abs(ip1 - ip2) / max(abs(ip1), abs(ip2), 1e-300)
         gt, dt, tms = plan.tiling()
-        out = {"ms": ms, "launches": launches, "info": plan.info(),
+        out = {"ms": ms, "launches": launches, "info": plan.info(), "adjointness": adjoint,
                "tiling": {"grid_warp_tile": list(gt), "degrid_tile": list(dt),
                           "tuned_launch_ms": [round(x, 3) for x in tms]}}
         if timing:
@@ -329,6 +335,7 @@ def run_b200(args, rank, world, local):
     res["gpu_launches"] = int(main["launches"])
     res["info"] = main["info"]
     res["tiling"] = main["tiling"]
+    res["adjointness"] = {"value_form": main["adjointness"]}
 
     # per-stage timing and roofline of the dominant kernel of this library
     tm = main["timing"]
@@ -358,6 +365,7 @@ def run_b200(args, rank, world, local):
 
     if not args.no_fp64:
         fp = timed_run("fp64", max(2, args.steps // 3), args.warmup)
+        res["adjointness"]["fp64_plain"] = fp["adjointness"]
         t64 = max_over_ranks(fp["ms"], world)
         v64 = total_rows * max(2, args.steps // 3) / (t64 / 1e3) / 1e6
         res["fp64_plain"] = {"value": round(v64, 2), "ms_per_step": round(t64 / max(2, args.steps // 3), 3),
@@ -717,7 +725,7 @@ def main():
             "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res.get("e2e"),
             "gpu_launches": res["gpu_launches"], "clocks": res["clocks"],
             "fp64_plain": res.get("fp64_plain"), "fp32_over_fp64": res.get("fp32_over_fp64"),
-            "accuracy": res.get("accuracy"),
+            "accuracy": res.get("accuracy"), "adjointness": res.get("adjointness"),
             "stages": res["stages"],
         }
         print(json.dumps(line), flush=True)
