@@ -951,6 +951,7 @@ int step_n(int N, float2* grid, int nf1, size_t plane, int nplanes, int c0a, int
     case 32: return CG_STEP_CALL(32);
     case 64: return CG_STEP_CALL(64);
     case 128: return CG_STEP_CALL(128);
+    case 256: return CG_STEP_CALL(256);
     default: return CG_ERR_ARG;
   }
 #undef CG_STEP_CALL
@@ -959,7 +960,8 @@ int step_n(int N, float2* grid, int nf1, size_t plane, int nplanes, int c0a, int
 }  // namespace
 
 bool four_step_supported(int L, int na, int nb) {
-  return (L == 1024 || L == 2048 || L == 4096 || L == 8192) && na % 16 == 0 && nb % 16 == 0;
+  return (L == 1024 || L == 2048 || L == 4096 || L == 8192 || L == 16384) && na % 16 == 0 &&
+         nb % 16 == 0;
 }
 
 int make_fft_roots(int L, float2* d_roots, cudaStream_t st) {

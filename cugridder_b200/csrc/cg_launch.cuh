@@ -107,7 +107,7 @@ int launch_degrid_tma(const Rec<float>* d_recs, const int* d_perm, const int* d_
 bool col_fft_supported(int L, int na, int nb);
 size_t col_fft_twiddle_count(int L);
 int make_col_fft_twiddles(int L, float2* d_tw, cudaStream_t st);
-// Four-step column transforms (FP32, L = 64 * L2, L in 1024..8192, na and nb
+// Four-step column transforms (FP32, L = 64 * L2, L in 1024..16384, na and nb
 // multiples of 16): inverse (sign +1) leaves index g at row
 // g / 64 + L2 (g % 64); forward (sign -1) expects its input there and
 // leaves natural order.  d_roots: e^{2 pi i n / L}, n < L (make_fft_roots).

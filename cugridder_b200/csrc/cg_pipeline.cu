@@ -320,10 +320,11 @@ static bool cols_all_env() {
 
 // L2 of the four-step column transform when it will run for this geometry
 // (FP32 plans with the column kernels, band-pruned transform, resident
-// planes, image halves in whole 16-column groups), else 0
+// planes, image halves in whole 16-column groups), else 0.  Chosen with
+// CG_COL_FFT_REG=4, and by default for L = 16384, beyond the one-pass kernels.
 static int four_step_rows(const cg_plan_s* P, const Geom& g) {
-  if (!P->four_step || P->precision != CG_PREC_FP32 || !P->col_fft || P->plane_batch ||
-      cols_all_env() || !fft_is_pruned(P, g) || g.N1 % 2 != 0)
+  if (!(P->four_step || g.nf2 == 16384) || P->precision != CG_PREC_FP32 || !P->col_fft ||
+      P->plane_batch || cols_all_env() || !fft_is_pruned(P, g) || g.N1 % 2 != 0)
     return 0;
   return four_step_supported(g.nf2, g.N1 / 2, g.N1 / 2) ? g.nf2 / 64 : 0;
 }

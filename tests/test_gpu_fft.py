@@ -94,3 +94,15 @@ def test_column_fft_non_square(torch_cuda, nx, ny, variant):
     assert a[2]["nf2"] == 2 * nx and a[2]["nf1"] == 2 * ny
     assert rel_l2(a[0], b[0]) < 2e-6
     assert rel_l2(a[1], b[1]) < 2e-6
+
+
+def test_four_step_16384(torch_cuda):
+    """8192 x 8192 image: columns of L = 16384, beyond the one-pass column
+    kernels, take the four-step transform by default."""
+    d = _narrow_band_case(8192, 200_000, seed=7)
+    img = synth.random_image(8192, 8192, seed=8)
+    a = _run(torch_cuda, d, img, True)
+    b = _run(torch_cuda, d, img, False)
+    assert a[2]["nf2"] == 16384
+    assert rel_l2(a[0], b[0]) < 2e-6
+    assert rel_l2(a[1], b[1]) < 2e-6
