@@ -297,10 +297,11 @@ size_t tma_smem(const TmaTile& tc, int ns) {
 
 // variant 1: 32 x 16 tiles, 512 threads, two stages; variant 2: 32 x 16
 // tiles, 256 threads, one stage; variant 3: 32 x 8 tiles, 128 threads, one
-// stage (three CTAs per SM)
+// stage (three CTAs per SM); variant 4: 16 x 8 tiles, 128 threads, one stage
+// (many planes: two CTAs per SM up to ~38 planes at W = 8)
 bool tma_tiling(const Geom& g, TmaTile& tc, int variant) {
   const int W = g.kw;
-  const int tx = 32, ty = variant == 3 ? 8 : 16;
+  const int tx = variant == 4 ? 16 : 32, ty = variant >= 3 ? 8 : 16;
   tc.TX = tx;
   tc.TY = ty;
   tc.SX = (tx + W + 1 + 1) & ~1;
@@ -312,9 +313,9 @@ bool tma_tiling(const Geom& g, TmaTile& tc, int variant) {
   tc.nslots = ((ty >> 3) + 1) * g.nw * 3;
   tc.stage_bytes = ((size_t)tc.SX * tc.SY * tc.SZ * sizeof(float2) + 1023) & ~(size_t)1023;
   // box dimensions <= 256, grid rows 16-byte multiples; two stages on one
-  // SM (variant 1), two (variant 2) or three (variant 3) one-stage CTAs per SM
-  const size_t limit = variant == 1 ? 220 * 1024 : (variant == 2 ? 110 * 1024 : 74 * 1024);
-  return variant >= 1 && variant <= 3 && g.nw <= 256 && tc.SX <= 256 && tc.SY <= 256 &&
+  // SM (variant 1), two (variants 2, 4) or three (variant 3) one-stage CTAs per SM
+  const size_t limit = variant == 1 ? 220 * 1024 : (variant == 3 ? 74 * 1024 : 110 * 1024);
+  return variant >= 1 && variant <= 4 && g.nw <= 256 && tc.SX <= 256 && tc.SY <= 256 &&
          (g.nf1 % 2) == 0 && g.nf1 >= tc.SX && g.nf2 >= tc.SY &&
          tma_smem(tc, variant == 1 ? 2 : 1) <= limit;
 }
@@ -370,7 +371,7 @@ int launch_degrid_tma(const Rec<float>* d_recs, const int* d_perm, const int* d_
   TmaTile tc{};
   if (!tma_tiling(g, tc, variant)) return CG_ERR_ARG;
 #define CG_TMA_CALL(w)                                                                        \
-  (variant == 3   ? launch_w<w, 128, 1>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis,  \
+  (variant >= 3   ? launch_w<w, 128, 1>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis,  \
                                         d_counter, d_err, st)                               \
    : variant == 2 ? launch_w<w, 256, 1>(d_recs, d_perm, d_hive_start, M, g, tc, d_fw, d_vis,  \
                                         d_counter, d_err, st)                               \

@@ -97,7 +97,8 @@ int launch_degrid(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_sta
 // ---- degridding with TMA-staged tiles (cg_degrid_tma.cu; FP32, W 4..8) ----
 // d_err: a device int set to 1 when a staging wait ran out (the host checks it)
 // variant 1: 512 threads and two stages per CTA; 2: 256 threads and one
-// stage, two CTAs per SM; 3: 32 x 8 tiles, 128 threads, three CTAs per SM
+// stage, two CTAs per SM; 3: 32 x 8 tiles, 128 threads, three CTAs per SM;
+// 4: 16 x 8 tiles, 128 threads (many planes)
 bool degrid_tma_supported(const Geom& g, int variant);
 int launch_degrid_tma(const Rec<float>* d_recs, const int* d_perm, const int* d_hive_start,
                       int64_t M, const Geom& g, const float* d_fw, float* d_vis, int* d_counter,

@@ -679,13 +679,13 @@ int degrid_slots(const TileCfg& tc, int W) { return slots_for(tc.TY, tc.PB, W); 
 static const int kGridCand[][4] = {{16, 16, 0, 0},  {16, 8, 0, 0},  {16, 8, 64, 0},
                                    {16, 8, 64, 12}, {16, 16, 64, 0}, {32, 8, 0, 0},
                                    {16, 16, 5, 16}, {16, 16, 0, 12}};
-// threads -1 / -2 / -3: the TMA-staged kernel's variants (all planes; 32 x
-// 16 tiles with 512 threads and two stages / 256 threads and one stage; 32 x
-// 8 tiles with 128 threads and one stage) where they apply.
+// threads -1 .. -4: the TMA-staged kernel's variants (all planes; 32 x 16
+// tiles with 512 threads and two stages / 256 threads and one stage; 32 x 8
+// and 16 x 8 tiles with 128 threads and one stage) where they apply.
 static const int kDegridCand[][4] = {{32, 16, 0, 512}, {32, 32, 0, 512}, {32, 8, 0, 512},
                                      {16, 16, 0, 512}, {64, 16, 0, 512}, {32, 16, 0, 256},
                                      {16, 16, 0, 256}, {32, 16, 8, 512}, {32, 16, 0, -1},
-                                     {32, 16, 0, -2}, {32, 8, 0, -3}};
+                                     {32, 16, 0, -2}, {32, 8, 0, -3}, {16, 8, 0, -4}};
 
 int tile_candidates(int dir, const int (**cand)[4]) {
   if (dir == 0) {

@@ -37,7 +37,7 @@ def _dirty2ms(torch, d, img, eps, tma, kernel=None, calls=2):
     return outs, W
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4])
 @pytest.mark.parametrize("N,fov,eps", [(256, 2.0, 1e-3), (512, 1.0, 1e-4), (1024, 3.0, 1e-6)])
 def test_tma_degridding_matches_tiled(torch_cuda, N, fov, eps, variant):
     d = synth.make("wstack_2048_10M", seed=N, nrow=200_000, nx=N, ny=N, fov=fov)
