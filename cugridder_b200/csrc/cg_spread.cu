@@ -676,9 +676,10 @@ int degrid_slots(const TileCfg& tc, int W) { return slots_for(tc.TY, tc.PB, W); 
 // Autotuner candidates.  Gridding warp tiles (x, y, planes, warps per CTA):
 // planes 64 = all planes of the grid; 0 = the default.  Degridding tiles
 // (x, y, planes, threads per CTA).  The first of each list is the default.
-static const int kGridCand[][4] = {{16, 16, 0, 0},  {16, 8, 0, 0},  {16, 8, 64, 0},
+static const int kGridCand[][4] = {{16, 16, 0, 0},  {16, 8, 0, 0},   {16, 8, 64, 0},
                                    {16, 8, 64, 12}, {16, 16, 64, 0}, {32, 8, 0, 0},
-                                   {16, 16, 5, 16}, {16, 16, 0, 12}};
+                                   {16, 16, 5, 16}, {16, 16, 0, 12}, {16, 8, 10, 16},
+                                   {16, 8, 13, 12}, {16, 16, 8, 10}};
 // threads -1 .. -4: the TMA-staged kernel's variants (all planes; 32 x 16
 // tiles with 512 threads and two stages / 256 threads and one stage; 32 x 8
 // and 16 x 8 tiles with 128 threads and one stage) where they apply.
