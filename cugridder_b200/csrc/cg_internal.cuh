@@ -41,6 +41,9 @@ struct Geom {
   // coefficients in the working precision; null pointers select ES
   const float* polyf;
   const double* polyd;
+  // the forward column transform does not load the rows outside the image in
+  // the image's columns (one-pass column kernel): the plane fill leaves them
+  int fill_skip;
   // four-step column transform active (its L2 = nf2 / 64; 0 = off): grid
   // index g along dim 1 sits at row g / 64 + rowperm * (g % 64) between the
   // column transform and the w stage (see row_of)

@@ -318,6 +318,18 @@ static bool cols_all_env() {
   return v;
 }
 
+// The forward transform's columns go through the one-pass register-resident
+// kernel, which skips loading the rows outside the image (so the plane fill
+// need not zero them in the image's columns)
+static bool fill_skip_ok(const cg_plan_s* P, const Geom& g, int rowperm) {
+  if (rowperm || P->precision != CG_PREC_FP32 || !P->col_fft || P->plane_batch ||
+      cols_all_env() || !fft_is_pruned(P, g) || g.N1 % 2 != 0)
+    return false;
+  const char* e = getenv("CG_COL_FFT_REG");
+  if (e && atoi(e) != 1) return false;  // the other column kernels load every row
+  return col_fft_supported(g.nf2, g.N1 / 2, g.N1 / 2);
+}
+
 // L2 of the four-step column transform when it will run for this geometry
 // (FP32 plans with the column kernels, band-pruned transform, resident
 // planes, image halves in whole 16-column groups), else 0.  Chosen with
@@ -446,6 +458,7 @@ static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw)
   CG_TRY(ensure(P->recs, (size_t)nrow * (tsz == 8 ? sizeof(Rec<double>) : sizeof(Rec<float>))));
   CG_TRY(ensure(P->recs_tmp, (size_t)nrow * (tsz == 8 ? sizeof(Rec<double>) : sizeof(Rec<float>))));
   P->geom.rowperm = four_step_rows(P, P->geom);
+  P->geom.fill_skip = fill_skip_ok(P, P->geom, P->geom.rowperm) ? 1 : 0;
   return CG_OK;
 }
 

@@ -136,6 +136,9 @@ __global__ void k_plane_fill(const T* __restrict__ dirty, Geom g, const double* 
   V* f = reinterpret_cast<V*>(fw) + (size_t)row_of(g, g1) * g.nf1 + g0;
   const int col = inv_cmcl(g0, g.N1, g.nf1), row = inv_cmcl(g1, g.N2, g.nf2);
   if (col < 0 || row < 0) {
+    // cells in the image's columns but outside its rows are neither loaded
+    // nor kept by the one-pass forward column transform: no zeros needed
+    if (g.fill_skip && col >= 0) return;
     V zero;
     zero.x = (T)0;
     zero.y = (T)0;
