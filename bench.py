@@ -230,10 +230,15 @@ def algorithmic_bytes(stage, d, info, prec):
     G = info["nf1"] * info["nf2"] * info["nw"]
     npix = d["nx"] * d["ny"]
     nq = (d["nx"] // 2 + 1) * (d["ny"] // 2 + 1)
+    # FP32 power-of-two grids: the forward column kernel does not load the rows
+    # outside the image in the image's columns, and the plane fill skips them
+    fill_cells = G
+    if prec == "fp32" and info["nf2"] in (1024, 2048, 4096, 8192):
+        fill_cells = (info["nf1"] * info["nf2"] - (info["nf2"] - d["nx"]) * d["ny"]) * info["nw"]
     return {
         "gridding": M * rec + G * s_c,
         "degridding": G * s_c + M * rec + M * 4 + M * s_c,
-        "plane_fill": G * s_c + npix * s_c + nq * 16,
+        "plane_fill": fill_cells * s_c + npix * s_c + nq * 16,
         "wdft_deconv": info["nw"] * npix * s_c + npix * s_c + nq * 16,
         "fft": 4 * G * s_c,
         "sorted_stream": M * (4 + 24 + s_c + s_c // 2) + M * rec,
