@@ -348,12 +348,11 @@ __device__ __forceinline__ void grid_warp_tile(
         const T vr0 = cur.vr0, vi0 = cur.vi0;
         const int vx = cur.vx, vy = cur.vy, vz = cur.vz;
         T kx[W];
-        unsigned xmask = 0;
 #pragma unroll
-        for (int e = 0; e < W; e++) {
-          kx[e] = __shfl_sync(0xffffffffu, kv[0], e);
-          xmask |= ((unsigned)(vx + e >= 0 && vx + e < wx)) << e;
-        }
+        for (int e = 0; e < W; e++) kx[e] = __shfl_sync(0xffffffffu, kv[0], e);
+        // x taps inside the tile: the bits xlo .. xhi-1 (a taken row overlaps it)
+        const int xlo = max(0, -vx), xhi = min(W, wx - vx);
+        const unsigned xmask = ((1u << xhi) - 1u) & ~((1u << xlo) - 1u);
 #pragma unroll
         for (int rr = 0; rr < NRR; rr++) {
           const int pp = lane + 32 * rr;
