@@ -274,8 +274,9 @@ __device__ __forceinline__ void grid_warp_tile(
     const int total = t.pref[nslots];
     __syncwarp();  // every lane has read the table head before it can be rebuilt
     if (total == 0) {
+      const TileDiv div_x(wx), div_xy(wx * wy);
       for (int i = lane; i < wx * wy * wz; i += 32) {
-        const int x = i % wx, y = (i / wx) % wy, z = i / (wx * wy);
+        const int z = div_xy(i), r = i - z * wx * wy, y = div_x(r), x = r - y * wx;
         fwc[(size_t)(p0 + z) * plane + (size_t)(ty0 + y) * nf1 + tx0 + x] = zero;
       }
       return;
@@ -436,8 +437,9 @@ __device__ __forceinline__ void grid_warp_tile(
       }
     }
     // flush the tile, coalesced along x
+    const TileDiv div_x(wx), div_xy(wx * wy);
     for (int i = lane; i < wx * wy * wz; i += 32) {
-      const int x = i % wx, y = (i / wx) % wy, z = i / (wx * wy);
+      const int z = div_xy(i), r = i - z * wx * wy, y = div_x(r), x = r - y * wx;
       fwc[(size_t)(p0 + z) * plane + (size_t)(ty0 + y) * nf1 + tx0 + x] = acc[z * PS + y * RS + x];
     }
     __syncwarp();
@@ -532,8 +534,9 @@ __device__ __forceinline__ void degrid_tile(const Rec<T>* __restrict__ recs,
     using V = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
     V* stv = reinterpret_cast<V*>(stg);
     const V* fwv = reinterpret_cast<const V*>(fw);
+    const TileDiv div_x(SX), div_xy(SX * SY);
     for (int i = threadIdx.x; i < nstage; i += blockDim.x) {
-      const int sx = i % SX, sy = (i / SX) % SY, sz = i / (SX * SY);
+      const int sz = div_xy(i), r = i - sz * SX * SY, sy = div_x(r), sx = r - sy * SX;
       const int gx = modi(gx0 + sx, nf1), gy = modi(gy0 + sy, nf2), gz = modi(gz0 + sz, nw);
       stv[(sz * SY + sy) * SXP + sx] = fwv[(size_t)gz * plane + (size_t)gy * nf1 + gx];
     }

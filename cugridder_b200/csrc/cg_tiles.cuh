@@ -15,6 +15,19 @@ struct Halo {
 
 __device__ __forceinline__ int floordiv8(int a) { return a >= 0 ? a >> 3 : -((7 - a) >> 3); }
 
+// n / d for a tile index: 0 <= n, 0 < d, n * d < 2^32.  m = floor((2^32 - 1) / d) + 1
+// exceeds 2^32 / d by e = m - 2^32 / d < 1, so n * m / 2^32 = n / d + n * e / 2^32 and
+// the excess n * e / 2^32 < n / 2^32 < 1 / d never carries floor(n / d) over: the
+// multiply-high is exact (d = 1 would overflow m and is answered directly).
+struct TileDiv {
+  unsigned m;
+  int d;
+  __device__ __forceinline__ explicit TileDiv(int d_) : m(0xFFFFFFFFu / (unsigned)d_ + 1u), d(d_) {}
+  __device__ __forceinline__ int operator()(int n) const {
+    return d == 1 ? n : (int)__umulhi((unsigned)n, m);
+  }
+};
+
 // Segment table of one work item: contiguous runs of sorted rows (hives that
 // are neighbours along x share one run) with the periodic shift of their cells.
 struct SegTable {
