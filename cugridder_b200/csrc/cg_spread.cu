@@ -268,12 +268,26 @@ __device__ __forceinline__ void grid_warp_tile(
     const int tx0 = tix * TX, ty0 = tiy * TY, p0 = tib * PB;
     const int tx1 = min(tx0 + TX, nf1), ty1 = min(ty0 + TY, nf2), p1 = min(p0 + PB, nw);
     const int wx = tx1 - tx0, wy = ty1 - ty0, wz = p1 - p0;
+    // FP32 cells are written two at a time (16 bytes) when every pair is aligned:
+    // an even tile width and grid row length and a 16-byte aligned grid
+    const bool flush_pairs = sizeof(T) == 4 && ((wx | nf1) & 1) == 0 &&
+                             (reinterpret_cast<uintptr_t>(fw) & 15) == 0;
     const int nslots = warp_build_segments(g, hive_start, floordiv8(tx0 - hi),
                                            floordiv8(tx1 - 1 + lo), floordiv8(ty0 - hi),
                                            floordiv8(ty1 - 1 + lo), p0 - hi, p1 - 1 + lo, t);
     const int total = t.pref[nslots];
     __syncwarp();  // every lane has read the table head before it can be rebuilt
     if (total == 0) {
+      if (flush_pairs) {
+        const int hx = wx >> 1;
+        const TileDiv div_x(hx), div_xy(hx * wy);
+        for (int i = lane; i < hx * wy * wz; i += 32) {
+          const int z = div_xy(i), r = i - z * hx * wy, y = div_x(r), x = 2 * (r - y * hx);
+          *reinterpret_cast<float4*>(fwc + (size_t)(p0 + z) * plane + (size_t)(ty0 + y) * nf1 + tx0 + x) =
+              make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        return;
+      }
       const TileDiv div_x(wx), div_xy(wx * wy);
       for (int i = lane; i < wx * wy * wz; i += 32) {
         const int z = div_xy(i), r = i - z * wx * wy, y = div_x(r), x = r - y * wx;
@@ -437,10 +451,22 @@ __device__ __forceinline__ void grid_warp_tile(
       }
     }
     // flush the tile, coalesced along x
-    const TileDiv div_x(wx), div_xy(wx * wy);
-    for (int i = lane; i < wx * wy * wz; i += 32) {
-      const int z = div_xy(i), r = i - z * wx * wy, y = div_x(r), x = r - y * wx;
-      fwc[(size_t)(p0 + z) * plane + (size_t)(ty0 + y) * nf1 + tx0 + x] = acc[z * PS + y * RS + x];
+    if (flush_pairs) {
+      const int hx = wx >> 1;
+      const TileDiv div_x(hx), div_xy(hx * wy);
+      for (int i = lane; i < hx * wy * wz; i += 32) {
+        const int z = div_xy(i), r = i - z * hx * wy, y = div_x(r), x = 2 * (r - y * hx);
+        const C* a = acc + z * PS + y * RS + x;
+        const C a0 = a[0], a1 = a[1];
+        *reinterpret_cast<float4*>(fwc + (size_t)(p0 + z) * plane + (size_t)(ty0 + y) * nf1 + tx0 + x) =
+            make_float4((float)a0.x, (float)a0.y, (float)a1.x, (float)a1.y);
+      }
+    } else {
+      const TileDiv div_x(wx), div_xy(wx * wy);
+      for (int i = lane; i < wx * wy * wz; i += 32) {
+        const int z = div_xy(i), r = i - z * wx * wy, y = div_x(r), x = r - y * wx;
+        fwc[(size_t)(p0 + z) * plane + (size_t)(ty0 + y) * nf1 + tx0 + x] = acc[z * PS + y * RS + x];
+      }
     }
     __syncwarp();
   }

@@ -99,13 +99,24 @@ __global__ void k_wdft_deconv(const T* __restrict__ fw, Geom g, const double* __
   sincos(zp * (double)(-(g.nw / 2)), &pi, &pr);
   double sr = 0.0, si = 0.0;
   const V* f = reinterpret_cast<const V*>(fw) + idx;
-  for (int p = 0; p < g.nw; p++) {
-    V v = f[(size_t)p * plane];
-    sr += (double)v.x * pr - (double)v.y * pi;
-    si += (double)v.x * pi + (double)v.y * pr;
-    double t = pr * cs - pi * sn;
-    pi = pr * sn + pi * cs;
-    pr = t;
+  // planes in groups of kAhead: the group's loads are issued before the
+  // rotation recurrence consumes them
+  constexpr int kAhead = 8;
+  for (int p0 = 0; p0 < g.nw; p0 += kAhead) {
+    V v[kAhead];
+#pragma unroll
+    for (int k = 0; k < kAhead; k++)
+      if (p0 + k < g.nw) v[k] = f[(size_t)(p0 + k) * plane];
+#pragma unroll
+    for (int k = 0; k < kAhead; k++) {
+      if (p0 + k < g.nw) {
+        sr += (double)v[k].x * pr - (double)v[k].y * pi;
+        si += (double)v[k].x * pi + (double)v[k].y * pr;
+        double t = pr * cs - pi * sn;
+        pi = pr * sn + pi * cs;
+        pr = t;
+      }
+    }
   }
   V out;
   out.x = (T)(sr * fr - si * fi);
