@@ -223,9 +223,11 @@ __global__ void __launch_bounds__(NT, NS == 1 ? (NT <= 128 ? 3 : 2) : 1) k_degri
       const int lz = bz + taps<float, W>(r.f[2], beta, c, poly, kz);
       if (lx < 0 || ly < 0 || lx + W > SX || ly + W > SY) continue;  // cannot happen: tile rows only
       float sr = 0.f, si = 0.f;
+#pragma unroll
       for (int a = 0; a < W; a++) {
         const int zz = wrapi(lz + a, nw);
         float pr = 0.f, pi = 0.f;
+#pragma unroll
         for (int b = 0; b < W; b++) {
           const float2* row = st + ((size_t)zz * SY + (ly + b)) * SX + lx;
           float qr = 0.f, qi = 0.f;
