@@ -86,7 +86,8 @@ struct TileCfg {
 };
 
 // Warp-owned tiles of the gridding kernel: TX x TY cells times PB planes per
-// warp, cell (x, y, z) at z * PS + y * RS + x (complex units).
+// warp, cell (x, y, z) at z * PS + y * RS + x (complex units), y-major: PS =
+// TX + 1 is the plane stride inside a tile row and RS >= PB * PS the row stride.
 struct WarpTile {
   int TX, TY, PB, RS, PS, slots;
   int ntx, nty, npb, nitems;

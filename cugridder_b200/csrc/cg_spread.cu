@@ -255,7 +255,7 @@ __device__ __forceinline__ void grid_warp_tile(
   const int lane = threadIdx.x & 31;
   const int TX = tc.TX, TY = tc.TY, PB = tc.PB, RS = tc.RS, PS = tc.PS;
   C* acc = reinterpret_cast<C*>(wsmem);
-  int* tb = reinterpret_cast<int*>(wsmem + (size_t)PB * PS * sizeof(C));
+  int* tb = reinterpret_cast<int*>(wsmem + (size_t)TY * RS * sizeof(C));
   const int ts = tc.slots + 1;
   SegTable t{tb, tb + ts, tb + 2 * ts};
   const T beta = (T)g.beta, c = (T)g.es_c, halfw = (T)W * (T)0.5;
@@ -295,7 +295,7 @@ __device__ __forceinline__ void grid_warp_tile(
       }
       return;
     }
-    for (int i = lane; i < PB * PS; i += 32) acc[i] = zero;
+    for (int i = lane; i < TY * RS; i += 32) acc[i] = zero;
     __syncwarp();
     // Candidates are pre-scanned 32 at a time (one per lane); the next
     // chunk's records are loaded while the current chunk is spread.  Within a
@@ -371,7 +371,7 @@ __device__ __forceinline__ void grid_warp_tile(
 #pragma unroll
         for (int rr = 0; rr < NRR; rr++) {
           const int pp = lane + 32 * rr;
-          const int dy = pp % W, dz = pp / W;
+          const int dz = pp % W, dy = pp / W;  // lane = dy * W + dz = cell offset (mod 16)
           const T ky = __shfl_sync(0xffffffffu, kv[0], W + dy);
           const int zs = 2 * W + dz;
           T kz = __shfl_sync(0xffffffffu, kv[0], zs & 31);
@@ -401,7 +401,7 @@ __device__ __forceinline__ void grid_warp_tile(
           for (int it = 0; it < NTAIL; it++) {
             const int t = lane + 32 * it;
             const int pp = 32 * NFULL + t / W, e = t - (t / W) * W;
-            const int dy = pp % W, dz = pp / W;
+            const int dz = pp % W, dy = pp / W;
             const T ky = __shfl_sync(0xffffffffu, kv[0], W + dy);
             const int zs = 2 * W + dz;
             T kz = __shfl_sync(0xffffffffu, kv[0], zs & 31);
@@ -707,7 +707,8 @@ int degrid_slots(const TileCfg& tc, int W) { return slots_for(tc.TY, tc.PB, W); 
 static const int kGridCand[][4] = {{16, 16, 0, 0},  {16, 8, 0, 0},   {16, 8, 64, 0},
                                    {16, 8, 64, 12}, {16, 16, 64, 0}, {32, 8, 0, 0},
                                    {16, 16, 5, 16}, {16, 16, 0, 12}, {16, 8, 10, 16},
-                                   {16, 8, 13, 12}, {16, 16, 8, 10}};
+                                   {16, 8, 13, 12}, {16, 16, 8, 10}, {16, 8, 64, 13},
+                                   {16, 8, 64, 14}};
 // threads -1 .. -4: the TMA-staged kernel's variants (all planes; 32 x 16
 // tiles with 512 threads and two stages / 256 threads and one stage; 32 x 8
 // and 16 x 8 tiles with 128 threads and one stage) where they apply.
@@ -735,7 +736,7 @@ void set_tile_candidate(TileTune& tt, int dir, const int* c) {
 
 // dynamic shared memory of one warp-tiled gridding CTA at most (the SM
 // offers 227 KB to one CTA)
-constexpr size_t kWarpSmemMax = 226 * 1024;
+constexpr size_t kWarpSmemMax = 227 * 1024;
 
 // Warp tiles: 16 x 16 cells by default (CG_WTILE_X / CG_WTILE_Y); the plane
 // batch and warps per CTA are chosen so that two CTAs fit on an SM.
@@ -754,16 +755,17 @@ WarpTile warp_tiling(const Geom& g, const TileTune* tt) {
   }
   tc.TX = std::max(16, (tx / 16) * 16);
   tc.TY = std::max(8, (ty / 8) * 8);
-  tc.RS = tc.TX + 1;
+  tc.PS = tc.TX + 1;  // = 1 (mod 16): consecutive dz of a lane group hit consecutive banks
   if (PB <= 0) PB = std::min(g.nw, 7);
   PB = std::min(PB, g.nw);
   tc.PB = PB;
-  int ps = tc.TY * tc.RS;
-  ps += ((W % 16) - (ps % 16) + 16) % 16;  // PS = W (mod 16)
-  tc.PS = ps;
-  tc.slots = ((tc.TY >> 3) + 2) * (PB + W) * 3;
+  int rs = PB * tc.PS;
+  rs += ((W % 16) - (rs % 16) + 16) % 16;  // RS = W (mod 16): consecutive dy, W lanes apart
+  tc.RS = rs;
+  // hive rows of a tile: (TY / 8 + 2) along y times PB + halo planes, 3 runs each
+  tc.slots = ((tc.TY >> 3) + 2) * (PB + (W - 1) / 2 + (W + 1) / 2) * 3;
   tc.warp_bytes =
-      ((size_t)PB * tc.PS * 2 * sizeof(T) + (size_t)(tc.slots + 1) * kSegInts * 4 + 15) & ~(size_t)15;
+      ((size_t)tc.TY * tc.RS * 2 * sizeof(T) + (size_t)(tc.slots + 1) * kSegInts * 4 + 15) & ~(size_t)15;
   if (warps <= 0) warps = (int)std::max<size_t>(1, std::min<size_t>(8, (110 * 1024) / tc.warp_bytes));
   warps = std::min(warps, 16);
   while (warps > 1 && tc.warp_bytes * warps > kWarpSmemMax) warps--;
