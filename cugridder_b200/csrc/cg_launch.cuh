@@ -71,6 +71,7 @@ struct MultiShape {
   int threads;        // degridding threads per CTA
   size_t dsmem;       // degridding bytes per CTA (largest of the jobs)
   int grid_items, degrid_items;
+  bool partial_hives;  // some job's grid has an axis that is not a multiple of 8 cells
 };
 // Fill the item prefixes and the shared shape of jobs (host array).
 template <typename T>

@@ -241,7 +241,9 @@ __device__ __forceinline__ void load_lane_poly(const T* __restrict__ poly,
 
 // One warp tile (work item `item` of tiling tc): accumulate the tile in the
 // warp's shared-memory region `wsmem` and write every cell of it to fw.
-template <typename T, int W, bool kPoly>
+// kExactWrap: halo hive bounds from the wrapped cells (raw_hive_lo/hi), needed
+// when an axis of the grid is not a multiple of 8 cells; otherwise floordiv8.
+template <typename T, int W, bool kPoly, bool kExactWrap>
 __device__ __forceinline__ void grid_warp_tile(
     const Rec<T>* __restrict__ recs, const int* __restrict__ hive_start, const Geom& g,
     const WarpTile& tc, T* __restrict__ fw, int item, unsigned char* wsmem,
@@ -272,9 +274,16 @@ __device__ __forceinline__ void grid_warp_tile(
     // an even tile width and grid row length and a 16-byte aligned grid
     const bool flush_pairs = sizeof(T) == 4 && ((wx | nf1) & 1) == 0 &&
                              (reinterpret_cast<uintptr_t>(fw) & 15) == 0;
-    const int nslots = warp_build_segments(g, hive_start, floordiv8(tx0 - hi),
-                                           floordiv8(tx1 - 1 + lo), floordiv8(ty0 - hi),
-                                           floordiv8(ty1 - 1 + lo), p0 - hi, p1 - 1 + lo, t);
+    int nslots;
+    if constexpr (kExactWrap)
+      nslots = warp_build_segments(
+          g, hive_start, raw_hive_lo(tx0 - hi, nf1, g.nhx), raw_hive_hi(tx1 - 1 + lo, nf1, g.nhx),
+          raw_hive_lo(ty0 - hi, nf2, g.nhy), raw_hive_hi(ty1 - 1 + lo, nf2, g.nhy), p0 - hi,
+          p1 - 1 + lo, t);
+    else
+      nslots = warp_build_segments(g, hive_start, floordiv8(tx0 - hi), floordiv8(tx1 - 1 + lo),
+                                   floordiv8(ty0 - hi), floordiv8(ty1 - 1 + lo), p0 - hi,
+                                   p1 - 1 + lo, t);
     const int total = t.pref[nslots];
     __syncwarp();  // every lane has read the table head before it can be rebuilt
     if (total == 0) {
@@ -472,7 +481,7 @@ __device__ __forceinline__ void grid_warp_tile(
   }
 }
 
-template <typename T, int W, bool kPoly>
+template <typename T, int W, bool kPoly, bool kExactWrap>
 __global__ void __launch_bounds__(512) k_grid_warp(const Rec<T>* __restrict__ recs,
                                                    const int* __restrict__ hive_start, Geom g,
                                                    WarpTile tc, T* __restrict__ fw) {
@@ -483,7 +492,7 @@ __global__ void __launch_bounds__(512) k_grid_warp(const Rec<T>* __restrict__ re
   unsigned char* wsmem = smem + (size_t)wib * tc.warp_bytes;
   const int gwarp = blockIdx.x * tc.warps + wib, nwarps = gridDim.x * tc.warps;
   for (int item = gwarp; item < tc.nitems; item += nwarps)
-    grid_warp_tile<T, W, kPoly>(recs, hive_start, g, tc, fw, item, wsmem, pc);
+    grid_warp_tile<T, W, kPoly, kExactWrap>(recs, hive_start, g, tc, fw, item, wsmem, pc);
 }
 
 // index of the job holding global work item `item` (item0 ascending, item0[0] = 0)
@@ -500,7 +509,7 @@ __device__ __forceinline__ int find_job(const J* __restrict__ jobs, int njobs, i
 // Many grids in one persistent launch: warps take (job, tile) items from a
 // global queue; every job shares W and the kernel.  warp_bytes is the largest
 // per-warp footprint of the jobs' tilings.
-template <typename T, int W, bool kPoly>
+template <typename T, int W, bool kPoly, bool kExactWrap>
 __global__ void __launch_bounds__(512) k_grid_warp_multi(const GridJob<T>* __restrict__ jobs,
                                                          int njobs, int nitems, size_t warp_bytes,
                                                          int* __restrict__ counter) {
@@ -516,7 +525,7 @@ __global__ void __launch_bounds__(512) k_grid_warp_multi(const GridJob<T>* __res
     if (item >= nitems) break;
     const int j = find_job(jobs, njobs, item, [](const GridJob<T>& x) { return x.grid_item0; });
     const GridJob<T>& J = jobs[j];
-    grid_warp_tile<T, W, kPoly>(J.recs, J.hive_start, J.g, J.wt, J.fw, item - J.grid_item0, wsmem,
+    grid_warp_tile<T, W, kPoly, kExactWrap>(J.recs, J.hive_start, J.g, J.wt, J.fw, item - J.grid_item0, wsmem,
                                 pc);
   }
 }
@@ -762,8 +771,10 @@ WarpTile warp_tiling(const Geom& g, const TileTune* tt) {
   int rs = PB * tc.PS;
   rs += ((W % 16) - (rs % 16) + 16) % 16;  // RS = W (mod 16): consecutive dy, W lanes apart
   tc.RS = rs;
-  // hive rows of a tile: (TY / 8 + 2) along y times PB + halo planes, 3 runs each
-  tc.slots = ((tc.TY >> 3) + 2) * (PB + (W - 1) / 2 + (W + 1) / 2) * 3;
+  // hive rows of a tile: (TY / 8 + 2) along y, one more when the last hive row
+  // is partial (its low halo then spans two hive rows), times PB + halo
+  // planes, 3 runs each
+  tc.slots = ((tc.TY >> 3) + 2 + (g.nf2 % 8 != 0)) * (PB + (W - 1) / 2 + (W + 1) / 2) * 3;
   tc.warp_bytes =
       ((size_t)tc.TY * tc.RS * 2 * sizeof(T) + (size_t)(tc.slots + 1) * kSegInts * 4 + 15) & ~(size_t)15;
   if (warps <= 0) warps = (int)std::max<size_t>(1, std::min<size_t>(8, (110 * 1024) / tc.warp_bytes));
@@ -794,7 +805,9 @@ static int grid_w(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, cons
     return CG_OK;
   }
   WarpTile tc = warp_tiling<T>(g, tt);
-  auto* kern = geom_poly_host<T>(g) ? k_grid_warp<T, W, true> : k_grid_warp<T, W, false>;
+  const bool exact = (g.nf1 % 8) != 0 || (g.nf2 % 8) != 0;
+  auto* kern = geom_poly_host<T>(g) ? (exact ? k_grid_warp<T, W, true, true> : k_grid_warp<T, W, true, false>)
+                                    : (exact ? k_grid_warp<T, W, false, true> : k_grid_warp<T, W, false, false>);
   int per_sm = 0;
   CG_CUDA(kernel_occupancy((const void*)kern, tc.warps * 32, tc.smem, &per_sm));
   if (per_sm < 1) {
@@ -907,6 +920,7 @@ int multi_shape(GridJob<T>* jobs, int njobs, MultiShape* sh) {
     gi += J.wt.nitems;
     di += J.dt.nitems;
     sh->warp_bytes = std::max(sh->warp_bytes, J.wt.warp_bytes);
+    if ((J.g.nf1 % 8) != 0 || (J.g.nf2 % 8) != 0) sh->partial_hives = true;
     sh->dsmem = std::max(sh->dsmem, J.dt.smem);
     warps = std::min(warps, J.wt.warps);
   }
@@ -921,7 +935,8 @@ int multi_shape(GridJob<T>* jobs, int njobs, MultiShape* sh) {
 template <typename T, int W>
 static int grid_multi_w(const GridJob<T>* d_jobs, int njobs, const MultiShape& sh, int* d_counter,
                         cudaStream_t st) {
-  auto* kern = sh.poly ? k_grid_warp_multi<T, W, true> : k_grid_warp_multi<T, W, false>;
+  auto* kern = sh.poly ? (sh.partial_hives ? k_grid_warp_multi<T, W, true, true> : k_grid_warp_multi<T, W, true, false>)
+                       : (sh.partial_hives ? k_grid_warp_multi<T, W, false, true> : k_grid_warp_multi<T, W, false, false>);
   const size_t smem = sh.warp_bytes * sh.warps;
   int per_sm = 0;
   CG_CUDA(kernel_occupancy((const void*)kern, sh.warps * 32, smem, &per_sm));

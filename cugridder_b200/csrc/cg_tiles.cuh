@@ -15,6 +15,24 @@ struct Halo {
 
 __device__ __forceinline__ int floordiv8(int a) { return a >= 0 ? a >> 3 : -((7 - a) >> 3); }
 
+// Raw hive bounds of the cells [a, b] of one axis that a tile and its kernel
+// halo reach (the tile inside [0, nf), the halo outside it by less than nf),
+// for build_segments' single periodic wrap of hive indices: a raw hive h < 0
+// stands for hive h + nh with its cells shifted by -nf, a raw hive h >= nh for
+// hive h - nh shifted by +nf.  The bounds come from the WRAPPED cells:
+// cells a + nf .. nf - 1 below, 0 .. b - nf above.  When nf % 8 != 0 the last
+// hive is partial and the low halo's wrapped cells can span two hives
+// (nh - 2 and nh - 1), which floor(a / 8) would miss; when nf % 8 == 0 the
+// bounds equal floordiv8(a) and floordiv8(b), which the gridding kernels then
+// use instead (a separate instantiation, so that the common grid sizes keep
+// the code generation they were tuned with).
+__device__ __forceinline__ int raw_hive_lo(int a, int nf, int nh) {
+  return a < 0 ? ((a + nf) >> 3) - nh : a >> 3;
+}
+__device__ __forceinline__ int raw_hive_hi(int b, int nf, int nh) {
+  return b >= nf ? nh + ((b - nf) >> 3) : b >> 3;
+}
+
 // n / d for a tile index: 0 <= n, 0 < d, n * d < 2^32.  m = floor((2^32 - 1) / d) + 1
 // exceeds 2^32 / d by e = m - 2^32 / d < 1, so n * m / 2^32 = n / d + n * e / 2^32 and
 // the excess n * e / 2^32 < n / 2^32 < 1 / d never carries floor(n / d) over: the

@@ -72,6 +72,27 @@ def test_wst_case(nrow, nxdirty, nydirty, fov, seed=42, f0=1e9, use_wgt=True, si
     return dict(uvw=uvw, ms=ms, dirty=dirty, wgt=wgt, freq=f0, fov=fov, nx=nxdirty, ny=nydirty)
 
 
+def wrap_case(nrow, nx, ny, fov, freq=1.0e9, seed=0, reach=1.2, w_frac=0.1):
+    """Rows spread over the WHOLE uv grid and past its edge: u and v uniform in
+    +-reach times the image's Nyquist limit (1 / (2 pixel size) wavelengths),
+    so after the shift to [0, nf) rows land in every cell, including the first
+    and last hive of each axis, and with reach > 1 alias around the periodic
+    wrap.  w ~ U(-w_frac, w_frac) times the u limit.  vis complex N(0, 1),
+    wgt U(0.5, 1.5)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    rad = np.deg2rad(fov)
+    lam = C_LIGHT / freq
+    umax = reach * nx / (2.0 * rad) * lam  # metres
+    vmax = reach * ny / (2.0 * rad) * lam
+    uvw = np.empty((nrow, 3), dtype=np.float64)
+    uvw[:, 0] = rng.uniform(-umax, umax, nrow)
+    uvw[:, 1] = rng.uniform(-vmax, vmax, nrow)
+    uvw[:, 2] = rng.uniform(-w_frac * umax, w_frac * umax, nrow)
+    vis = rng.standard_normal(nrow) + 1j * rng.standard_normal(nrow)
+    wgt = rng.uniform(0.5, 1.5, nrow)
+    return dict(uvw=uvw, vis=vis, wgt=wgt, nx=nx, ny=ny, fov=float(fov), freq=float(freq))
+
+
 def random_image(nx, ny, seed=1, dtype=np.complex128):
     rng = np.random.Generator(np.random.PCG64(seed))
     img = np.zeros((nx, ny), dtype=dtype)

@@ -1,7 +1,17 @@
 """Shared helpers of the GPU tests: run the plan API on device buffers."""
 import numpy as np
 
-from cugridder_b200 import Plan
+from cugridder_b200 import Plan, synth
+
+
+def payload(d, p, sign=-1):
+    """Gridded strengths c_j = vis * wgt * exp(i o_c w_eff) of the reference's
+    prestage (ra_exec.cu:103-111; cuft.cu:46-66), for the oracle's spreading."""
+    w_eff = (d["uvw"][:, 2] * (d["freq"] / synth.C_LIGHT * sign)) * (2 * np.pi)
+    c = d["vis"].astype(np.complex128)
+    if d.get("wgt") is not None:
+        c = c * d["wgt"].astype(np.float64)
+    return c * np.exp(1j * p.o_center * w_eff)
 
 
 def to_dev(torch, a, dtype=None):
