@@ -82,6 +82,7 @@ SIGNATURES = {
     "cg_plan_destroy": (c_int, [c_void_p]),
     "cg_plan_copy_buffer": (c_int, [c_void_p, c_int, c_void_p, c_size_t, ctypes.POINTER(c_size_t)]),
     "cg_plan_set_stop_stage": (c_int, [c_void_p, c_int]),
+    "cg_plan_status": (c_int, [c_void_p]),
     "cg_plan_set_grid_budget": (c_int, [c_void_p, c_size_t]),
     "cg_plan_set_fixed_uvw": (c_int, [c_void_p, c_int]),
     "cg_plan_set_method": (c_int, [c_void_p, c_int]),

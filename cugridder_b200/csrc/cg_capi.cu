@@ -399,6 +399,13 @@ int cg_plan_dirty2ms(cg_plan* plan, int64_t nrow, double freq, const double* d_u
   return cg::dirty2ms_device(plan, nrow, freq, d_uvw, d_dirty, d_wgt, d_vis);
 }
 
+int cg_plan_status(cg_plan* plan) {
+  if (!plan) return CG_ERR_ARG;
+  std::lock_guard<std::mutex> lock(plan->mu);
+  CG_CUDA(cudaSetDevice(plan->device));
+  return cg::tma_status(plan);
+}
+
 int cg_plan_ms2dirty_chan(cg_plan* plan, int64_t nrow, int nchan, const double* freqs,
                           const double* d_uvw, const void* d_vis, const void* d_wgt,
                           void* d_dirty) {

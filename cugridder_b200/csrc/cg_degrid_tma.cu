@@ -15,7 +15,11 @@
 // start coordinate is >= 0 and the box lies inside the grid (interior tiles
 // only); the global strides are multiples of 16 bytes; the stages are
 // 1024-byte aligned.  Every wait on the stage barriers is bounded; a wait
-// that runs out sets *err and the CTA stops taking tiles.
+// that runs out sets *err and the CTA stops taking tiles, so the call's
+// visibilities are incomplete and the call reports the error.  The bound of
+// the stage waits is a launch argument: CG_TMA_STAGE_WAIT_TRIES (test only)
+// lowers it, down to 0 tries, which makes the first staged box's wait run
+// out; the drain of boxes still in flight always keeps the full bound.
 #include <cuda.h>
 
 #include <algorithm>
@@ -51,9 +55,10 @@ __device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes) {
                : "memory");
 }
 
-// bounded wait for phase `parity` of the barrier; false if it ran out
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
-  for (int i = 0; i < kWaitTries; i++) {
+// bounded wait (at most `tries` polls) for phase `parity` of the barrier;
+// false if it ran out
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, int tries = kWaitTries) {
+  for (int i = 0; i < tries; i++) {
     unsigned done;
     asm volatile(
         "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
@@ -83,7 +88,7 @@ __global__ void __launch_bounds__(NT, NS == 1 ? (NT <= 128 ? 3 : 2) : 1) k_degri
     const __grid_constant__ CUtensorMap map, const Rec<float>* __restrict__ recs,
     const int* __restrict__ perm, const int* __restrict__ hive_start, int64_t M, Geom g,
     TmaTile tc, const float2* __restrict__ fw, float* __restrict__ vis, int* __restrict__ counter,
-    int* __restrict__ err) {
+    int* __restrict__ err, int stage_tries) {
   extern __shared__ unsigned char smem_raw[];
   constexpr int lo = Halo<W>::lo;
   unsigned char* base =
@@ -192,7 +197,7 @@ __global__ void __launch_bounds__(NT, NS == 1 ? (NT <= 128 ? 3 : 2) : 1) k_degri
     // the current tile's box
     bool ok = true;
     if (cur_tma) {
-      ok = mbar_wait(smem_u32(&bars[s]), phase[s]);
+      ok = mbar_wait(smem_u32(&bars[s]), phase[s], stage_tries);
       if (ok) {
         phase[s] ^= 1u;
         pending[s] = false;
@@ -265,8 +270,9 @@ __global__ void __launch_bounds__(NT, NS == 1 ? (NT <= 128 ? 3 : 2) : 1) k_degri
       }
     }
   }
-  // after a timed-out wait boxes may still be in flight: wait for them
-  // (bounded) before the CTA's shared memory is released
+  // after a timed-out wait boxes may still be in flight: wait for them, with
+  // the full bound whatever stage_tries is, before the CTA's shared memory is
+  // released
   if (threadIdx.x == 0)
     for (int k = 0; k < 2; k++)
       if (pending[k]) mbar_wait(smem_u32(&bars[k]), phase[k]);
@@ -349,9 +355,12 @@ int launch_w(const Rec<float>* d_recs, const int* d_perm, const int* d_hive_star
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms = 148;
   }
   const int blocks = std::min(tc.nitems, per_sm * sms);
+  int stage_tries = kWaitTries;
+  if (const char* e = getenv("CG_TMA_STAGE_WAIT_TRIES")) stage_tries = std::max(0, std::min(atoi(e), kWaitTries));
   CG_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(int), st));
   k_degrid_tma<W, NT, NS><<<blocks, NT, smem, st>>>(map, d_recs, d_perm, d_hive_start, M, g, tc,
-                                                    (const float2*)d_fw, d_vis, d_counter, d_err);
+                                                    (const float2*)d_fw, d_vis, d_counter, d_err,
+                                                    stage_tries);
   count_launches(1);
   CG_CUDA(cudaGetLastError());
   return CG_OK;

@@ -121,6 +121,9 @@ int ms2dirty_split(cg_plan_s* P, int part, int64_t nrow, double freq, const doub
                    const void* d_vis, const void* d_wgt, void* d_dirty, bool* split);
 int dirty2ms_split(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw,
                    const void* d_dirty, const void* d_wgt, void* d_vis, bool* split);
+// Waits for the plan's stream and reports (and clears) a timed-out TMA
+// staging wait of the degridding: CG_ERR_CUDA, else CG_OK.
+int tma_status(cg_plan_s* P);
 }  // namespace cg
 
 #define CG_CUDA(call)                                  \

@@ -341,6 +341,41 @@ static int four_step_rows(const cg_plan_s* P, const Geom& g) {
   return four_step_supported(g.nf2, g.N1 / 2, g.N1 / 2) ? g.nf2 / 64 : 0;
 }
 
+int call_geometry(double fov, double freq, int sign, double sigma, int64_t nrow,
+                  const unsigned long long* h_mm, Geom& g) {
+  g.pixx = fov / 180.0 * kPi / (double)g.N2;
+  g.pixy = fov / 180.0 * kPi / (double)g.N1;
+  g.foc = freq / kSpeedOfLight;
+  g.sign = sign;
+  double wmin = 0, wmax = 0;
+  if (nrow > 0) {
+    const double rmin = decode_ordered(h_mm[4]), rmax = decode_ordered(h_mm[5]);
+    // same rounding chain as eff_coords(); monotone in w
+    auto scale = [&](double w) { return (w * (g.foc * (double)g.sign)) * (2 * kPi); };
+    const double a = scale(rmin), b = scale(rmax);
+    wmin = std::min(a, b);
+    wmax = std::max(a, b);
+  }
+  const double l_min = 0 - 0.5 * g.pixx * g.N2;
+  const double m_min = 0 - 0.5 * g.pixy * g.N1;
+  const double temp = 1.0 - std::pow(l_min, 2) - std::pow(m_min, 2);
+  const double n_lm = temp <= 0 ? 0 : std::sqrt(temp);
+  g.i_center = (wmax + wmin) / 2.0;
+  g.i_half_width = (wmax - wmin) / 2.0;
+  const double o_min = n_lm - 1;
+  g.o_center = o_min / 2.0;
+  g.o_half_width = std::fabs(o_min / 2.0);
+  set_nhg_w(g.o_half_width, g.i_half_width, g.kw, sigma, g.nw, g.h, g.gamma);
+  if (g.nw > 65535) {
+    set_last_error("number of w planes too large");
+    return CG_ERR_SIZE;
+  }
+  g.nhx = (g.nf1 - 1) / 8 + 1;
+  g.nhy = (g.nf2 - 1) / 8 + 1;
+  g.nhz = g.nw;
+  return CG_OK;
+}
+
 static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw) {
   if (nrow < 0 || nrow > 2147483647LL) {
     set_last_error("nrow out of range");
@@ -360,6 +395,8 @@ static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw)
   CG_CUDA(cudaStreamSynchronize(st));
   timer_flush(P, P->timer.cur ^ 1);
   if (P->tma_armed && ((const int*)P->h_mm)[18]) {  // word 72: a TMA staging wait ran out
+    // only a call captured into a CUDA graph (or one whose status was not
+    // read) leaves the word set: non-captured calls report it themselves
     CG_CUDA(cudaMemsetAsync((char*)P->mm.p + 72, 0, sizeof(int), st));
     set_last_error("degridding: a TMA staging wait timed out in an earlier call");
     return CG_ERR_CUDA;
@@ -376,39 +413,10 @@ static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw)
   g.kw = P->kw;
   g.beta = P->beta;
   g.es_c = P->es_c;
-  g.pixx = P->fov / 180.0 * kPi / (double)g.N2;
-  g.pixy = P->fov / 180.0 * kPi / (double)g.N1;
-  g.foc = freq / kSpeedOfLight;
-  g.sign = P->sign;
   const bool poly = P->kernel_kind == CG_KERNEL_POLY;
   g.polyf = poly ? (const float*)P->polyf.p : nullptr;
   g.polyd = poly ? (const double*)P->polyd.p : nullptr;
-  double wmin = 0, wmax = 0;
-  if (nrow > 0) {
-    double rmin = decode_ordered(P->h_mm[4]), rmax = decode_ordered(P->h_mm[5]);
-    // same rounding chain as eff_coords(); monotone in w
-    auto scale = [&](double w) { return (w * (g.foc * (double)g.sign)) * (2 * kPi); };
-    double a = scale(rmin), b = scale(rmax);
-    wmin = std::min(a, b);
-    wmax = std::max(a, b);
-  }
-  double l_min = 0 - 0.5 * g.pixx * g.N2;
-  double m_min = 0 - 0.5 * g.pixy * g.N1;
-  double temp = 1.0 - std::pow(l_min, 2) - std::pow(m_min, 2);
-  double n_lm = temp <= 0 ? 0 : std::sqrt(temp);
-  g.i_center = (wmax + wmin) / 2.0;
-  g.i_half_width = (wmax - wmin) / 2.0;
-  double o_min = n_lm - 1;
-  g.o_center = o_min / 2.0;
-  g.o_half_width = std::fabs(o_min / 2.0);
-  set_nhg_w(g.o_half_width, g.i_half_width, g.kw, P->sigma, g.nw, g.h, g.gamma);
-  if (g.nw > 65535) {
-    set_last_error("number of w planes too large");
-    return CG_ERR_SIZE;
-  }
-  g.nhx = (g.nf1 - 1) / 8 + 1;
-  g.nhy = (g.nf2 - 1) / 8 + 1;
-  g.nhz = g.nw;
+  CG_TRY(call_geometry(P->fov, freq, P->sign, P->sigma, nrow, P->h_mm, g));
   // band of grid rows (g1 <- u) / columns (g0 <- v) reached by the taps: the
   // grid coordinate is monotone in u (v) while the scaled value stays inside
   // [-pi, pi); otherwise the data wraps and the band is the whole axis.
@@ -895,6 +903,23 @@ static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const
   return CG_OK;
 }
 
+// Status of the TMA-staged degridding launched on the plan's stream: waits
+// for the stream, reads and clears the error word.  CG_ERR_CUDA when a
+// staging wait ran out (that call's visibilities are incomplete).
+int tma_status(cg_plan_s* P) {
+  if (!P->tma_armed) return CG_OK;
+  CG_CUDA(cudaMemcpyAsync(P->h_mm + 9, tma_error_word(P), sizeof(int), cudaMemcpyDeviceToHost,
+                          P->stream));
+  CG_CUDA(cudaStreamSynchronize(P->stream));
+  if (*(const int*)(P->h_mm + 9)) {
+    CG_CUDA(cudaMemsetAsync(tma_error_word(P), 0, sizeof(int), P->stream));
+    CG_CUDA(cudaStreamSynchronize(P->stream));
+    set_last_error("degridding: a TMA staging wait timed out; the visibilities are incomplete");
+    return CG_ERR_CUDA;
+  }
+  return CG_OK;
+}
+
 // fixed-uvw mode: the last call's geometry and binning still describe this one
 static bool reuse_geometry(const cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw) {
   return P->fixed_uvw && P->bins_valid && !P->timer.on && P->stop_stage == 0 &&
@@ -966,6 +991,13 @@ static int dirty2ms_run(cg_plan_s* P, int part, int64_t nrow, double freq, const
                ? dirty2ms_t<double>(P, d_uvw, (const double*)d_dirty, (const double*)d_wgt, (double*)d_vis, reuse, part)
                : dirty2ms_t<float>(P, d_uvw, (const float*)d_dirty, (const float*)d_wgt, (float*)d_vis, reuse, part);
   if (st == CG_OK) remember_geometry(P, nrow, freq, d_uvw);
+  // a call that is not being captured reports a timed-out TMA staging wait
+  // itself (one more stream synchronization, only when the TMA kernel ran)
+  if (st == CG_OK && part == 0 && P->tma_armed) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CG_CUDA(cudaStreamIsCapturing(P->stream, &cs));
+    if (cs == cudaStreamCaptureStatusNone) st = tma_status(P);
+  }
   return st != CG_OK ? st : P->eps_status;
 }
 

@@ -108,6 +108,14 @@ namespace cg {
 int setup_conv_opts(double eps, double sigma, double eps_floor, int& kw, double& beta, double& c);
 int get_num_cells(int ms, double sigma, int kw);
 void set_nhg_w(double S, double X, int kw, double sigma, int& nf, double& h, double& gam);
+// Geometry of one call (setup_gridder_plan, cugridder.cu:29-86): fills g's
+// pixel sizes, f/c, sign, the w range's centre and half width (from the
+// range words h_mm[4..5] of launch_wminmax; zero width when nrow == 0), o_c,
+// the w planes (set_nhg_w) and the hive counts.  g.N1, N2, nf1, nf2, kw,
+// beta and es_c must be set.  Shared by the plan path and the allocation-free
+// binning, so that both key the same rows alike.
+int call_geometry(double fov, double freq, int sign, double sigma, int64_t nrow,
+                  const unsigned long long* h_mm, Geom& g);
 void make_quad(int kw, double beta, double c, const double* poly, Quad& q);
 void fseries_uv(const Quad& q, int nf, double* out);
 int plan_configure(cg_plan_s* P, int nx, int ny, double fov, double eps, double sigma, int sign,

@@ -113,10 +113,6 @@ int cg_bin_static(int64_t nrow, int nxdirty, int nydirty, double fov, double fre
   g.kw = kw;
   g.beta = beta;
   g.es_c = c;
-  g.pixx = fov / 180.0 * kPi / (double)g.N2;
-  g.pixy = fov / 180.0 * kPi / (double)g.N1;
-  g.foc = freq / kSpeedOfLight;
-  g.sign = sign;
 
   unsigned long long* d_mm = (unsigned long long*)scratch;
   int* d_bad = (int*)(d_mm + 6);
@@ -128,28 +124,7 @@ int cg_bin_static(int64_t nrow, int nxdirty, int nydirty, double fov, double fre
     set_last_error("non-finite uvw coordinate");
     return CG_ERR_ARG;
   }
-  double wmin = 0, wmax = 0;
-  if (nrow > 0) {
-    auto scale = [&](double w) { return (w * (g.foc * (double)g.sign)) * (2 * kPi); };
-    const double a = scale(decode_ordered(h_mm[4])), b = scale(decode_ordered(h_mm[5]));
-    wmin = std::min(a, b);
-    wmax = std::max(a, b);
-  }
-  const double l_min = 0 - 0.5 * g.pixx * g.N2, m_min = 0 - 0.5 * g.pixy * g.N1;
-  const double temp = 1.0 - std::pow(l_min, 2) - std::pow(m_min, 2);
-  const double n_lm = temp <= 0 ? 0 : std::sqrt(temp);
-  g.i_center = (wmax + wmin) / 2.0;
-  g.i_half_width = (wmax - wmin) / 2.0;
-  g.o_center = (n_lm - 1) / 2.0;
-  g.o_half_width = std::fabs((n_lm - 1) / 2.0);
-  set_nhg_w(g.o_half_width, g.i_half_width, g.kw, sigma, g.nw, g.h, g.gamma);
-  if (g.nw > 65535) {
-    set_last_error("number of w planes too large");
-    return CG_ERR_SIZE;
-  }
-  g.nhx = (g.nf1 - 1) / 8 + 1;
-  g.nhy = (g.nf2 - 1) / 8 + 1;
-  g.nhz = g.nw;
+  CG_TRY(call_geometry(fov, freq, sign, sigma, nrow, h_mm, g));
   const int64_t nh = (int64_t)g.nhx * g.nhy * g.nhz;
   if (n_hives) *n_hives = nh;
   if (!d_hive_start || hive_start_len < nh + 1) {

@@ -117,6 +117,11 @@ class Plan:
     def set_stop_stage(self, stage):
         _lib.check(self._lib.cg_plan_set_stop_stage(self._h, int(stage)))
 
+    def check_status(self):
+        """Wait for the plan's stream; raise GridderError if a bounded TMA
+        staging wait of the degridding ran out since the last check."""
+        return _lib.check(self._lib.cg_plan_status(self._h))
+
     def copy_buffer(self, which):
         """Copy an internal buffer (CG_BUF_*) of the last call to a numpy array."""
         need = ctypes.c_size_t()

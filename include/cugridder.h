@@ -227,6 +227,17 @@ int cg_plan_get_tiling(const cg_plan *plan, int *tiling, float *tuned_ms);
  * 3 = after the FFT. */
 int cg_plan_set_stop_stage(cg_plan *plan, int stage);
 
+/* Status of the plan's asynchronous work (no reference counterpart: the
+ * reference synchronizes after every kernel and exit()s on errors,
+ * include/utils.h:18-27).  Waits for the plan's stream, then returns
+ * CG_ERR_CUDA (message in cg_last_error) if a bounded staging wait of the
+ * TMA degridding ran out since the last check, which leaves that call's
+ * visibilities incomplete, and clears the condition; else CG_OK.  A
+ * dirty2ms call that is not being captured into a CUDA graph runs this
+ * check itself before it returns; a captured call's condition is reported
+ * by this function or by the plan's next call. */
+int cg_plan_status(cg_plan *plan);
+
 /* Per-stage CUDA-event timers of a plan (profiling; off by default).
  * Stages of ms2dirty: 0 w range, 1 quarter tables, 2 binning, 3 sorted
  * stream, 4 gridding, 5 FFT, 6 w-DFT + corrections.  Stages of dirty2ms:

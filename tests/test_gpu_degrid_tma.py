@@ -74,3 +74,55 @@ def test_tma_degridding_non_square(torch_cuda, nx, ny):
     b, _ = _dirty2ms(torch_cuda, d, img, 1e-5, 0)
     for x in a:
         assert rel_l2(x, b[0]) < 1e-6
+
+
+@pytest.mark.parametrize("variant", [1, 2])
+def test_tma_stage_wait_timeout_is_reported_by_the_call(torch_cuda, variant):
+    """A staging wait that runs out fails THAT call with CG_ERR_CUDA.
+
+    CG_TMA_STAGE_WAIT_TRIES=0 (a test-only bound) makes the wait for every
+    CTA's first staged box give up at once; the CTA stops taking tiles, and
+    the drain of its boxes still in flight keeps the full bound, so no copy
+    is pending when it exits.  The plan API and the host API both return the
+    error from the call that hit it; the next call on the same plan is clean
+    and correct, and cg_plan_status then reports nothing."""
+    from cugridder_b200 import _lib, dirty2ms_mixed, release_cache
+
+    N = 1024
+    d = synth.make("wstack_2048_10M", seed=77, nrow=200_000, nx=N, ny=N, fov=1.0)
+    img = synth.random_image(N, N, seed=78, dtype=np.complex64)
+    ref, _ = _dirty2ms(torch_cuda, d, img, 1e-5, 0, calls=1)
+    os.environ["CG_DEGRID_TMA"] = str(variant)
+    try:
+        p = Plan(N, N, d["fov"], 1e-5, precision="fp32")
+    finally:
+        del os.environ["CG_DEGRID_TMA"]
+    uvw = to_dev(torch_cuda, d["uvw"], np.float64)
+    wgt = to_dev(torch_cuda, d["wgt"], np.float32)
+    dimg = to_dev(torch_cuda, img, np.complex64)
+    vis = torch_cuda.zeros(d["uvw"].shape[0], dtype=torch_cuda.complex64, device="cuda")
+    os.environ["CG_TMA_STAGE_WAIT_TRIES"] = "0"
+    try:
+        with pytest.raises(_lib.GridderError) as ex:
+            p.dirty2ms(uvw, d["freq"], dimg, wgt, vis)
+    finally:
+        del os.environ["CG_TMA_STAGE_WAIT_TRIES"]
+    assert ex.value.code == 3 and "timed out" in str(ex.value)
+    vis.zero_()
+    assert p.dirty2ms(uvw, d["freq"], dimg, wgt, vis) == 0
+    torch_cuda.cuda.synchronize()
+    assert rel_l2(vis.cpu().numpy(), ref[0]) < 1e-6
+    assert p.check_status() == 0
+    p.close()
+    # host-pointer API (its cached plan runs the default TMA variant 2)
+    if variant == 2:
+        release_cache()
+        os.environ["CG_TMA_STAGE_WAIT_TRIES"] = "0"
+        try:
+            with pytest.raises(_lib.GridderError) as ex:
+                dirty2ms_mixed(d["uvw"], d["freq"], img, d["wgt"], d["fov"], 1e-5)
+        finally:
+            del os.environ["CG_TMA_STAGE_WAIT_TRIES"]
+        assert ex.value.code == 3
+        v = dirty2ms_mixed(d["uvw"], d["freq"], img, d["wgt"], d["fov"], 1e-5)
+        assert rel_l2(v, ref[0]) < 1e-6

@@ -19,11 +19,13 @@ pytestmark = pytest.mark.gpu
 CG_ERR_SIZE = 6
 
 
-def _plan_binning(torch, d, precision, eps, sign):
+def _plan_binning(torch, d, precision, eps, sign, grid_budget=0):
     cdt = np.complex128 if precision == "fp64" else np.complex64
     rdt = np.float64 if precision == "fp64" else np.float32
     plan = Plan(d["nx"], d["ny"], d["fov"], eps, sign=sign, precision=precision)
     try:
+        if grid_budget:
+            plan.set_grid_budget(grid_budget)
         uvw = torch.from_numpy(d["uvw"]).cuda()
         vis = torch.from_numpy(d["vis"].astype(cdt)).cuda()
         wgt = torch.from_numpy(d["wgt"].astype(rdt)).cuda()
@@ -73,6 +75,29 @@ def test_static_binning_matches_plan_two_calls(torch_cuda, precision, eps, sign)
         np.testing.assert_array_equal(h, h_ref)
         assert h[-1] == d["uvw"].shape[0]
         assert np.array_equal(np.sort(p), np.arange(d["uvw"].shape[0], dtype=np.int32))
+
+
+def test_static_binning_eight_byte_keys_at_cap(torch_cuda, oracle):
+    """nhx * nhy * nw * 64 > 2^32 (4096^2 image, w up to 20 km: 84 planes of
+    1024^2 hives), so both paths sort 64-bit cell keys; at the row cap that
+    layout fills most of the 15 MiB array.  Bit for bit against the plan path
+    (whose grid is held to a 2 GiB budget of planes: binning only)."""
+    torch = torch_cuda
+    lib = _lib.load()
+    cap = lib.cg_bin_static_max_rows()
+    d = synth.make("wstack_4096_20M", seed=13, nrow=cap, w_max=20000.0)
+    p = oracle.setup(d["uvw"], d["nx"], d["ny"], d["fov"], d["freq"], 1e-5, eps_floor=6e-8)
+    nh = p.nhive[0] * p.nhive[1] * p.nhive[2]
+    assert nh * 64 > 2 ** 32
+    keys = oracle.bin_keys(p, d["uvw"])
+    assert keys.max() >= 2 ** 32  # rows whose keys need the upper word
+    p_ref, h_ref = _plan_binning(torch, d, "fp32", 1e-5, -1, grid_budget=2 << 30)
+    for _ in range(2):
+        perm, hs = _static_binning(torch, lib, d, "fp32", 1e-5, -1)
+        np.testing.assert_array_equal(perm, p_ref)
+        np.testing.assert_array_equal(hs, h_ref)
+    assert hs.size == nh + 1 and hs[-1] == cap
+    np.testing.assert_array_equal(perm, np.argsort(keys, kind="stable"))
 
 
 def test_static_binning_rejects_oversize(torch_cuda):
