@@ -8,4 +8,4 @@ piecewise degree-7 Horner polynomials that the gridder evaluates
     plan.set_kernel("poly", k.W, k.horner)
 """
 from .model import (H, NTHETA, LearnedKernel, available_widths, es_horner, horner_fit,  # noqa: F401
-                    init_theta, kernel_path, load_kernel, phi_np)
+                    init_theta, kernel_path, load_kernel, phi_np, smallest_width)

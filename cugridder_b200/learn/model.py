@@ -153,3 +153,19 @@ def available_widths(directory=None):
 def load_kernel(W, directory=None):
     with open(kernel_path(W, directory)) as f:
         return LearnedKernel.from_json(json.load(f))
+
+
+def smallest_width(eps, directory=None):
+    """The learned kernel at the smallest width that met eps in the committed
+    width search (kernels/wsearch_2048_10M.json), or None when none did."""
+    import json
+
+    p = os.path.join(directory or KERNEL_DIR, "wsearch_2048_10M.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        best = json.load(f).get("smallest_W", {})
+    W = (best.get("%g" % eps) or {}).get("learned")
+    if W is None or W not in available_widths(directory):
+        return None
+    return load_kernel(W, directory)

@@ -9,6 +9,10 @@
 #
 #   make -f oracle/ref.mk -j8          (from the repo root)
 #
+# It also builds oracle/_ref/libref_bins.so from oracle/ref_bins.cu (test code
+# of this repository) against that library: the reference's binning stage
+# with its hive offsets and per-cell counts read back.
+#
 # Flags follow the reference's own build line (Makefile:15-16): -O3,
 # --default-stream per-thread, -use_fast_math, relocatable device code, FP64
 # objects plus FP32 objects built with -DSINGLE.  -lnvToolsExt is dropped
@@ -35,7 +39,7 @@ OBJ_COMMON := $(OUT)/obj/$(call flat,$(SRC_COMMON_CU)).o $(OUT)/obj/$(call flat,
 OBJ_64 := $(foreach s,$(SRC_PREC),$(OUT)/obj/$(call flat,$(s)).o)
 OBJ_32 := $(foreach s,$(SRC_PREC),$(OUT)/obj/$(call flat,$(s))_32.o)
 
-all: $(OUT)/libcurafft_ref.so
+all: $(OUT)/libcurafft_ref.so $(OUT)/libref_bins.so
 
 $(OUT)/obj:
 	mkdir -p $@
@@ -56,6 +60,12 @@ $(OUT)/obj/$(call flat,$(SRC_COMMON_C)).o: $(REF)/$(SRC_COMMON_C) | $(OUT)/obj
 
 $(OUT)/libcurafft_ref.so: $(OBJ_COMMON) $(OBJ_64) $(OBJ_32)
 	$(NVCC) -shared $(NVFLAGS) $^ -o $@ -lm -lcudart -lcufft
+
+# the binning harness (oracle/ref_bins.cu, this repository's test code) calls
+# the FP64 reference functions of libcurafft_ref.so through their own headers
+$(OUT)/libref_bins.so: oracle/ref_bins.cu $(OUT)/libcurafft_ref.so
+	$(NVCC) -shared $(NVFLAGS) $(INC) $< -o $@ -L$(OUT) -lcurafft_ref -lcudart \
+	    -Xlinker -rpath,'$$ORIGIN'
 
 clean:
 	rm -rf $(OUT)
