@@ -58,6 +58,14 @@ def parse():
                          "committed width search, else ES")
     ap.add_argument("--accuracy-samples", type=int, default=256,
                     help="pixels / rows checked against the FP64 direct sums (0: skip)")
+    ap.add_argument("--eps-fp64-leg", type=float, default=1e-9,
+                    help="epsilon of the workload's FP64 leg, timed beside the main line (0: skip)")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched workload's forms in the main line")
+    ap.add_argument("--ref-reps", type=int, default=3,
+                    help="timed calls of the reference's CUDA build (--impl reference)")
+    ap.add_argument("--_ref-cuda-worker", dest="ref_cuda_worker", action="store_true",
+                    help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -212,6 +220,20 @@ def ncu_traffic(kernel, workload):
 
 
 # --------------------------------------------------------------------------- workload
+def workload_config(args, world):
+    """The workload's defining parameters: the same dict in both arms'
+    lines (implementation details are reported under "impl_detail")."""
+    from cugridder_b200 import synth
+
+    cfg = synth.CONFIGS[args.config]
+    return {"workload": args.config, "nx": cfg["nx"], "ny": cfg["ny"],
+            "fov_deg": args.fov or cfg["fov"], "nrow_per_gpu": args.nrow or cfg["nrow"],
+            "freq_hz": cfg["freq"], "eps": args.eps, "sigma": 2.0, "sign": -1,
+            "uv_sigma_m": cfg["uv_sigma"], "uv_clip_m": cfg["uv_clip"], "w_max_m": cfg["w_max"],
+            "parallelism": "independent datasets per GPU" if world > 1 else "single GPU",
+            "l2": "inputs larger than L2 (uvw 480 MB, grid 7.5 GB)"}
+
+
 def make_data(cfg_name, seed, nrow, torch, fov=None):
     from cugridder_b200 import synth
 
@@ -376,12 +398,44 @@ def run_b200(args, rank, world, local):
         res["fp64_plain"] = {"value": round(v64, 2), "ms_per_step": round(t64 / max(2, args.steps // 3), 3),
                              "eps": args.eps, "kw": fp["info"]["kw"], "nw": fp["info"]["nw"]}
         res["fp32_over_fp64"] = round(res["value"] / v64, 3)
+        if args.eps_fp64_leg > 0:
+            # the workload's FP64 leg at its own epsilon (1e-9: W = 10)
+            n9 = max(2, args.steps // 5)
+            eps_main, args.eps = args.eps, args.eps_fp64_leg
+            try:
+                f9 = timed_run("fp64", n9, max(1, args.warmup - 1))
+            finally:
+                args.eps = eps_main
+            t9 = max_over_ranks(f9["ms"], world)
+            res["fp64_eps_leg"] = {"eps": args.eps_fp64_leg, "value": round(total_rows * n9 / (t9 / 1e3) / 1e6, 2),
+                                   "ms_per_step": round(t9 / n9, 3), "kw": f9["info"]["kw"],
+                                   "nw": f9["info"]["nw"], "adjointness": f9["adjointness"],
+                                   "steps": n9}
+            if nsamp:
+                res["fp64_eps_leg"]["accuracy"] = accuracy(d, img, pix, rows, f9, None)["value_form"]
 
     if nsamp:
         res["accuracy"] = accuracy(d, img, pix, rows, main, fp if not args.no_fp64 else None)
 
     if not args.no_e2e:
         res["e2e"] = run_e2e(args, d, img, world, kern)
+
+    if not args.no_batched and world == 1:
+        # the batched workload: learned FP32 against plain ES FP64, both batched
+        del uvw
+        torch.cuda.empty_cache()
+        eps_main, args.eps = args.eps, 1e-4
+        try:
+            bk = select_kernel(args)
+            forms, meta, _ = batched_forms(args, bk, max(3, args.steps // 2), args.warmup,
+                                           sequential=False)
+        finally:
+            args.eps = eps_main
+        res["batched"] = {"config": meta, "learned_fp32": forms["learned_fp32"]["value"],
+                          "es_fp32": forms["es_fp32"]["value"], "es_fp64": forms["es_fp64"]["value"],
+                          "learned_fp32_over_es_fp64": round(forms["learned_fp32"]["value"] /
+                                                             forms["es_fp64"]["value"], 3),
+                          "forms": forms}
     return res
 
 
@@ -478,75 +532,195 @@ def run_e2e(args, d, img, world, kern):
 
 
 # --------------------------------------------------------------------------- CPU (oracle port)
-def cpu_reference_rate(cfg_name, nsample=200_000, seed=0):
-    """Mvis/s of the reference algorithm restated on the host cores, for the
-    full workload, assembled from measured parts: per-row gridding and
-    degridding cost (nsample rows, same kernel width), one full-size 2-D FFT
-    plane per direction (times nw), and the per-pixel w stage / corrections
-    (measured on a 256x256 image, scaled to the workload's pixels)."""
-    from cugridder_b200 import synth
-    from oracle import oracle as O
+class CpuReference:
+    """Mvis/s of the reference algorithm restated on the host cores (the
+    oracle's C/OpenMP port, all threads) for the full workload, EXTRAPOLATED
+    from measured parts:
+      - gridding and degridding of a sample of rows on the workload's
+        full-size grid (same nf, nw, W, so cache behaviour is the real one),
+        per row, times the workload's rows, plus one zeroing of the grid;
+      - one full-size 2-D FFT plane, times nw, per direction;
+      - the per-pixel w stage and corrections of a 256^2 run, times the
+        workload's pixels, per direction.
+    The fixed-cost parts are measured once; each sample() times new rows."""
 
-    full = synth.CONFIGS[cfg_name]
-    d = synth.make(cfg_name, seed=seed, nrow=nsample)
-    p = O.setup(np.array([[0, 0, -full["w_max"]], [0, 0, full["w_max"]]], float), full["nx"],
-                full["ny"], full["fov"], full["freq"], 1e-5)
-    # gridding / degridding per row, on a small grid with the same W
-    ps = O.setup(d["uvw"], 256, 256, 2.0, full["freq"], 1e-5)
-    X = O.grid_coords(ps, d["uvw"])
-    c = d["vis"].astype(np.complex128)
-    t0 = time.perf_counter()
-    fw = O.grid(ps, X, c)
-    t1 = time.perf_counter()
-    O.degrid(ps, X, fw)
-    t2 = time.perf_counter()
-    t_grid, t_degrid = (t1 - t0) / nsample, (t2 - t1) / nsample
-    # one full-size plane FFT per direction
-    pf = O.Params()
-    ctypes_fields = O.setup(np.zeros((1, 3)), full["nx"], full["ny"], full["fov"], full["freq"], 1e-5)
-    for name, _ in O.Params._fields_:
-        setattr(pf, name, getattr(ctypes_fields, name))
-    pf.nf3 = 1
-    plane = np.zeros((1, pf.nf2, pf.nf1), np.complex128)
-    plane[0, :64, :64] = 1.0
-    t0 = time.perf_counter()
-    O.fft2_planes(pf, plane, +1)
-    t1 = time.perf_counter()
-    t_fft_plane = (t1 - t0)
-    # w stage + corrections per pixel: a 256^2 run minus its gridding and FFT
-    small = synth.make("ms2dirty_256_fp64", seed=seed, nrow=2000)
-    t0 = time.perf_counter()
-    O.ms2dirty(small["uvw"], small["vis"], small["wgt"], 256, 256, 2.0, 1e8, 1e-5)
-    t1 = time.perf_counter()
-    psm = O.setup(small["uvw"], 256, 256, 2.0, 1e8, 1e-5)
-    t_small_fft = t_fft_plane * (psm.nf1 * psm.nf2) / (pf.nf1 * pf.nf2) * psm.nf3
-    t_pix = max((t1 - t0) - t_small_fft - 2000 * t_grid, 0.0) / (256 * 256)
-    M = full["nrow"]
-    npix = full["nx"] * full["ny"]
-    t_total = M * (t_grid + t_degrid) + 2 * p.nf3 * t_fft_plane + 2 * npix * t_pix
-    return {
-        "value": round(M / t_total / 1e6, 6), "unit": "Mvis/s", "cores": O.num_threads(),
-        "kind": "port",
-        "sample": ("oracle (C/OpenMP restatement of the reference pipeline): gridding+degridding "
-                   "timed on %d rows (W=%d), one %dx%d FFT plane per direction x nw=%d, w stage "
-                   "per pixel from a 256^2 run; assembled for %d rows on %dx%d"
-                   % (nsample, p.kw, pf.nf1, pf.nf2, p.nf3, M, full["nx"], full["ny"])),
-        "seconds_for_full_workload": round(t_total, 1),
-    }
+    def __init__(self, cfg_name):
+        from cugridder_b200 import synth
+        from oracle import oracle as O
+
+        self.O = O
+        self.cfg_name = cfg_name
+        full = self.full = synth.CONFIGS[cfg_name]
+        # geometry of the full workload (its w range is +-w_max)
+        self.p = O.setup(np.array([[0, 0, -full["w_max"]], [0, 0, full["w_max"]]], float),
+                         full["nx"], full["ny"], full["fov"], full["freq"], 1e-5)
+        p = self.p
+        self.fw = np.empty((p.nf3, p.nf2, p.nf1), dtype=np.complex128)
+        p0 = type(p).from_buffer_copy(p)
+        p0.nrow = 0
+        none = np.zeros((3, 0))
+        O.grid(p0, none, np.zeros(0, np.complex128), out=self.fw)  # first touch of the pages
+        t0 = time.perf_counter()
+        O.grid(p0, none, np.zeros(0, np.complex128), out=self.fw)
+        self.t_zero = time.perf_counter() - t0
+        # one full-size FFT plane
+        pf = type(p).from_buffer_copy(p)
+        pf.nf3 = 1
+        plane = self.fw[0:1]
+        t0 = time.perf_counter()
+        O.fft2_planes(pf, plane, +1)
+        self.t_fft_plane = time.perf_counter() - t0
+        # w stage + corrections per pixel: a 256^2 run minus its gridding and FFT
+        small = synth.make("ms2dirty_256_fp64", seed=0, nrow=2000)
+        psm = O.setup(small["uvw"], 256, 256, 2.0, 1e8, 1e-5)
+        Xs = O.grid_coords(psm, small["uvw"])
+        t0 = time.perf_counter()
+        O.grid(psm, Xs, small["vis"])
+        t_small_grid = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        O.ms2dirty(small["uvw"], small["vis"], small["wgt"], 256, 256, 2.0, 1e8, 1e-5)
+        t1 = time.perf_counter()
+        t_small_fft = self.t_fft_plane * (psm.nf1 * psm.nf2) / (p.nf1 * p.nf2) * psm.nf3
+        self.t_pix = max((t1 - t0) - t_small_fft - t_small_grid, 0.0) / (256 * 256)
+
+    def sample(self, nsample, seed):
+        from cugridder_b200 import synth
+
+        O, p, full = self.O, self.p, self.full
+        d = synth.make(self.cfg_name, seed=seed, nrow=nsample)
+        ps = type(p).from_buffer_copy(p)
+        ps.nrow = nsample
+        X = O.grid_coords(ps, d["uvw"])
+        c = d["vis"].astype(np.complex128)
+        t0 = time.perf_counter()
+        O.grid(ps, X, c, out=self.fw)
+        t1 = time.perf_counter()
+        O.degrid(ps, X, self.fw)
+        t2 = time.perf_counter()
+        t_grid = max(t1 - t0 - self.t_zero, 0.0) / nsample
+        t_degrid = (t2 - t1) / nsample
+        M = full["nrow"]
+        npix = full["nx"] * full["ny"]
+        t_total = (self.t_zero + M * (t_grid + t_degrid) + 2 * p.nf3 * self.t_fft_plane
+                   + 2 * npix * self.t_pix)
+        return {
+            "value": round(M / t_total / 1e6, 6), "unit": "Mvis/s", "cores": O.num_threads(),
+            "kind": "port",
+            "sample": ("EXTRAPOLATED, not a full run: the oracle (C/OpenMP restatement of the "
+                       "reference pipeline) gridded and degridded %d rows (W=%d) on the full "
+                       "%dx%dx%d grid, one %dx%d FFT plane per direction x nw=%d, the w stage "
+                       "per pixel from a 256^2 run; assembled for %d rows on %dx%d"
+                       % (nsample, p.kw, p.nf1, p.nf2, p.nf3, p.nf1, p.nf2, p.nf3, M, full["nx"],
+                          full["ny"])),
+            "seconds_for_full_workload": round(t_total, 1),
+        }
+
+
+def cpu_reference_rate(cfg_name, nsample=200_000, seed=0):
+    return CpuReference(cfg_name).sample(nsample, seed)
+
+
+def reference_cuda_worker(args):
+    """Child process of --impl reference: time the reference's own CUDA build
+    (oracle/_ref/libcurafft_ref.so, its sources compiled for sm_100a by
+    oracle/ref.mk) through its own host API -- ms2dirty_2 / dirty2ms_2 (FP64
+    build) and ms2dirtyf_2 / dirty2msf_2 (FP32 build, FP32 coordinates) -- on
+    the main line's data (seed 0).  Its API takes host buffers and returns
+    when the result is back, so each call is timed by the host clock; median
+    of `reps` calls after one warm-up call.  Prints one JSON line."""
+    import ctypes
+
+    from cugridder_b200 import synth
+
+    lib = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libcurafft_ref.so"))
+    P, D, F, I = ctypes.c_void_p, ctypes.c_double, ctypes.c_float, ctypes.c_int
+    fns = {}
+    for name, real in (("ms2dirty_2", D), ("dirty2ms_2", D), ("ms2dirtyf_2", F), ("dirty2msf_2", F)):
+        f = getattr(lib, name)
+        f.argtypes = [I, I, I, real, real, P, P, P, P, real, real, I]
+        f.restype = I
+        fns[name] = f
+    d = synth.make(args.config, seed=0, nrow=args.nrow)
+    img = synth.random_image(d["nx"], d["ny"], seed=1000, dtype=np.complex64)
+    M = d["uvw"].shape[0]
+    out = {}
+    clocks = ClockSampler(0)
+    clocks.start()
+    for prec in ("fp32", "fp64"):
+        single = prec == "fp32"
+        rt, ct = (np.float32, np.complex64) if single else (np.float64, np.complex128)
+        uvw = np.ascontiguousarray(d["uvw"], dtype=rt)
+        vis = np.ascontiguousarray(d["vis"], dtype=ct)
+        wgt = np.ascontiguousarray(d["wgt"], dtype=rt)
+        dimg = np.ascontiguousarray(img, dtype=ct)
+        dirty = np.zeros((d["nx"], d["ny"]), dtype=ct)
+        vout = np.zeros(M, dtype=ct)
+        sfx = "f" if single else ""
+        t_m, t_d, st = [], [], []
+        for r in range(args.ref_reps + 1):
+            t0 = time.perf_counter()
+            s1 = fns["ms2dirty%s_2" % sfx](M, d["nx"], d["ny"], d["fov"], d["freq"], uvw.ctypes.data,
+                                           vis.ctypes.data, wgt.ctypes.data, dirty.ctypes.data,
+                                           args.eps, 2.0, -1)
+            t1 = time.perf_counter()
+            s2 = fns["dirty2ms%s_2" % sfx](M, d["nx"], d["ny"], d["fov"], d["freq"], uvw.ctypes.data,
+                                           vout.ctypes.data, wgt.ctypes.data, dimg.ctypes.data,
+                                           args.eps, 2.0, -1)
+            t2 = time.perf_counter()
+            st.append([int(s1), int(s2)])
+            if r > 0:
+                t_m.append(t1 - t0)
+                t_d.append(t2 - t1)
+        m, dd = statistics.median(t_m), statistics.median(t_d)
+        out[prec] = {"value": round(M / (m + dd) / 1e6, 3), "unit": "Mvis/s",
+                     "ms2dirty_s": round(m, 4), "dirty2ms_s": round(dd, 4), "reps": args.ref_reps,
+                     "status": st[-1],
+                     "api": "ms2dirty%s_2 + dirty2ms%s_2 (host buffers)" % (sfx, sfx)}
+    clocks.stop()
+    out["eps"] = args.eps
+    out["timing"] = "host clock around each synchronous call; median after one warm-up call"
+    out["clocks"] = clocks.summary()
+    print(json.dumps(out), flush=True)
+
+
+def reference_cuda(args):
+    """reference_cuda key of --impl reference (see reference_cuda_worker)."""
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libcurafft_ref.so")):
+        return {"unavailable": "oracle/_ref/libcurafft_ref.so is not built here (build() builds it "
+                               "where the reference sources are present)"}
+    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--_ref-cuda-worker",
+           "--config", args.config, "--eps", str(args.eps), "--ref-reps", str(args.ref_reps)]
+    if args.nrow:
+        cmd += ["--nrow", str(args.nrow)]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": "the reference CUDA build did not finish within 900 s"}
+    lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+    if r.returncode != 0 or not lines:
+        tail = (r.stderr or r.stdout or "").strip().splitlines()[-1:] or [""]
+        return {"unavailable": "the reference CUDA build exited with status %d: %s"
+                               % (r.returncode, tail[0][:200])}
+    return json.loads(lines[-1])
 
 
 def run_reference(args, rank, world):
-    """--impl reference: rank 0 times the reference algorithm on the host."""
+    """--impl reference: rank 0 times the reference algorithm on the host
+    cores (the oracle port, extrapolated from samples: CpuReference), and
+    reports the reference's own CUDA build beside it (reference_cuda)."""
     if rank != 0:
         return None
+    cpu = CpuReference(args.config)
     vals = []
     for i in range(args.warmup + args.steps):
-        r = cpu_reference_rate(args.config, nsample=100_000, seed=i)
+        r = cpu.sample(100_000, seed=i)
         if i >= args.warmup:
             vals.append(r)
+    del cpu
     v = statistics.median(x["value"] for x in vals)
     r = dict(vals[-1])
     r["value"] = v
+    r["reference_cuda"] = reference_cuda(args)
     return r
 
 
@@ -573,33 +747,31 @@ def make_batch_data(specs, torch):
     return out
 
 
-def run_batch(args):
-    """Batched uneven solves through cugridder_b200.batch.Batch (one persistent
-    spreading / interpolation launch per direction, autotuned tiling, CUDA
-    graph replay) against the same datasets through one Plan each, called in
-    sequence.  One step = ms2dirty then dirty2ms of every dataset; Mvis/s =
-    sum(nrow * nchan) / step time.  The visibilities are restored between
-    steps, outside the timed brackets."""
+def batched_forms(args, kern, steps, warmup, sequential=True):
+    """The batched workload (synth.batch_specs: 32 uneven datasets, eps 1e-4)
+    through cugridder_b200.batch.Batch -- one persistent spreading /
+    interpolation launch per direction, autotuned tiling, CUDA graph replay --
+    in three forms: the learned kernel in FP32, ES in FP32 and plain ES in
+    FP64; and (sequential=True) the same datasets through one Plan each,
+    called in sequence.  One step = ms2dirty then dirty2ms of every dataset;
+    Mvis/s = sum(nrow * nchan) / step time.  The visibilities are restored
+    between steps, outside the timed brackets."""
     import torch
 
     from cugridder_b200 import Plan, _lib, synth
     from cugridder_b200.batch import Batch
 
-    args.eps = 1e-4
     eps = 1e-4
-    torch.cuda.set_device(0)
     lib = _lib.load()
-    kern = select_kernel(args)
     specs = synth.batch_specs()
-    ds = make_batch_data(specs, torch)
+    ds32 = make_batch_data(specs, torch)
     nvis = sum(sp["nrow"] * sp["nchan"] for sp in specs)
-    pristine = [d["vis"].clone() for d in ds]
     st = torch.cuda.current_stream()
 
-    def timed(step_fn, steps, restore):
-        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(steps)]
+    def timed(step_fn, nsteps, restore):
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(nsteps)]
         torch.cuda.synchronize()
-        for k in range(steps):
+        for k in range(nsteps):
             restore()
             ev[k][0].record(st)
             step_fn(0)
@@ -611,14 +783,23 @@ def run_batch(args):
         d2m = [e[1].elapsed_time(e[2]) for e in ev]
         return statistics.median(m2d), statistics.median(d2m)
 
-    def restore():
-        for d, v in zip(ds, pristine):
-            d["vis"].copy_(v)
-
+    es = {"kind": "es", "W": 0, "coef": None}
     out = {}
-    clocks = ClockSampler(0)
-    for label, kk, prec in (("learned_fp32", kern, "fp32"),
-                            ("es_fp32", {"kind": "es", "W": 0, "coef": None}, "fp32")):
+    clocks = ClockSampler(torch.cuda.current_device())
+    for label, kk, prec in (("learned_fp32", kern, "fp32"), ("es_fp32", es, "fp32"),
+                            ("es_fp64", es, "fp64")):
+        if prec == "fp64":
+            ds = [dict(d, vis=d["vis"].to(torch.complex128), wgt=d["wgt"].to(torch.float64),
+                       dirty=torch.zeros(d["dirty"].shape, dtype=torch.complex128, device="cuda"))
+                  for d in ds32]
+        else:
+            ds = ds32
+        pristine = [d["vis"].clone() for d in ds]
+
+        def restore():
+            for d, v in zip(ds, pristine):
+                d["vis"].copy_(v)
+
         b = Batch(ds, epsilon=eps, precision=prec)
         if kk["kind"] == "poly":
             b.set_kernel("poly", kk["W"], kk["coef"])
@@ -631,65 +812,90 @@ def run_batch(args):
         b.dirty2ms()
         torch.cuda.synchronize()
         launches = lib.cg_kernel_launches() - l1
-        for _ in range(max(1, args.warmup - 2)):
+        for _ in range(max(1, warmup - 2)):
             b.ms2dirty()
             b.dirty2ms()
         if label == "learned_fp32":
             clocks.start()
-        m2d, d2m = timed(lambda dr: b.ms2dirty() if dr == 0 else b.dirty2ms(), args.steps, restore)
+        m2d, d2m = timed(lambda dr: b.ms2dirty() if dr == 0 else b.dirty2ms(), steps, restore)
         if label == "learned_fp32":
             clocks.stop()
         gt, dt, tms = b.tiling()
-        out[label] = {"value": nvis / ((m2d + d2m) * 1e-3) / 1e6, "ms_ms2dirty": m2d, "ms_dirty2ms": d2m,
+        out[label] = {"value": round(nvis / ((m2d + d2m) * 1e-3) / 1e6, 2),
+                      "ms_ms2dirty": round(m2d, 3), "ms_dirty2ms": round(d2m, 3),
                       "kernels_per_step": launches, "eager_first_call_launches": l1 - l0,
                       "tiling": {"grid_warp_tile": gt, "degrid_tile": dt,
                                  "phase2_ms": [round(x, 3) for x in tms]},
                       "W": kk["W"] or None}
+        restore()
         b.close()
         del b
+        if prec == "fp64":
+            del ds, pristine
         torch.cuda.synchronize()
+        torch.cuda.empty_cache()
 
-    # the same datasets through one Plan each, called in sequence
-    seq_m2d = seq_d2m = 0.0
-    for d, v in zip(ds, pristine):
-        n = d["dirty"].shape[0]
-        p = Plan(n, n, d["fov"], eps, precision="fp32")
-        if kern["kind"] == "poly":
-            p.set_kernel("poly", kern["W"], kern["coef"])
-        out_vis = torch.empty_like(d["vis"])
+    if sequential:
+        # the same datasets through one Plan each, called in sequence
+        ds = ds32
+        seq_m2d = seq_d2m = 0.0
+        for d in ds:
+            nx, ny = d["dirty"].shape
+            p = Plan(nx, ny, d["fov"], eps, precision="fp32")
+            if kern["kind"] == "poly":
+                p.set_kernel("poly", kern["W"], kern["coef"])
+            out_vis = torch.empty_like(d["vis"])
 
-        def step(dr):
-            if dr == 0:
-                p.ms2dirty_chan(d["uvw"], d["freqs"], d["vis"], d["wgt"], d["dirty"])
-            else:
-                p.dirty2ms_chan(d["uvw"], d["freqs"], d["dirty"], d["wgt"], out_vis)
+            def step(dr):
+                if dr == 0:
+                    p.ms2dirty_chan(d["uvw"], d["freqs"], d["vis"], d["wgt"], d["dirty"])
+                else:
+                    p.dirty2ms_chan(d["uvw"], d["freqs"], d["dirty"], d["wgt"], out_vis)
 
-        step(0)
-        step(1)
-        m2d, d2m = timed(step, 2, lambda: None)
-        seq_m2d += m2d
-        seq_d2m += d2m
-        p.close()
-    out["sequential_plans_learned_fp32"] = {"value": nvis / ((seq_m2d + seq_d2m) * 1e-3) / 1e6,
-                                            "ms_ms2dirty": seq_m2d, "ms_dirty2ms": seq_d2m}
+            step(0)
+            step(1)
+            m2d, d2m = timed(step, 2, lambda: None)
+            seq_m2d += m2d
+            seq_d2m += d2m
+            p.close()
+        out["sequential_plans_learned_fp32"] = {
+            "value": round(nvis / ((seq_m2d + seq_d2m) * 1e-3) / 1e6, 2),
+            "ms_ms2dirty": round(seq_m2d, 3), "ms_dirty2ms": round(seq_d2m, 3)}
+    meta = {"workload": "batch_32_uneven", "datasets": len(specs),
+            "rows": sum(sp["nrow"] for sp in specs), "visibilities": nvis,
+            "images": sorted({sp["nx"] for sp in specs}), "eps": eps,
+            "kernel": kern.get("label", "ES"),
+            "l2": "inputs larger than L2 (%.1f GB of visibilities)" % (nvis * 8 / 1e9)}
+    del ds32
+    torch.cuda.empty_cache()
+    return out, meta, clocks.summary()
+
+
+def run_batch(args):
+    """--batch: the batched workload's own line (see batched_forms)."""
+    import torch
+
+    args.eps = 1e-4
+    torch.cuda.set_device(0)
+    kern = select_kernel(args)
+    out, meta, clocks = batched_forms(args, kern, args.steps, args.warmup)
     main = out["learned_fp32"]
-    line = {"metric": BATCH_METRIC, "value": round(main["value"], 2), "unit": "Mvis/s", "n_gpus": 1,
+    line = {"metric": BATCH_METRIC, "value": main["value"], "unit": "Mvis/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(main["ms_ms2dirty"] + main["ms_dirty2ms"], 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 (fp64 uvw/coordinates)", "data": "synthetic",
-            "config": {"workload": "batch_32_uneven", "datasets": len(specs),
-                       "rows": sum(sp["nrow"] for sp in specs), "visibilities": nvis,
-                       "images": sorted({sp["nx"] for sp in specs}), "eps": eps,
-                       "kernel": kern.get("label", "ES"),
-                       "l2": "inputs larger than L2 (%.1f GB of visibilities)" % (nvis * 8 / 1e9)},
-            "forms": out, "clocks": clocks.summary(),
+            "dtype": "f32 (fp64 uvw/coordinates)", "data": "synthetic", "config": meta,
+            "forms": out, "clocks": clocks,
+            "learned_fp32_over_es_fp64": round(main["value"] / out["es_fp64"]["value"], 3),
             "batched_over_sequential": round(main["value"] / out["sequential_plans_learned_fp32"]["value"], 3)}
     print(json.dumps(line), flush=True)
 
 
 def main():
     args = parse()
+    if args.ref_cuda_worker:
+        reference_cuda_worker(args)
+        return
     if args.batch:
         run_batch(args)
         return
@@ -701,35 +907,36 @@ def main():
                     "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                     "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                     "dtype": "f64", "data": "synthetic",
-                    "config": {"workload": args.config, "eps": args.eps},
+                    "config": workload_config(args, world),
                     "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
                     "e2e": {"value": r["value"], "unit": "Mvis/s", "h2d_bytes_per_step": 0,
-                            "d2h_bytes_per_step": 0}}
+                            "d2h_bytes_per_step": 0},
+                    "reference_cuda": r["reference_cuda"]}
             print(json.dumps(line), flush=True)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
         return
     res = run_b200(args, rank, world, local)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_reference_rate(args.config)
     if rank == 0:
-        from cugridder_b200 import synth
-
-        cfg = synth.CONFIGS[args.config]
         info = res.pop("info")
         line = {
             "metric": METRIC, "value": round(res["value"], 2), "unit": "Mvis/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(res["ms_per_step"], 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (fp64 uvw/coordinates)", "data": "synthetic",
-            "config": {"workload": args.config, "nx": cfg["nx"], "ny": cfg["ny"], "fov_deg": args.fov or cfg["fov"],
-                       "nrow_per_gpu": args.nrow or cfg["nrow"], "freq_hz": cfg["freq"], "eps": args.eps,
-                       "kernel": res["kernel"]["label"], "W": info["kw"], "nw": info["nw"], "grid": [info["nf1"], info["nf2"]],
-                       "tiling": dict(res["tiling"], autotuned=not args.no_autotune),
-                       "parallelism": "independent datasets per GPU" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (uvw 480 MB, grid 7.5 GB)"},
+            "config": workload_config(args, world),
+            "impl_detail": {"kernel": res["kernel"]["label"], "W": info["kw"], "nw": info["nw"],
+                            "grid": [info["nf1"], info["nf2"]],
+                            "tiling": dict(res["tiling"], autotuned=not args.no_autotune)},
             "roofline": res["roofline"], "cpu_baseline": cpu, "e2e": res.get("e2e"),
             "gpu_launches": res["gpu_launches"], "clocks": res["clocks"],
             "fp64_plain": res.get("fp64_plain"), "fp32_over_fp64": res.get("fp32_over_fp64"),
+            "fp64_eps_leg": res.get("fp64_eps_leg"), "batched": res.get("batched"),
             "accuracy": res.get("accuracy"), "adjointness": res.get("adjointness"),
             "stages": res["stages"],
         }

@@ -167,11 +167,17 @@ def fseries_w(p):
     return out, zp
 
 
-def grid(p, X, c):
-    """Periodic ES spreading; returns fw [nf3, nf2, nf1] complex128."""
+def grid(p, X, c, out=None):
+    """Periodic ES spreading; returns fw [nf3, nf2, nf1] complex128 (written
+    into `out` when given: a C-contiguous complex128 array of that shape)."""
     c = _c128(c)
     X = _f64c(X)
-    fw = np.zeros((p.nf3, p.nf2, p.nf1), dtype=np.complex128)
+    if out is not None:
+        assert out.dtype == np.complex128 and out.flags.c_contiguous
+        assert out.shape == (p.nf3, p.nf2, p.nf1)
+        fw = out
+    else:
+        fw = np.zeros((p.nf3, p.nf2, p.nf1), dtype=np.complex128)
     lib().og_grid(ctypes.byref(p), _d(X[0]), _d(X[1]), _d(X[2]), _d(c.view(np.float64)),
                   _d(fw.view(np.float64)))
     return fw

@@ -1,7 +1,13 @@
-"""Batched solves (cg_batch_*) against one plan per dataset: uneven datasets
-(image sizes, fov, rows, channels, one without rows), the eager and
-autotuned first call, the captured second call and graph replays with new
-visibilities / images; and the untuned eager form."""
+"""Batched solves (cg_batch_*) against the oracle and against one plan per
+dataset: uneven datasets (image sizes, fov, rows, channels, one without rows,
+one non-square image on a grid with partial last hives and rows over its
+whole band), the eager and autotuned first call, the captured second call and
+graph replays with new visibilities / images; and the untuned eager form.
+
+The oracle sees each dataset as the library defines multi-channel calls:
+row r of channel c becomes row r * nchan + c at f_0 = freqs[0] with
+uvw * (f_c / f_0), which has the same phase as row r at f_c.  A direct sum
+over the channels at their own frequencies checks that definition itself."""
 import numpy as np
 import pytest
 
@@ -13,27 +19,70 @@ from tests.gpu_helpers import to_dev
 
 pytestmark = pytest.mark.gpu
 
-SPECS = [(64, 1.0, 3000, 1), (96, 2.5, 12000, 3), (128, 1.5, 20000, 2), (64, 4.0, 5000, 4),
-         (80, 3.0, 800, 1), (128, 2.0, 30000, 1), (64, 2.0, 0, 2)]
+# (nx, ny, fov, rows, channels); the 42 x 74 image (grid 90 x 150) has rows
+# over its whole band and past it
+SPECS = [(64, 64, 1.0, 3000, 1), (96, 96, 2.5, 12000, 3), (128, 128, 1.5, 20000, 2),
+         (64, 64, 4.0, 5000, 4), (80, 80, 3.0, 800, 1), (128, 128, 2.0, 30000, 1),
+         (64, 64, 2.0, 0, 2), (42, 74, 3.0, 6000, 2)]
 
 
 def _datasets(torch):
     out = []
-    for i, (n, fov, nrow, nchan) in enumerate(SPECS):
-        d = synth.make("ms2dirty_256_fp64", seed=100 + i, nrow=nrow, nx=n, ny=n, fov=fov)
+    for i, (nx, ny, fov, nrow, nchan) in enumerate(SPECS):
+        if nx == ny:
+            d = synth.make("ms2dirty_256_fp64", seed=100 + i, nrow=nrow, nx=nx, ny=ny, fov=fov)
+        else:
+            d = synth.wrap_case(nrow, nx, ny, fov, freq=1.0e8, seed=100 + i)
         freqs = np.linspace(1.0e8, 2.0e8, nchan) if nchan > 1 else np.array([1.0e8])
         rng = np.random.Generator(np.random.PCG64(200 + i))
         vis = (rng.standard_normal((nrow, nchan)) + 1j * rng.standard_normal((nrow, nchan))).astype(np.complex64)
         wgt = rng.uniform(0.5, 1.5, (nrow, nchan)).astype(np.float32)
         out.append(dict(uvw=to_dev(torch, d["uvw"]), freqs=freqs, vis=to_dev(torch, vis),
-                        wgt=to_dev(torch, wgt), fov=fov,
-                        dirty=torch.zeros((n, n), dtype=torch.complex64, device="cuda")))
+                        wgt=to_dev(torch, wgt), fov=fov, h_uvw=d["uvw"], h_wgt=wgt, h_vis=vis,
+                        dirty=torch.zeros((nx, ny), dtype=torch.complex64, device="cuda")))
     return out
 
 
+def _flatten(d):
+    """The dataset's rows and channels as the library flattens them."""
+    f0 = d["freqs"][0]
+    s = np.array([1.0] + [f / f0 for f in d["freqs"][1:]])
+    uvw = (d["h_uvw"][:, None, :] * s[None, :, None]).reshape(-1, 3)
+    return uvw, f0
+
+
+def _oracle_ref(d, direction, eps, kernel=None):
+    """The oracle's result for one dataset of the batch (channels flattened)."""
+    from oracle import oracle as O
+
+    nx, ny = d["dirty"].shape
+    uvw, f0 = _flatten(d)
+    wgt = d["h_wgt"].reshape(-1).astype(np.float64)
+    if kernel is not None:
+        O.set_kernel("poly", kernel.W, kernel.horner)
+    try:
+        if direction == 0:
+            vis = d["vis"].cpu().numpy().reshape(-1)
+            out, _ = O.ms2dirty(uvw, vis, wgt, nx, ny, d["fov"], f0, eps)
+        else:
+            out, _ = O.dirty2ms(uvw, d["dirty"].cpu().numpy(), wgt, d["fov"], f0, eps)
+            out = out.reshape(d["vis"].shape)
+    finally:
+        if kernel is not None:
+            O.set_kernel("es")
+    return out
+
+
+def _close_oracle(out, d, direction, eps, kernel=None, tol=2e-5):
+    ref = _oracle_ref(d, direction, eps, kernel)
+    if ref.size == 0 or not np.any(ref):
+        return not np.any(out)
+    return rel_l2(out, ref) < tol
+
+
 def _plan_ref(torch, d, direction, kernel=None):
-    n = d["dirty"].shape[0]
-    p = Plan(n, n, d["fov"], 1e-4, precision="fp32")
+    nx, ny = d["dirty"].shape
+    p = Plan(nx, ny, d["fov"], 1e-4, precision="fp32")
     if kernel is not None:
         p.set_kernel("poly", kernel.W, kernel.horner)
     if direction == 0:
@@ -59,8 +108,10 @@ def _check_batch(torch, ds, b, ncalls, kernel=None):
             d["vis"].mul_(complex(0.5 + 0.1 * call, 0.2))
         b.ms2dirty()
         torch.cuda.synchronize()
-        for d in ds:
-            assert _close(d["dirty"].cpu().numpy(), _plan_ref(torch, d, 0, kernel)), call
+        for i, d in enumerate(ds):
+            out = d["dirty"].cpu().numpy()
+            assert _close(out, _plan_ref(torch, d, 0, kernel)), call
+            assert _close_oracle(out, d, 0, 1e-4, kernel), (call, i)
     for call in range(ncalls):
         for i, d in enumerate(ds):
             d["dirty"].copy_(torch.from_numpy(
@@ -68,8 +119,10 @@ def _check_batch(torch, ds, b, ncalls, kernel=None):
                                    dtype=np.complex64)).cuda())
         b.dirty2ms()
         torch.cuda.synchronize()
-        for d in ds:
-            assert _close(d["vis"].cpu().numpy(), _plan_ref(torch, d, 1, kernel)), call
+        for i, d in enumerate(ds):
+            out = d["vis"].cpu().numpy()
+            assert _close(out, _plan_ref(torch, d, 1, kernel)), call
+            assert _close_oracle(out, d, 1, 1e-4, kernel), (call, i)
 
 
 def test_batch_learned_kernel(torch_cuda):
@@ -106,6 +159,7 @@ def test_batch_matches_plans_through_graph_replays(torch_cuda):
         torch.cuda.synchronize()
         for d in ds:
             assert _close(d["dirty"].cpu().numpy(), _plan_ref(torch, d, 0)), call
+            assert _close_oracle(d["dirty"].cpu().numpy(), d, 0, 1e-4), call
     for call in range(3):
         for i, d in enumerate(ds):
             d["dirty"].copy_(torch.from_numpy(
@@ -115,6 +169,7 @@ def test_batch_matches_plans_through_graph_replays(torch_cuda):
         torch.cuda.synchronize()
         for d in ds:
             assert _close(d["vis"].cpu().numpy(), _plan_ref(torch, d, 1)), call
+            assert _close_oracle(d["vis"].cpu().numpy(), d, 1, 1e-4), call
     grid_t, degrid_t, ms = b.tiling()
     assert grid_t[0] in (16, 32) and grid_t[1] in (8, 16, 32), grid_t
     assert degrid_t[3] in (256, 512), degrid_t
@@ -127,14 +182,14 @@ def test_batch_fp64_matches_plans(torch_cuda):
     against one FP64 plan per dataset."""
     torch = torch_cuda
     ds = []
-    for i, (n, fov, nrow, nchan) in enumerate(SPECS[:4]):
+    for i, (n, _, fov, nrow, nchan) in enumerate(SPECS[:4]):
         d = synth.make("ms2dirty_256_fp64", seed=400 + i, nrow=nrow, nx=n, ny=n, fov=fov)
         freqs = np.linspace(1.0e8, 2.0e8, nchan) if nchan > 1 else np.array([1.0e8])
         rng = np.random.Generator(np.random.PCG64(500 + i))
         vis = rng.standard_normal((nrow, nchan)) + 1j * rng.standard_normal((nrow, nchan))
         wgt = rng.uniform(0.5, 1.5, (nrow, nchan))
         ds.append(dict(uvw=to_dev(torch, d["uvw"]), freqs=freqs, vis=to_dev(torch, vis),
-                       wgt=to_dev(torch, wgt), fov=fov,
+                       wgt=to_dev(torch, wgt), fov=fov, h_uvw=d["uvw"], h_wgt=wgt,
                        dirty=torch.zeros((n, n), dtype=torch.complex128, device="cuda")))
     b = Batch(ds, epsilon=1e-9, precision="fp64")
     for call in range(3):
@@ -148,6 +203,7 @@ def test_batch_fp64_matches_plans(torch_cuda):
             torch.cuda.synchronize()
             p.close()
             assert rel_l2(d["dirty"].cpu().numpy(), out.cpu().numpy()) < 1e-12, call
+            assert _close_oracle(d["dirty"].cpu().numpy(), d, 0, 1e-9, tol=1e-10), call
     for call in range(2):
         b.dirty2ms()
         torch.cuda.synchronize()
@@ -159,4 +215,46 @@ def test_batch_fp64_matches_plans(torch_cuda):
             torch.cuda.synchronize()
             p.close()
             assert rel_l2(d["vis"].cpu().numpy(), out.cpu().numpy()) < 1e-12, call
+            assert _close_oracle(d["vis"].cpu().numpy(), d, 1, 1e-9, tol=1e-10), call
+    b.close()
+
+
+def test_batch_channel_flattening_vs_direct_sums(torch_cuda):
+    """The flattened-channel definition itself: the batch's image equals the
+    FP64 direct sum over every (row, channel) at the channel's own frequency,
+    and its visibilities the direct adjoint sums per channel, within 2 eps on
+    pixel / row subsets."""
+    from oracle import oracle as O
+
+    torch = torch_cuda
+    ds = _datasets(torch)
+    b = Batch(ds, epsilon=1e-4, precision="fp32")
+    b.ms2dirty()
+    torch.cuda.synchronize()
+    images = [d["dirty"].cpu().numpy() for d in ds]
+    imgs_in = []
+    for i, d in enumerate(ds):
+        img = synth.random_image(d["dirty"].shape[0], d["dirty"].shape[1], seed=700 + i,
+                                 dtype=np.complex64)
+        imgs_in.append(img)
+        d["dirty"].copy_(torch.from_numpy(img).cuda())
+    b.dirty2ms()
+    torch.cuda.synchronize()
+    rng = np.random.default_rng(5)
+    for i, d in enumerate(ds):
+        nx, ny = images[i].shape
+        nrow, nchan = d["vis"].shape
+        if nrow == 0:
+            continue
+        vis_out = d["vis"].cpu().numpy()  # dirty2ms output; the ms2dirty input is h_vis
+        wgt = d["h_wgt"].astype(np.float64)
+        pix = rng.choice(nx * ny, min(256, nx * ny), replace=False)
+        rows = rng.choice(nrow, min(256, nrow), replace=False)
+        for c in range(nchan):
+            truth_v = O.dft_dirty2ms(d["h_uvw"], imgs_in[i], wgt[:, c], d["fov"], d["freqs"][c],
+                                     rows=rows)
+            assert rel_l2(vis_out[rows, c], truth_v) < 2e-4, (i, c)
+        truth_d = sum(O.dft_ms2dirty(d["h_uvw"], d["h_vis"][:, c], wgt[:, c], nx, ny, d["fov"],
+                                     d["freqs"][c], pixels=pix) for c in range(nchan))
+        assert rel_l2(images[i].reshape(-1)[pix], truth_d) < 2e-4, i
     b.close()

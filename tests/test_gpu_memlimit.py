@@ -1,5 +1,6 @@
 """Memory-limited mode (cg_plan_set_grid_budget): w planes processed window by
-window give the resident path's results, in both directions."""
+window (the reference's plane-cube loop, ra_exec.cu:292-389 and 522-613) give
+the oracle's results and the resident path's, in both directions."""
 import numpy as np
 import pytest
 
@@ -32,11 +33,24 @@ def _run(torch, d, img, precision, budget, kernel=None):
     return dirty.cpu().numpy(), vis.cpu().numpy(), info
 
 
+def _eps(precision):
+    return 1e-5 if precision == "fp32" else 1e-9
+
+
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("fp32", 1e-5)])
 @pytest.mark.parametrize("planes_per_window", [1, 3])
-def test_windows_match_resident(torch_cuda, precision, tol, planes_per_window):
-    d = synth.make("ms2dirty_256_fp64", seed=13, nrow=30000, nx=160, ny=128)
-    img = synth.random_image(160, 128, seed=14)
+@pytest.mark.parametrize("case", ["c1_160x128", "wrap_122x250"])
+def test_windows_match_oracle_and_resident(torch_cuda, oracle, precision, tol, planes_per_window,
+                                           case):
+    """Both directions against the oracle (FP64: 1e-10; FP32: 2e-5) and
+    against the resident path; the second case has rows over the whole band
+    and past it on a grid with partial last hives (nf 250 x 500)."""
+    if case == "c1_160x128":
+        d = synth.make("ms2dirty_256_fp64", seed=13, nrow=30000, nx=160, ny=128)
+    else:
+        d = synth.wrap_case(30000, 122, 250, 3.0, seed=19)
+    nx, ny = d["nx"], d["ny"]
+    img = synth.random_image(nx, ny, seed=14)
     ref = _run(torch_cuda, d, img, precision, 0)
     info = ref[2]
     tsz = 16 if precision == "fp64" else 8
@@ -45,6 +59,12 @@ def test_windows_match_resident(torch_cuda, precision, tol, planes_per_window):
     assert got[2]["nw"] == info["nw"] and info["nw"] > planes_per_window
     assert rel_l2(got[0], ref[0]) < tol
     assert rel_l2(got[1], ref[1]) < tol
+    eps = _eps(precision)
+    ora_tol = 1e-10 if precision == "fp64" else 2e-5
+    o_d, _ = oracle.ms2dirty(d["uvw"], d["vis"], d["wgt"], nx, ny, d["fov"], d["freq"], eps)
+    o_v, _ = oracle.dirty2ms(d["uvw"], img, d["wgt"], d["fov"], d["freq"], eps)
+    assert rel_l2(got[0], o_d) < ora_tol
+    assert rel_l2(got[1], o_v) < ora_tol
 
 
 def test_windows_with_learned_kernel(torch_cuda):
@@ -58,6 +78,15 @@ def test_windows_with_learned_kernel(torch_cuda):
     ref = _run(torch_cuda, d, img, "fp32", 0, k)
     got = _run(torch_cuda, d, img, "fp32", 2 * ref[2]["nf1"] * ref[2]["nf2"] * 8, k)
     assert rel_l2(got[0], ref[0]) < 1e-5 and rel_l2(got[1], ref[1]) < 1e-5
+    from oracle import oracle as O
+
+    O.set_kernel("poly", k.W, k.horner)
+    try:
+        o_d, _ = O.ms2dirty(d["uvw"], d["vis"], d["wgt"], 128, 128, d["fov"], d["freq"], 1e-5)
+        o_v, _ = O.dirty2ms(d["uvw"], img, d["wgt"], d["fov"], d["freq"], 1e-5)
+    finally:
+        O.set_kernel("es")
+    assert rel_l2(got[0], o_d) < 2e-5 and rel_l2(got[1], o_v) < 2e-5
 
 
 def test_budget_below_one_plane(torch_cuda):
