@@ -23,7 +23,7 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libcugridder.so")
 ALIAS = os.path.join(LIBDIR, "libcurafft.so")
 
-SOURCES = ["cg_bin.cu", "cg_spread.cu", "cg_grid_mma.cu", "cg_wstage.cu", "cg_pipeline.cu",
+SOURCES = ["cg_bin.cu", "cg_spread.cu", "cg_grid_slide.cu", "cg_grid_mma.cu", "cg_wstage.cu", "cg_pipeline.cu",
            "cg_capi.cu", "cg_static.cu", "cg_learn.cu",
            "cg_explicit.cu", "cg_fft.cu", "cg_nufft.cu", "cg_batch.cu", "cg_degrid_tma.cu"]
 

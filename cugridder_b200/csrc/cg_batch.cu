@@ -182,6 +182,7 @@ int prepare_phase2(cg_batch_s* B, int dir, cudaStream_t st) {
     cg::TileTune best_tt = B->tune;
     for (int c = 0; c < ncand; c++) {
       if (dir == 1 && cand[c][3] < 0) continue;  // the TMA-staged kernel is single-grid only
+      if (dir == 0 && cand[c][0] < 0) continue;  // so are the x-sliding gridding windows
       cg::TileTune tt = B->tune;
       cg::set_tile_candidate(tt, dir, cand[c]);
       if (build_jobs<T>(B, dir, tt, jobs, order, &sh) != CG_OK || jobs.empty()) continue;

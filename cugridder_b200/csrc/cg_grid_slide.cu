@@ -1,0 +1,415 @@
+// Gridding (spreading) by x-sliding warp windows.
+//
+// Same sum as k_grid_warp (conv_3d_outputdriven_t1, conv.cu:522-627):
+//   fw[p][g1][g0] = sum_j c_j phi(g0 - X0_j) phi(g1 - X1_j) phi(p - X2_j),
+// periodic in all three axes, every grid cell written exactly once, no
+// atomics, a deterministic result.
+//
+// Work item = (band of TY grid rows g1, segment of SEG hive columns along
+// g0), all w planes.  The warp walks the segment's hive columns left to right
+// (rows are sorted hive-major with the hive column fastest, so each hive of a
+// column is one contiguous run of the sorted stream) and accumulates into a
+// circular window of kXW = 16 columns x TY rows x nw planes in shared memory.
+// A row in hive column c has its taps in cells [8c - lo, 8c + 7 + hi]; once
+// column c is done, no later column reaches below 8(c + 1) - lo, so the 8
+// cells [8c - 4, 8c + 4) are final (4 >= lo for W <= 8): they are flushed to
+// HBM and their window slots zeroed.  The window then holds at most
+// 8 + 4 + hi <= 16 columns, and a segment needs one warm-up column (c =
+// first - 1) whose cells are not flushed.  Consequences against the tiled
+// kernel: a row is visited once along x (only the band edges in g1 revisit
+// it: (TY + W - 1) / TY visits), and along w every plane is resident, so the
+// plane index wraps inside the lane instead of revisiting rows with a shift.
+//
+// Lanes take the (dy, dz) tap pairs of a row that fall inside the band: pair
+// p = lane -> (dy, dz) = (dya + p / W, p % W), so a row that only partly
+// overlaps the band needs one round of 32 pairs; the pairs beyond 32 are
+// spread one tap per lane.  Cell (x, y, z) is at y * RS + z * PS + (x & 15)
+// with PS = 17 and RS = W (mod 16): lane p then hits bank p + const (mod 16),
+// conflict-free for every row whose taps do not wrap around the w axis.
+//
+// Applies to W in 4..8 with nf1 and nf2 multiples of 8 (whole hive columns
+// and rows); launch_grid_slide returns CG_ERR_ARG otherwise and the plan
+// keeps the tiled kernel.
+#include <algorithm>
+#include <cstdlib>
+
+#include "cg_coords.cuh"
+#include "cg_launch.cuh"
+#include "cg_tiles.cuh"
+
+namespace cg {
+namespace {
+
+constexpr int kXW = 16;      // window columns (circular)
+constexpr int kPS = kXW + 1;  // plane stride (complex units)
+constexpr int kFlushL = 4;    // flushed cells of column c: [8c - 4, 8c + 4)
+
+struct SlideTile {
+  int TY, logTY, SEG;  // band rows (8, 16 or 32), hive columns per segment
+  int RS;              // row stride of the window (complex units)
+  int nslots;          // (hive rows of a band's halo) x nw
+  int nbands, nsegs, nitems;
+  int warps;
+  size_t warp_bytes, smem;
+};
+
+template <typename T>
+struct Cx;
+template <>
+struct Cx<float> { using type = float2; };
+template <>
+struct Cx<double> { using type = double2; };
+
+__device__ __forceinline__ int warp_scan_excl(int x, int& total) {
+  const int lane = threadIdx.x & 31;
+  int inc = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  total = __shfl_sync(0xffffffffu, inc, 31);
+  return inc - x;
+}
+
+// zero-fill the cells [x0, x0 + n) (n even, x0 even, may start below 0:
+// wrapped) of rows [y0, y0 + wy) on every plane
+template <typename T>
+__device__ __forceinline__ void zero_region(T* __restrict__ fw, const Geom& g, int x0, int n, int y0,
+                                            int wy) {
+  using C = typename Cx<T>::type;
+  C* fwc = reinterpret_cast<C*>(fw);
+  const int lane = threadIdx.x & 31;
+  const int np = n >> 1;
+  const size_t plane = (size_t)g.nf1 * g.nf2;
+  const int total = np * wy * g.nw;
+  for (int i = lane; i < total; i += 32) {
+    const int q = i % np, r = i / np, y = r % wy, z = r / wy;
+    int x = x0 + 2 * q;
+    if (x < 0) x += g.nf1;
+    C* dst = fwc + (size_t)z * plane + (size_t)(y0 + y) * g.nf1 + x;
+    if constexpr (sizeof(T) == 4) {
+      *reinterpret_cast<float4*>(dst) = make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+      dst[0] = make_double2(0.0, 0.0);
+      dst[1] = make_double2(0.0, 0.0);
+    }
+  }
+}
+
+template <typename T, int W, bool kPoly>
+__device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
+                                           const int* __restrict__ hive_start, const Geom& g,
+                                           const SlideTile& tc, T* __restrict__ fw, int item,
+                                           unsigned char* wsmem, const T (&pc)[kPolyCoef]) {
+  using C = typename Cx<T>::type;
+  constexpr int lo = Halo<W>::lo, hi = Halo<W>::hi;
+  const int lane = threadIdx.x & 31;
+  const int TY = tc.TY, RS = tc.RS, nw = g.nw, nf1 = g.nf1, nf2 = g.nf2;
+  const int nhx = g.nhx, nhy = g.nhy;
+  C* acc = reinterpret_cast<C*>(wsmem);
+  int* t_start = reinterpret_cast<int*>(wsmem + (size_t)TY * RS * sizeof(C));
+  int* t_pref = t_start + tc.nslots;      // nslots + 1
+  int* t_shy = t_pref + tc.nslots + 1;
+  const size_t plane = (size_t)nf1 * nf2;
+  C* fwc = reinterpret_cast<C*>(fw);
+  const T beta = (T)g.beta, ces = (T)g.es_c, halfw = (T)W * (T)0.5;
+
+  const int band = item / tc.nsegs, seg = item - band * tc.nsegs;
+  const int y0 = band * TY, y1 = min(y0 + TY, nf2), wy = y1 - y0;
+  const int hs = seg * tc.SEG, he = min(hs + tc.SEG, nhx);
+  const int hya = floordiv8(y0 - hi), hyb = floordiv8(y1 - 1 + lo);
+  const int nyr = hyb - hya + 1;
+  const int nslots = nyr * nw;
+
+  // rows of the item: the hive columns [hs - 1, he) of every slot
+  {
+    int any = 0;
+    for (int s = lane; s < nslots; s += 32) {
+      const int hz = s / nyr;
+      int hy = hya + (s - hz * nyr);
+      hy += hy < 0 ? nhy : (hy >= nhy ? -nhy : 0);
+      const int64_t rb = ((int64_t)hz * nhy + hy) * nhx;
+      int cnt = hive_start[rb + he] - hive_start[rb + max(hs - 1, 0)];
+      if (hs == 0) cnt += hive_start[rb + nhx] - hive_start[rb + nhx - 1];
+      any |= cnt > 0;
+    }
+    if (!__any_sync(0xffffffffu, any)) {
+      zero_region<T>(fw, g, 8 * hs - kFlushL, 8 * (he - hs), y0, wy);
+      return;
+    }
+  }
+  {
+    const int n = TY * RS;
+    for (int i = lane; i < n; i += 32) acc[i] = C{(T)0, (T)0};
+  }
+  __syncwarp();
+
+  for (int c = hs - 1; c < he; c++) {
+    const int cc = c < 0 ? c + nhx : c;
+    const int sx = c < 0 ? -nf1 : 0;
+    // segment table of column c: slot s = (hive row hya + s % nyr, plane s / nyr)
+    int carry = 0;
+    for (int base = 0; base < nslots; base += 32) {
+      const int s = base + lane;
+      int cnt = 0;
+      if (s < nslots) {
+        const int hz = s / nyr;
+        const int hyr = hya + (s - hz * nyr);
+        int hy = hyr, shy = 0;
+        if (hy < 0) { hy += nhy; shy = -nf2; }
+        else if (hy >= nhy) { hy -= nhy; shy = nf2; }
+        const int64_t h = ((int64_t)hz * nhy + hy) * nhx + cc;
+        const int st = hive_start[h];
+        cnt = hive_start[h + 1] - st;
+        t_start[s] = st;
+        t_shy[s] = shy;
+      }
+      int tot;
+      const int ex = carry + warp_scan_excl(cnt, tot);
+      if (s < nslots) t_pref[s] = ex;
+      carry += tot;
+    }
+    if (lane == 0) t_pref[nslots] = carry;
+    __syncwarp();
+    const int total = carry;
+
+    for (int q0 = 0; q0 < total; q0 += 32) {
+      const int q = q0 + lane;
+      bool ok = q < total;
+      T f0 = 0, f1 = 0, f2 = 0, c0 = 0, c1 = 0;
+      int ox = 0, oy = 0, oz = 0;
+      if (ok) {
+        int lo_s = 0, hi_s = nslots;  // t_pref[lo_s] <= q < t_pref[hi_s]
+        while (hi_s - lo_s > 1) {
+          const int mid = (lo_s + hi_s) >> 1;
+          if (t_pref[mid] <= q) lo_s = mid; else hi_s = mid;
+        }
+        const Rec<T> r = recs[t_start[lo_s] + (q - t_pref[lo_s])];
+        f0 = r.f[0]; f1 = r.f[1]; f2 = r.f[2]; c0 = r.c[0]; c1 = r.c[1];
+        ox = (int)(r.bxy & 0xFFFFu) + sx + tap_offset<W>(f0);
+        oy = (int)(r.bxy >> 16) + t_shy[lo_s] + tap_offset<W>(f1);
+        oz = (int)r.bz + tap_offset<W>(f2);
+        ok = oy < y1 && oy + W > y0;
+      }
+      unsigned mask = __ballot_sync(0xffffffffu, ok);
+      while (mask) {
+        const int src = __ffs(mask) - 1;
+        mask &= mask - 1;
+        const T g0 = __shfl_sync(0xffffffffu, f0, src), g1 = __shfl_sync(0xffffffffu, f1, src);
+        const T g2 = __shfl_sync(0xffffffffu, f2, src);
+        const T vr0 = __shfl_sync(0xffffffffu, c0, src), vi0 = __shfl_sync(0xffffffffu, c1, src);
+        const int vx = __shfl_sync(0xffffffffu, ox, src);
+        const int vy = __shfl_sync(0xffffffffu, oy, src) - y0;
+        const int vz = __shfl_sync(0xffffffffu, oz, src);
+        // kernel values: lane l < 3W holds tap l % W of axis l / W
+        T kv = (T)0;
+        if (lane < 3 * W) {
+          const int axis = lane / W, i = lane - axis * W;
+          const T f = axis == 0 ? g0 : (axis == 1 ? g1 : g2);
+          if constexpr (kPoly)
+            kv = poly_eval(pc, poly_arg<W>(f));
+          else
+            kv = es_kernel<T>((T)(tap_offset<W>(f) + i) - f, beta, ces, halfw);
+        }
+        T kx[W];
+#pragma unroll
+        for (int e = 0; e < W; e++) kx[e] = __shfl_sync(0xffffffffu, kv, e);
+        const int dya = max(0, -vy), dyb = min(W, wy - vy);
+        const int np = (dyb - dya) * W;
+        const int xs = vx & (kXW - 1);
+        {
+          const int p = lane, dq = p / W, dz = p - dq * W, dy = dya + dq;
+          const T ky = __shfl_sync(0xffffffffu, kv, (W + dy) & 31);
+          const T kz = __shfl_sync(0xffffffffu, kv, 2 * W + dz);
+          if (p < np) {
+            int z = vz + dz;
+            z += z < 0 ? nw : (z >= nw ? -nw : 0);
+            const T k = ky * kz;
+            const T vr = vr0 * k, vi = vi0 * k;
+            C* a = acc + (vy + dy) * RS + z * kPS;
+#pragma unroll
+            for (int e = 0; e < W; e++) {
+              C* cell = a + ((xs + e) & (kXW - 1));
+              C cur = *cell;
+              cur.x += vr * kx[e];
+              cur.y += vi * kx[e];
+              *cell = cur;
+            }
+          }
+        }
+        if (np > 32) {  // pairs 32 .. np - 1, one tap per lane (warp-uniform loop)
+          const int nt = (np - 32) * W;
+          for (int t0 = 0; t0 < nt; t0 += 32) {
+            const int t = t0 + lane;
+            const int pq = t / W, e = t - pq * W, p = 32 + pq;
+            const int dq = p / W, dz = p - dq * W, dy = dya + dq;
+            const T ky = __shfl_sync(0xffffffffu, kv, (W + dy) & 31);
+            const T kz = __shfl_sync(0xffffffffu, kv, (2 * W + dz) & 31);
+            const T kxe = __shfl_sync(0xffffffffu, kv, e & 31);
+            if (t < nt) {
+              int z = vz + dz;
+              z += z < 0 ? nw : (z >= nw ? -nw : 0);
+              const T k = ky * kz;
+              C* cell = acc + (vy + dy) * RS + z * kPS + ((xs + e) & (kXW - 1));
+              C cur = *cell;
+              cur.x += vr0 * k * kxe;
+              cur.y += vi0 * k * kxe;
+              *cell = cur;
+            }
+          }
+        }
+        __syncwarp();
+      }
+    }
+
+    {
+      // cells [8c - 4, 8c + 4) of every row and plane are final: flush them
+      // and zero their slots.  The warm-up column (c = hs - 1) only zeroes
+      // them: they belong to the previous segment, and their slots are those
+      // of cells [8c + 12, 8c + 20) that the next columns reach.
+      const bool write = c >= hs;
+      const int x0 = 8 * c - kFlushL;
+      const int n = TY * nw * 4;  // cell pairs
+      for (int i = lane; i < n; i += 32) {
+        const int pr = i & 3, rest = i >> 2;
+        const int y = rest & (TY - 1), z = rest >> tc.logTY;
+        if (y >= wy) continue;
+        const int x = x0 + 2 * pr;
+        const int slot = x & (kXW - 1);
+        C* a = acc + y * RS + z * kPS + slot;
+        const C a0 = a[0], a1 = a[1];
+        a[0] = C{(T)0, (T)0};
+        a[1] = C{(T)0, (T)0};
+        if (!write) continue;
+        const int gx = x < 0 ? x + nf1 : x;
+        C* dst = fwc + (size_t)z * plane + (size_t)(y0 + y) * nf1 + gx;
+        if constexpr (sizeof(T) == 4) {
+          *reinterpret_cast<float4*>(dst) = make_float4(a0.x, a0.y, a1.x, a1.y);
+        } else {
+          dst[0] = a0;
+          dst[1] = a1;
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+template <typename T, int W, bool kPoly>
+__global__ void __launch_bounds__(512) k_grid_slide(const Rec<T>* __restrict__ recs,
+                                                    const int* __restrict__ hive_start, Geom g,
+                                                    SlideTile tc, T* __restrict__ fw,
+                                                    int* __restrict__ counter) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  // piecewise-polynomial kernel: lane l < 3W evaluates segment l % W
+  T pc[kPolyCoef];
+#pragma unroll
+  for (int n = 0; n < kPolyCoef; n++) pc[n] = (T)0;
+  if constexpr (kPoly) {
+    const T* poly = geom_poly<T>(g);
+    if (lane < 3 * W) {
+      const int i = lane % W;
+#pragma unroll
+      for (int n = 0; n < kPolyCoef; n++) pc[n] = poly[i * kPolyCoef + n];
+    }
+  }
+  unsigned char* wsmem = smem + (size_t)wib * tc.warp_bytes;
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(counter, 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= tc.nitems) break;
+    slide_item<T, W, kPoly>(recs, hive_start, g, tc, fw, item, wsmem, pc);
+  }
+}
+
+constexpr size_t kSlideSmemMax = 227 * 1024;
+
+int env_or(const char* name, int dflt) {
+  const char* v = getenv(name);
+  return v ? atoi(v) : dflt;
+}
+
+// Band rows, hive columns per segment and warps per CTA: the tuned values,
+// else CG_SLIDE_TY / CG_SLIDE_SEG / CG_SLIDE_WARPS, else 8 / 32 / as many as
+// fit.
+bool slide_tiling(const Geom& g, size_t tsz, const TileTune* tt, SlideTile& tc) {
+  const int W = g.kw;
+  if (W < 4 || W > 8 || (g.nf1 % 8) != 0 || (g.nf2 % 8) != 0 || g.nf1 < kXW) return false;
+  int TY = (tt && tt->wy > 0 && tt->wx < 0) ? tt->wy : env_or("CG_SLIDE_TY", 8);
+  if (TY != 8 && TY != 16 && TY != 32) return false;
+  int SEG = (tt && tt->wpb > 0 && tt->wx < 0) ? tt->wpb : env_or("CG_SLIDE_SEG", 32);
+  SEG = std::max(1, std::min(SEG, g.nhx));
+  tc.TY = TY;
+  tc.logTY = TY == 8 ? 3 : (TY == 16 ? 4 : 5);
+  tc.SEG = SEG;
+  int rs = g.nw * kPS;
+  rs += ((W % 16) - (rs % 16) + 16) % 16;  // RS = W (mod 16)
+  tc.RS = rs;
+  const int nyr = (TY >> 3) + 2;
+  tc.nslots = nyr * g.nw;
+  tc.nbands = (g.nf2 + TY - 1) / TY;
+  tc.nsegs = (g.nhx + SEG - 1) / SEG;
+  if ((int64_t)tc.nbands * tc.nsegs > 2147483647LL) return false;
+  tc.nitems = tc.nbands * tc.nsegs;
+  tc.warp_bytes = ((size_t)TY * rs * 2 * tsz + (size_t)(3 * tc.nslots + 1) * 4 + 15) & ~(size_t)15;
+  int warps = (tt && tt->warps > 0 && tt->wx < 0) ? tt->warps : env_or("CG_SLIDE_WARPS", 0);
+  if (warps <= 0) warps = (int)std::max<size_t>(1, std::min<size_t>(16, kSlideSmemMax / tc.warp_bytes));
+  warps = std::min(warps, 16);
+  while (warps > 1 && tc.warp_bytes * warps > kSlideSmemMax) warps--;
+  if (tc.warp_bytes * warps > kSlideSmemMax) return false;
+  tc.warps = warps;
+  tc.smem = tc.warp_bytes * warps;
+  return true;
+}
+
+int sms_of_device() {
+  int dev = 0, n = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) n = 148;
+  return n;
+}
+
+template <typename T, int W>
+int launch_w(const Rec<T>* d_recs, const int* d_hive_start, const Geom& g, T* d_fw,
+             int* d_counter, cudaStream_t st, const SlideTile& tc) {
+  auto* kern = geom_poly_host<T>(g) ? k_grid_slide<T, W, true> : k_grid_slide<T, W, false>;
+  int per_sm = 0;
+  CG_CUDA(kernel_occupancy((const void*)kern, tc.warps * 32, tc.smem, &per_sm));
+  if (per_sm < 1) return CG_ERR_ARG;
+  static int sms = 0;
+  if (!sms) sms = sms_of_device();
+  const int blocks = std::min((tc.nitems + tc.warps - 1) / tc.warps, per_sm * sms);
+  CG_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(int), st));
+  kern<<<std::max(1, blocks), tc.warps * 32, tc.smem, st>>>(d_recs, d_hive_start, g, tc, d_fw,
+                                                            d_counter);
+  count_launches(1);
+  CG_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+}  // namespace
+
+template <typename T>
+int launch_grid_slide(const Rec<T>* d_recs, const int* d_hive_start, const Geom& g, T* d_fw,
+                      int* d_counter, cudaStream_t st, const TileTune* tt) {
+  SlideTile tc{};
+  if (!slide_tiling(g, sizeof(T), tt, tc)) return CG_ERR_ARG;
+  switch (g.kw) {
+    case 4: return launch_w<T, 4>(d_recs, d_hive_start, g, d_fw, d_counter, st, tc);
+    case 5: return launch_w<T, 5>(d_recs, d_hive_start, g, d_fw, d_counter, st, tc);
+    case 6: return launch_w<T, 6>(d_recs, d_hive_start, g, d_fw, d_counter, st, tc);
+    case 7: return launch_w<T, 7>(d_recs, d_hive_start, g, d_fw, d_counter, st, tc);
+    case 8: return launch_w<T, 8>(d_recs, d_hive_start, g, d_fw, d_counter, st, tc);
+    default: return CG_ERR_ARG;
+  }
+}
+
+template int launch_grid_slide<float>(const Rec<float>*, const int*, const Geom&, float*, int*,
+                                      cudaStream_t, const TileTune*);
+template int launch_grid_slide<double>(const Rec<double>*, const int*, const Geom&, double*, int*,
+                                       cudaStream_t, const TileTune*);
+
+}  // namespace cg

@@ -33,6 +33,13 @@ int launch_build_stream(const int* d_perm, int64_t M, const double* d_uvw, const
 constexpr int kGridDirect = 0;
 constexpr int kGridTiled = 1;
 constexpr int kGridMma = 2;  // tensor-core gridding (FP32, W <= 8); degridding uses tiled
+// x-sliding warp windows (cg_grid_slide.cu): tt->wy band rows (8/16/32),
+// tt->wpb hive columns per segment, tt->warps per CTA (0 = defaults).
+// CG_ERR_ARG when they do not apply (W outside 4..8, an axis not a multiple
+// of 8 cells, or a window that does not fit on an SM).
+template <typename T>
+int launch_grid_slide(const Rec<T>* d_recs, const int* d_hive_start, const Geom& g, T* d_fw,
+                      int* d_counter, cudaStream_t st, const TileTune* tt);
 int launch_grid_mma(const Rec<float>* d_recs, const int* d_hive_start, const Geom& g, float* d_fw,
                     cudaStream_t st);
 template <typename T>

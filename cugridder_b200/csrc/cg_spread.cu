@@ -713,11 +713,15 @@ int degrid_slots(const TileCfg& tc, int W) { return slots_for(tc.TY, tc.PB, W); 
 // Autotuner candidates.  Gridding warp tiles (x, y, planes, warps per CTA):
 // planes 64 = all planes of the grid; 0 = the default.  Degridding tiles
 // (x, y, planes, threads per CTA).  The first of each list is the default.
+// x = -1: the x-sliding windows (cg_grid_slide.cu) with y band rows, planes =
+// hive columns per segment.
 static const int kGridCand[][4] = {{16, 16, 0, 0},  {16, 8, 0, 0},   {16, 8, 64, 0},
                                    {16, 8, 64, 12}, {16, 16, 64, 0}, {32, 8, 0, 0},
                                    {16, 16, 5, 16}, {16, 16, 0, 12}, {16, 8, 10, 16},
                                    {16, 8, 13, 12}, {16, 16, 8, 10}, {16, 8, 64, 13},
-                                   {16, 8, 64, 14}};
+                                   {16, 8, 64, 14}, {-1, 8, 32, 0},  {-1, 8, 32, 12},
+                                   {-1, 8, 16, 0},  {-1, 8, 64, 0},  {-1, 16, 32, 0},
+                                   {-1, 8, 32, 10}};
 // threads -1 .. -4: the TMA-staged kernel's variants (all planes; 32 x 16
 // tiles with 512 threads and two stages / 256 threads and one stage; 32 x 8
 // and 16 x 8 tiles with 128 threads and one stage) where they apply.
@@ -803,6 +807,11 @@ static int grid_w(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, cons
     count_launches(1);
     CG_CUDA(cudaGetLastError());
     return CG_OK;
+  }
+  // x-sliding windows: a tuning candidate with wx < 0, or CG_GRID_SLIDE=1
+  if ((tt && tt->wx < 0) || env_int("CG_GRID_SLIDE", 0)) {
+    const int s = launch_grid_slide<T>(d_recs, d_hive_start, g, d_fw, d_counter, st, tt);
+    if (s != CG_ERR_ARG || (tt && tt->wx < 0)) return s;
   }
   WarpTile tc = warp_tiling<T>(g, tt);
   const bool exact = (g.nf1 % 8) != 0 || (g.nf2 % 8) != 0;
