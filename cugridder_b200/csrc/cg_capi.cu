@@ -125,6 +125,8 @@ void destroy_plan(cg_plan_s* P) {
   if (P->h_mm) cudaFreeHost(P->h_mm);
   if (P->io_stream) cudaStreamDestroy(P->io_stream);
   if (P->io_event) cudaEventDestroy(P->io_event);
+  if (P->io_ev_uvw) cudaEventDestroy(P->io_ev_uvw);
+  if (P->io_ev_main) cudaEventDestroy(P->io_ev_main);
   if (P->timer.created)
     for (int s = 0; s < 2; s++)
       for (int i = 0; i <= kMaxStages; i++) cudaEventDestroy(P->timer.ev[s][i]);
@@ -236,41 +238,53 @@ int host_call(bool to_dirty, int precision, int64_t nrow, int nx, int ny, double
   if (!P->io_stream) {
     CG_CUDA(cudaStreamCreateWithFlags(&P->io_stream, cudaStreamNonBlocking));
     CG_CUDA(cudaEventCreateWithFlags(&P->io_event, cudaEventDisableTiming));
+    CG_CUDA(cudaEventCreateWithFlags(&P->io_ev_uvw, cudaEventDisableTiming));
+    CG_CUDA(cudaEventCreateWithFlags(&P->io_ev_main, cudaEventDisableTiming));
   }
   cudaStream_t s2 = P->io_stream;
   // every return below leaves both streams idle (the host buffers may be
-  // reused as soon as the call returns) and the plan without the wait
+  // reused as soon as the call returns) and the plan without the waits
   struct Finish {
     cg_plan_s* P;
     ~Finish() {
       P->inputs_ready = nullptr;
+      P->main_ready = nullptr;
       cudaStreamSynchronize(P->io_stream);
       cudaStreamSynchronize(P->stream);
     }
   } finish{P};
   double* d_uvw = (double*)P->io_uvw.p;
-  // uvw first, on the plan's stream: the w range and the binning read it
+  // All copies on the second stream, one after the other at full bandwidth,
+  // in the order the stages need them: uvw (w range, binning), then the
+  // visibilities or the image (sorted stream / plane fill), then the weights.
+  // The binning runs while the rest is still arriving.
+  // (the previous call left both streams idle: see Finish)
   if (nrow > 0) {
     if (uvw_is_float) {
       float* d_f = (float*)(d_uvw + n_uvw);
-      CG_CUDA(cudaMemcpyAsync(d_f, uvw, n_uvw * 4, cudaMemcpyHostToDevice, s));
+      CG_CUDA(cudaMemcpyAsync(d_f, uvw, n_uvw * 4, cudaMemcpyHostToDevice, s2));
+      CG_CUDA(cudaEventRecord(P->io_ev_uvw, s2));
+      CG_CUDA(cudaStreamWaitEvent(s, P->io_ev_uvw, 0));
       k_widen_uvw<<<592, 256, 0, s>>>(d_f, d_uvw, (int64_t)n_uvw);
       cg::count_launches(1);
       CG_CUDA(cudaGetLastError());
     } else {
-      CG_CUDA(cudaMemcpyAsync(d_uvw, uvw, n_uvw * 8, cudaMemcpyHostToDevice, s));
+      CG_CUDA(cudaMemcpyAsync(d_uvw, uvw, n_uvw * 8, cudaMemcpyHostToDevice, s2));
+      CG_CUDA(cudaEventRecord(P->io_ev_uvw, s2));
+      CG_CUDA(cudaStreamWaitEvent(s, P->io_ev_uvw, 0));
     }
   }
-  // vis / wgt / dirty on the second stream, overlapping the w range and binning
-  if (nrow > 0 && wgt)
-    CG_CUDA(cudaMemcpyAsync(P->io_wgt.p, wgt, (size_t)nrow * tsz, cudaMemcpyHostToDevice, s2));
   if (to_dirty) {
     if (nrow > 0)
       CG_CUDA(cudaMemcpyAsync(P->io_vis.p, vis, (size_t)nrow * 2 * tsz, cudaMemcpyHostToDevice, s2));
   } else {
     CG_CUDA(cudaMemcpyAsync(P->io_dirty.p, dirty, (size_t)nx * ny * 2 * tsz, cudaMemcpyHostToDevice, s2));
   }
+  CG_CUDA(cudaEventRecord(P->io_ev_main, s2));
+  if (nrow > 0 && wgt)
+    CG_CUDA(cudaMemcpyAsync(P->io_wgt.p, wgt, (size_t)nrow * tsz, cudaMemcpyHostToDevice, s2));
   CG_CUDA(cudaEventRecord(P->io_event, s2));
+  P->main_ready = P->io_ev_main;
   P->inputs_ready = P->io_event;
   int rs;
   if (to_dirty) {

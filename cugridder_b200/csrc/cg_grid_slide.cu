@@ -115,7 +115,13 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
   C* fwc = reinterpret_cast<C*>(fw);
   const T beta = (T)g.beta, ces = (T)g.es_c, halfw = (T)W * (T)0.5;
 
-  const int band = item / tc.nsegs, seg = item - band * tc.nsegs;
+  // items are handed out from the grid's centre outward (bands, then the
+  // segments inside a band): uv data is densest around u = v = 0, the centre
+  // of the grid, so the heaviest items start first and the launch ends on
+  // light ones
+  const int kb = item / tc.nsegs, ks = item - kb * tc.nsegs;
+  const int band = tc.nbands / 2 + ((kb & 1) ? -((kb + 1) >> 1) : (kb >> 1));
+  const int seg = tc.nsegs / 2 + ((ks & 1) ? -((ks + 1) >> 1) : (ks >> 1));
   const int y0 = band * TY, y1 = min(y0 + TY, nf2), wy = y1 - y0;
   const int hs = seg * tc.SEG, he = min(hs + tc.SEG, nhx);
   const int hya = floordiv8(y0 - hi), hyb = floordiv8(y1 - 1 + lo);
@@ -333,14 +339,15 @@ int env_or(const char* name, int dflt) {
 }
 
 // Band rows, hive columns per segment and warps per CTA: the tuned values,
-// else CG_SLIDE_TY / CG_SLIDE_SEG / CG_SLIDE_WARPS, else 8 / 32 / as many as
-// fit.
+// else CG_SLIDE_TY / CG_SLIDE_SEG / CG_SLIDE_WARPS, else 8 / 8 / as many as
+// fit.  Short segments keep the densest items (around the grid centre) well
+// below a warp's share of the work; each costs one warm-up hive column.
 bool slide_tiling(const Geom& g, size_t tsz, const TileTune* tt, SlideTile& tc) {
   const int W = g.kw;
   if (W < 4 || W > 8 || (g.nf1 % 8) != 0 || (g.nf2 % 8) != 0 || g.nf1 < kXW) return false;
   int TY = (tt && tt->wy > 0 && tt->wx < 0) ? tt->wy : env_or("CG_SLIDE_TY", 8);
   if (TY != 8 && TY != 16 && TY != 32) return false;
-  int SEG = (tt && tt->wpb > 0 && tt->wx < 0) ? tt->wpb : env_or("CG_SLIDE_SEG", 32);
+  int SEG = (tt && tt->wpb > 0 && tt->wx < 0) ? tt->wpb : env_or("CG_SLIDE_SEG", 8);
   SEG = std::max(1, std::min(SEG, g.nhx));
   tc.TY = TY;
   tc.logTY = TY == 8 ? 3 : (TY == 16 ? 4 : 5);

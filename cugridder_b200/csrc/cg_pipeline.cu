@@ -805,9 +805,11 @@ static int autotune_launch(cg_plan_s* P, int dir, T* d_vis) {
   return CG_OK;
 }
 
-// host entry points: wait for the inputs copied on the second stream
-static int wait_inputs(cg_plan_s* P) {
-  if (P->inputs_ready) CG_CUDA(cudaStreamWaitEvent(P->stream, P->inputs_ready, 0));
+// host entry points: wait for the inputs copied on the second stream (all
+// of them; or, main_only, the visibilities / the image)
+static int wait_inputs(cg_plan_s* P, bool main_only = false) {
+  cudaEvent_t e = main_only && P->main_ready ? P->main_ready : P->inputs_ready;
+  if (e) CG_CUDA(cudaStreamWaitEvent(P->stream, e, 0));
   return CG_OK;
 }
 
@@ -878,7 +880,7 @@ static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const
                       (int*)P->hive_start.p + (nh_of(g) + 1)));
   timer_mark(P);  // 2: binning
   if (P->stop_stage == 1) return CG_OK;
-  CG_TRY(wait_inputs(P));
+  CG_TRY(wait_inputs(P, P->plane_batch == 0));  // the image (the weights before the stream)
   if (P->plane_batch) {  // memory-limited mode: fill, FFT and degridding per plane window
     CG_TRY(launch_build_stream<T>((const int*)P->perm.p, M, d_uvw, (const T*)nullptr, d_wgt, g,
                                   false, (Rec<T>*)P->recs_tmp.p, (Rec<T>*)P->recs.p, st));
@@ -893,6 +895,7 @@ static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const
   CG_TRY(fft_exec_pruned(P, P->grid.p, CUFFT_FORWARD));
   timer_mark(P);  // 4: FFT
   if (P->stop_stage == 3) return CG_OK;
+  CG_TRY(wait_inputs(P));  // the weights
   CG_TRY(launch_build_stream<T>((const int*)P->perm.p, M, d_uvw, (const T*)nullptr, d_wgt, g,
                                 false, (Rec<T>*)P->recs_tmp.p, (Rec<T>*)P->recs.p, st));
   timer_mark(P);  // 5: sorted stream

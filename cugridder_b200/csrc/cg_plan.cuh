@@ -95,12 +95,15 @@ struct cg_plan_s {
   bool fft1_valid = false;
   int fft1_nf1 = 0, fft1_nf2 = 0;
   cg_stage_timer timer;
-  // host entry points: inputs the first stages do not read are copied on
-  // io_stream; a call waits on inputs_ready (when set) before the first stage
-  // that reads vis, wgt or the dirty image
+  // host entry points: every input is copied on io_stream, one copy after the
+  // other in the order the stages need them (uvw, then the visibilities or
+  // the image, then the weights), each at the link's full bandwidth; the
+  // plan's stream waits for uvw before the w range, on main_ready (when set)
+  // before the first stage that reads the visibilities or the image, and on
+  // inputs_ready (when set) before the first stage that reads the weights
   cudaStream_t io_stream = nullptr;
-  cudaEvent_t io_event = nullptr;
-  cudaEvent_t inputs_ready = nullptr;
+  cudaEvent_t io_event = nullptr, io_ev_uvw = nullptr, io_ev_main = nullptr;
+  cudaEvent_t inputs_ready = nullptr, main_ready = nullptr;
   std::mutex mu;
 };
 
