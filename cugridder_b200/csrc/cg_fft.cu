@@ -300,15 +300,21 @@ __device__ __forceinline__ void fft_regs(float2 (&a)[16], float2 (&b)[16], int s
 // one CTA.
 //
 // Rows [mid0, mid1) of every column are outside the image (the CMCL map
-// reaches rows [0, mid0) and [mid1, L) only): with skip = 1 they are zero on
-// input (the plane fill wrote zeros there) and are not loaded; with skip = 2
-// nothing reads them afterwards (the w-DFT) and they are not stored.
+// reaches rows [0, mid0) and [mid1, L) only), and rows outside [b0, b1) are
+// outside the band of rows the row transforms cover.  skip is a set of flags:
+//   1: rows outside the image are zero on input (the plane fill wrote zeros
+//      there): not loaded;
+//   2: nothing reads rows outside the image afterwards (the w-DFT): not stored;
+//   4: rows outside the band are zero on input (the grid holds no data there
+//      and the row transforms did not touch them): not loaded;
+//   8: nothing reads rows outside the band afterwards (the row transforms and
+//      the degridding stay inside it): not stored.
 template <int L>
 __global__ void __launch_bounds__(L / 16) k_col_fft_reg(float2* __restrict__ grid, int nf1,
                                                         size_t plane, int nplanes, int c0a,
                                                         int na, int c0b, int nb, int sign,
                                                         const float2* __restrict__ tw, int mid0,
-                                                        int mid1, int skip) {
+                                                        int mid1, int skip, int b0, int b1) {
   constexpr int T = L / 16;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* pre = reinterpret_cast<float4*>(smem_raw);                       // L rows x 2 columns
@@ -322,12 +328,18 @@ __global__ void __launch_bounds__(L / 16) k_col_fft_reg(float2* __restrict__ gri
     return grid + (size_t)p * plane + col0;
   };
   auto outside = [&](int row) { return row >= mid0 && row < mid1; };
+  auto no_load = [&](int row) {
+    return ((skip & 1) && outside(row)) || ((skip & 4) && (row < b0 || row >= b1));
+  };
+  auto no_store = [&](int row) {
+    return ((skip & 2) && outside(row)) || ((skip & 8) && (row < b0 || row >= b1));
+  };
   auto prefetch = [&](int64_t it) {
     const float2* b = base_of(it);
 #pragma unroll
     for (int m = 0; m < 16; m++) {
       const int row = t + m * T;
-      if (skip == 1 && outside(row)) continue;  // zero rows: not loaded
+      if (no_load(row)) continue;  // zero rows: not loaded
       const unsigned dst = (unsigned)__cvta_generic_to_shared(pre + row);
       const float2* src = b + (size_t)row * nf1;
       asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
@@ -343,7 +355,7 @@ __global__ void __launch_bounds__(L / 16) k_col_fft_reg(float2* __restrict__ gri
 #pragma unroll
     for (int m = 0; m < 16; m++) {
       const int row = t + m * T;
-      const float4 v = (skip == 1 && outside(row)) ? make_float4(0.f, 0.f, 0.f, 0.f) : pre[row];
+      const float4 v = no_load(row) ? make_float4(0.f, 0.f, 0.f, 0.f) : pre[row];
       a[m] = make_float2(v.x, v.y);
       b[m] = make_float2(v.z, v.w);
     }
@@ -354,7 +366,7 @@ __global__ void __launch_bounds__(L / 16) k_col_fft_reg(float2* __restrict__ gri
 #pragma unroll
     for (int m = 0; m < 16; m++) {
       const int row = t + m * T;
-      if (skip == 2 && outside(row)) continue;  // rows nothing reads
+      if (no_store(row)) continue;  // rows nothing reads
       *reinterpret_cast<float4*>(bs + (size_t)row * nf1) =
           make_float4(a[m].x, a[m].y, b[m].x, b[m].y);
     }
@@ -756,7 +768,8 @@ int launch_row(float2* grid, size_t plane, int nplanes, int r0, int nrows, int s
 
 template <int L>
 int launch_reg(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, int c0b, int nb,
-               int sign, const float2* tw, cudaStream_t st, int mid0, int mid1, int skip) {
+               int sign, const float2* tw, cudaStream_t st, int mid0, int mid1, int skip, int b0,
+               int b1) {
   const size_t smem = (size_t)L * sizeof(float4) + (size_t)(pad16(L) + 16) * sizeof(float2);
   int per_sm = 0;
   CG_CUDA(kernel_occupancy((const void*)k_col_fft_reg<L>, L / 16, smem, &per_sm));
@@ -770,7 +783,7 @@ int launch_reg(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na
   const int64_t items = (int64_t)(na / 2 + nb / 2) * nplanes;
   const int blocks = (int)std::min<int64_t>(items, (int64_t)per_sm * sms);
   k_col_fft_reg<L><<<blocks, L / 16, smem, st>>>(grid, nf1, plane, nplanes, c0a, na, c0b, nb,
-                                                 sign, tw, mid0, mid1, skip);
+                                                 sign, tw, mid0, mid1, skip, b0, b1);
   count_launches(1);
   CG_CUDA(cudaGetLastError());
   return CG_OK;
@@ -809,7 +822,8 @@ int launch_lc(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na,
 
 template <int L>
 int launch_l(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, int c0b, int nb,
-             int sign, const float2* tw, cudaStream_t st, int mid0, int mid1, int skip) {
+             int sign, const float2* tw, cudaStream_t st, int mid0, int mid1, int skip, int b0,
+             int b1) {
   // CG_COL_FFT_REG=0: the shared-memory-resident kernel instead of the register-resident one
   const char* e = getenv("CG_COL_FFT_REG");
   const int reg = e ? atoi(e) : 1;
@@ -818,7 +832,7 @@ int launch_l(float2* grid, int nf1, size_t plane, int nplanes, int c0a, int na, 
   if (reg == 2) return launch_reg2<L>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st);
   if (reg != 0)
     return launch_reg<L>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st, mid0, mid1,
-                         skip);
+                         skip, b0, b1);
   return col_fft_cb(L) == 1
              ? launch_lc<L, 1>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st)
              : launch_lc<L, 2>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, tw, st);
@@ -1050,10 +1064,11 @@ int make_col_fft_twiddles(int L, float2* d_tw, cudaStream_t st) {
 // of nplanes planes (row stride nf1, plane stride `plane` elements), length L.
 int launch_col_fft(float2* grid, int L, int nf1, size_t plane, int nplanes, int c0a, int na,
                    int c0b, int nb, int sign, const float2* d_tw, cudaStream_t st, int mid0,
-                   int mid1, int skip) {
-  if (skip != 0 && !(0 <= mid0 && mid0 <= mid1 && mid1 <= L)) skip = 0;
+                   int mid1, int skip, int b0, int b1) {
+  if ((skip & 3) != 0 && !(0 <= mid0 && mid0 <= mid1 && mid1 <= L)) skip &= ~3;
+  if ((skip & 12) != 0 && !(0 <= b0 && b0 <= b1 && b1 <= L)) skip &= ~12;
 #define CG_COL_CALL(l) \
-  launch_l<l>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, d_tw, st, mid0, mid1, skip)
+  launch_l<l>(grid, nf1, plane, nplanes, c0a, na, c0b, nb, sign, d_tw, st, mid0, mid1, skip, b0, b1)
   switch (L) {
     case 1024: return CG_COL_CALL(1024);
     case 2048: return CG_COL_CALL(2048);

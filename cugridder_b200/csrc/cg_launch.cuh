@@ -130,11 +130,13 @@ int launch_col_fft_four_step(float2* grid, int L, int nf1, size_t plane, int npl
 // elements [mid0, mid1) skipped as for launch_col_fft.
 int launch_row_fft(float2* grid, int L, size_t plane, int nplanes, int r0, int nrows, int sign,
                    const float2* d_tw, cudaStream_t st, int mid0 = 0, int mid1 = 0, int skip = 0);
-// Rows [mid0, mid1) of the columns: skip 1 = zero on input (not loaded),
-// 2 = unused on output (not stored), 0 = transformed like the others.
+// Flags of skip (the default register-resident kernel; the other variants
+// transform every row): rows [mid0, mid1) of the columns zero on input (1:
+// not loaded) or unused on output (2: not stored); rows outside [b0, b1)
+// zero on input (4) or unused on output (8).
 int launch_col_fft(float2* grid, int L, int nf1, size_t plane, int nplanes, int c0a, int na,
                    int c0b, int nb, int sign, const float2* d_tw, cudaStream_t st, int mid0 = 0,
-                   int mid1 = 0, int skip = 0);
+                   int mid1 = 0, int skip = 0, int b0 = 0, int b1 = 0);
 
 // ---- memory-limited mode: plane windows [p0, p1) (cg_spread.cu, cg_wstage.cu) ----
 template <typename T>

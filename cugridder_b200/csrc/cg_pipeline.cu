@@ -644,12 +644,16 @@ static int fft_exec_pruned(cg_plan_s* P, void* d_grid, int direction) {
     }
     // image rows of a column under the CMCL map: [0, N2 - N2/2) and [nf2 - N2/2, nf2);
     // the rows between are zero before the forward transform (plane fill)
-    // and unread after the inverse one (w-DFT)
+    // and unread after the inverse one (w-DFT).  Rows outside the band of
+    // the row transforms, [r0, r0 + batch), are zero before the inverse
+    // transform (gridding wrote zeros, the row pass left them) and unread
+    // after the forward one (row pass and degridding stay in the band).
     const int mid0 = g.N2 - g.N2 / 2, mid1 = g.nf2 - g.N2 / 2;
     auto all_cols = [&]() {
       return launch_col_fft((float2*)d_grid, g.nf2, g.nf1, plane, g.nw, 0, half, g.nf1 - half, half,
                             direction == CUFFT_INVERSE ? 1 : -1, (const float2*)P->coltw.p,
-                            P->stream, mid0, mid1, direction == CUFFT_INVERSE ? 2 : 1);
+                            P->stream, mid0, mid1, direction == CUFFT_INVERSE ? (2 | 4) : (1 | 8),
+                            r0, r0 + batch);
     };
     // rows by cuFFT, or (CG_ROW_FFT=1, slower on B200) by the register-resident
     // row kernel on square grids (the same twiddles), which skips the columns
