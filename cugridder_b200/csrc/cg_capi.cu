@@ -13,7 +13,10 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <limits>
+#include <sched.h>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "cg_plan.cuh"
@@ -125,6 +128,9 @@ void destroy_plan(cg_plan_s* P) {
   if (P->h_mm) cudaFreeHost(P->h_mm);
   if (P->io_stream) cudaStreamDestroy(P->io_stream);
   if (P->io_event) cudaEventDestroy(P->io_event);
+  if (P->aux_stream) cudaStreamDestroy(P->aux_stream);
+  if (P->aux_ev0) cudaEventDestroy(P->aux_ev0);
+  if (P->aux_ev1) cudaEventDestroy(P->aux_ev1);
   if (P->io_ev_uvw) cudaEventDestroy(P->io_ev_uvw);
   if (P->io_ev_main) cudaEventDestroy(P->io_ev_main);
   if (P->timer.created)
@@ -212,6 +218,71 @@ int expand_channels(cg_plan_s* P, int64_t nrow, int nchan, const double* freqs,
   return CG_OK;
 }
 
+// order-preserving integer key of a double (the device's ordered_key)
+unsigned long long ordered_key_host(double x) {
+  unsigned long long b;
+  memcpy(&b, &x, sizeof(b));
+  return (b & 0x8000000000000000ULL) ? ~b : (b | 0x8000000000000000ULL);
+}
+
+// The u, v, w ranges and the non-finite flag of the caller's uvw ([nrow][3],
+// float or double) computed on the host, in the layout launch_wminmax writes
+// (order-preserving keys of u_min, u_max, v_min, v_max, w_min, w_max, then
+// the flag): min and max are exact, so the values equal the device pass's.
+// Threads split the rows; it runs while the DMA engine copies the inputs.
+template <typename F>
+void scan_uvw_host(const F* uvw, int64_t nrow, unsigned long long out[7]) {
+  struct Part {
+    double lo[3], hi[3];
+    int bad;
+  };
+  // Branch-free compares (a NaN never replaces a bound, as fmin/fmax) and
+  // one running sum of x - x, which is NaN as soon as any x is not finite:
+  // this loop vectorizes, where fmin / isfinite per element do not.
+  auto scan = [&](int64_t r0, int64_t r1, Part& p) {
+    double lo0 = std::numeric_limits<double>::max(), lo1 = lo0, lo2 = lo0;
+    double hi0 = -lo0, hi1 = -lo0, hi2 = -lo0, acc = 0.0;
+    for (int64_t i = r0; i < r1; i++) {
+      const double x0 = (double)uvw[3 * i], x1 = (double)uvw[3 * i + 1], x2 = (double)uvw[3 * i + 2];
+      acc += (x0 - x0) + (x1 - x1) + (x2 - x2);
+      lo0 = x0 < lo0 ? x0 : lo0;
+      hi0 = x0 > hi0 ? x0 : hi0;
+      lo1 = x1 < lo1 ? x1 : lo1;
+      hi1 = x1 > hi1 ? x1 : hi1;
+      lo2 = x2 < lo2 ? x2 : lo2;
+      hi2 = x2 > hi2 ? x2 : hi2;
+    }
+    p.lo[0] = lo0; p.lo[1] = lo1; p.lo[2] = lo2;
+    p.hi[0] = hi0; p.hi[1] = hi1; p.hi[2] = hi2;
+    p.bad = !(acc == 0.0);
+  };
+  int ncpu = 1;
+  {
+    cpu_set_t cs;
+    if (sched_getaffinity(0, sizeof(cs), &cs) == 0) ncpu = std::max(1, CPU_COUNT(&cs));
+  }
+  const int nt = nrow < (1 << 20) ? 1 : std::min(16, ncpu);
+  std::vector<Part> parts(nt);
+  std::vector<std::thread> th;
+  for (int t = 1; t < nt; t++)
+    th.emplace_back(scan, nrow * t / nt, nrow * (t + 1) / nt, std::ref(parts[t]));
+  scan(0, nrow / nt, parts[0]);
+  for (auto& x : th) x.join();
+  Part r = parts[0];
+  for (int t = 1; t < nt; t++) {
+    for (int a = 0; a < 3; a++) {
+      r.lo[a] = parts[t].lo[a] < r.lo[a] ? parts[t].lo[a] : r.lo[a];
+      r.hi[a] = parts[t].hi[a] > r.hi[a] ? parts[t].hi[a] : r.hi[a];
+    }
+    r.bad |= parts[t].bad;
+  }
+  for (int a = 0; a < 3; a++) {
+    out[2 * a] = nrow > 0 ? ordered_key_host(r.lo[a]) : ~0ULL;
+    out[2 * a + 1] = nrow > 0 ? ordered_key_host(r.hi[a]) : 0ULL;
+  }
+  out[6] = (unsigned long long)(r.bad ? 1 : 0);
+}
+
 // Host-pointer driver shared by every host entry point.
 // uvw_is_float: uvw given in float (reference -DSINGLE API), widened on device.
 int host_call(bool to_dirty, int precision, int64_t nrow, int nx, int ny, double fov,
@@ -237,55 +308,78 @@ int host_call(bool to_dirty, int precision, int64_t nrow, int nx, int ny, double
   cudaStream_t s = P->stream;
   if (!P->io_stream) {
     CG_CUDA(cudaStreamCreateWithFlags(&P->io_stream, cudaStreamNonBlocking));
+    CG_CUDA(cudaStreamCreateWithFlags(&P->aux_stream, cudaStreamNonBlocking));
     CG_CUDA(cudaEventCreateWithFlags(&P->io_event, cudaEventDisableTiming));
     CG_CUDA(cudaEventCreateWithFlags(&P->io_ev_uvw, cudaEventDisableTiming));
     CG_CUDA(cudaEventCreateWithFlags(&P->io_ev_main, cudaEventDisableTiming));
+    CG_CUDA(cudaEventCreateWithFlags(&P->aux_ev0, cudaEventDisableTiming));
+    CG_CUDA(cudaEventCreateWithFlags(&P->aux_ev1, cudaEventDisableTiming));
   }
   cudaStream_t s2 = P->io_stream;
-  // every return below leaves both streams idle (the host buffers may be
+  // every return below leaves all streams idle (the host buffers may be
   // reused as soon as the call returns) and the plan without the waits
   struct Finish {
     cg_plan_s* P;
     ~Finish() {
       P->inputs_ready = nullptr;
       P->main_ready = nullptr;
+      P->uvw_ready = nullptr;
+      P->host_mm = nullptr;
       cudaStreamSynchronize(P->io_stream);
+      cudaStreamSynchronize(P->aux_stream);
       cudaStreamSynchronize(P->stream);
     }
   } finish{P};
   double* d_uvw = (double*)P->io_uvw.p;
   // All copies on the second stream, one after the other at full bandwidth,
-  // in the order the stages need them: uvw (w range, binning), then the
-  // visibilities or the image (sorted stream / plane fill), then the weights.
-  // The binning runs while the rest is still arriving.
-  // (the previous call left both streams idle: see Finish)
-  if (nrow > 0) {
+  // in the order the stages need them.  ms2dirty: uvw (binning), then the
+  // visibilities and the weights (sorted stream), so the binning runs while
+  // they arrive.  dirty2ms: the image first (plane fill and FFT, which need
+  // nothing else), then uvw (binning), then the weights (sorted stream).
+  // (The previous call left every stream idle: see Finish.)
+  auto copy_uvw = [&]() -> int {
+    if (nrow <= 0) return CG_OK;
     if (uvw_is_float) {
       float* d_f = (float*)(d_uvw + n_uvw);
       CG_CUDA(cudaMemcpyAsync(d_f, uvw, n_uvw * 4, cudaMemcpyHostToDevice, s2));
-      CG_CUDA(cudaEventRecord(P->io_ev_uvw, s2));
-      CG_CUDA(cudaStreamWaitEvent(s, P->io_ev_uvw, 0));
-      k_widen_uvw<<<592, 256, 0, s>>>(d_f, d_uvw, (int64_t)n_uvw);
+      k_widen_uvw<<<592, 256, 0, s2>>>(d_f, d_uvw, (int64_t)n_uvw);
       cg::count_launches(1);
       CG_CUDA(cudaGetLastError());
     } else {
       CG_CUDA(cudaMemcpyAsync(d_uvw, uvw, n_uvw * 8, cudaMemcpyHostToDevice, s2));
-      CG_CUDA(cudaEventRecord(P->io_ev_uvw, s2));
-      CG_CUDA(cudaStreamWaitEvent(s, P->io_ev_uvw, 0));
     }
-  }
+    CG_CUDA(cudaEventRecord(P->io_ev_uvw, s2));
+    return CG_OK;
+  };
   if (to_dirty) {
+    CG_TRY(copy_uvw());
     if (nrow > 0)
       CG_CUDA(cudaMemcpyAsync(P->io_vis.p, vis, (size_t)nrow * 2 * tsz, cudaMemcpyHostToDevice, s2));
+    CG_CUDA(cudaEventRecord(P->io_ev_main, s2));
   } else {
     CG_CUDA(cudaMemcpyAsync(P->io_dirty.p, dirty, (size_t)nx * ny * 2 * tsz, cudaMemcpyHostToDevice, s2));
+    CG_CUDA(cudaEventRecord(P->io_ev_main, s2));
+    CG_TRY(copy_uvw());
   }
-  CG_CUDA(cudaEventRecord(P->io_ev_main, s2));
   if (nrow > 0 && wgt)
     CG_CUDA(cudaMemcpyAsync(P->io_wgt.p, wgt, (size_t)nrow * tsz, cudaMemcpyHostToDevice, s2));
   CG_CUDA(cudaEventRecord(P->io_event, s2));
   P->main_ready = P->io_ev_main;
   P->inputs_ready = P->io_event;
+  P->uvw_ready = nrow > 0 ? P->io_ev_uvw : nullptr;
+  // dirty2ms: the u/v/w ranges from the caller's uvw while the copies run,
+  // so the geometry is known before uvw is in and the plane fill and FFT
+  // start as soon as the image is (ms2dirty gains nothing from it: its
+  // binning waits for uvw anyway and is done before the visibilities are in)
+  unsigned long long host_mm[7];
+  const char* hr = getenv("CG_HOST_RANGES");  // 0: the device range pass instead (A/B timing)
+  if (!to_dirty && !(hr && atoi(hr) == 0)) {
+    if (uvw_is_float)
+      scan_uvw_host((const float*)uvw, nrow, host_mm);
+    else
+      scan_uvw_host((const double*)uvw, nrow, host_mm);
+    P->host_mm = host_mm;
+  }
   int rs;
   if (to_dirty) {
     rs = cg::ms2dirty_device(P, nrow, freq, d_uvw, P->io_vis.p, wgt ? P->io_wgt.p : nullptr,

@@ -390,9 +390,17 @@ static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw)
   if (!P->h_mm) CG_CUDA(cudaMallocHost(&P->h_mm, 128));
   unsigned long long* d_mm = (unsigned long long*)P->mm.p;
   int* d_bad = (int*)(d_mm + 6);
-  CG_TRY(launch_wminmax(d_uvw, nrow, d_mm, d_bad, st));
-  CG_CUDA(cudaMemcpyAsync(P->h_mm, d_mm, 80, cudaMemcpyDeviceToHost, st));
-  CG_CUDA(cudaStreamSynchronize(st));
+  if (P->host_mm) {
+    // ranges computed on the host from the caller's uvw: no device pass, no
+    // synchronization (host entry points, which check the TMA status per call)
+    memcpy(P->h_mm, P->host_mm, 7 * sizeof(unsigned long long));
+    ((int*)P->h_mm)[18] = 0;
+  } else {
+    if (P->uvw_ready) CG_CUDA(cudaStreamWaitEvent(st, P->uvw_ready, 0));
+    CG_TRY(launch_wminmax(d_uvw, nrow, d_mm, d_bad, st));
+    CG_CUDA(cudaMemcpyAsync(P->h_mm, d_mm, 80, cudaMemcpyDeviceToHost, st));
+    CG_CUDA(cudaStreamSynchronize(st));
+  }
   timer_flush(P, P->timer.cur ^ 1);
   if (P->tma_armed && ((const int*)P->h_mm)[18]) {  // word 72: a TMA staging wait ran out
     // only a call captured into a CUDA graph (or one whose status was not
@@ -816,6 +824,11 @@ static int wait_inputs(cg_plan_s* P, bool main_only = false) {
   if (e) CG_CUDA(cudaStreamWaitEvent(P->stream, e, 0));
   return CG_OK;
 }
+// host entry points: wait for uvw (before the binning)
+static int wait_uvw(cg_plan_s* P) {
+  if (P->uvw_ready) CG_CUDA(cudaStreamWaitEvent(P->stream, P->uvw_ready, 0));
+  return CG_OK;
+}
 
 // the stages after gridding: FFT, then w-DFT with the corrections
 template <typename T>
@@ -842,10 +855,12 @@ static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T
   timer_mark(P);  // stage 0: w range + geometry
   if (!reuse) CG_TRY(launch_quarter(g, P->quad, (double*)P->K3q.p, (double*)P->zq.p, st));
   timer_mark(P);  // 1: quarter tables
-  if (!reuse)
+  if (!reuse) {
+    CG_TRY(wait_uvw(P));
     CG_TRY(launch_bin(d_uvw, M, g, P->key_bytes, P->binws.p, P->binws.cap, (int*)P->perm.p,
                       P->skeys.p, (int*)P->hive_start.p, st,
                       (int*)P->hive_start.p + (nh_of(g) + 1)));
+  }
   timer_mark(P);  // 2: binning
   if (P->stop_stage == 1) return CG_OK;
   CG_TRY(wait_inputs(P));
@@ -878,10 +893,41 @@ static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const
   timer_mark(P);  // stage 0: w range + geometry
   if (!reuse) CG_TRY(launch_quarter(g, P->quad, (double*)P->K3q.p, (double*)P->zq.p, st));
   timer_mark(P);  // 1: quarter tables
-  if (!reuse)
+  // Host entry points whose ranges came from the host: the plane fill and
+  // the FFT need only the image and the geometry, so they run on aux_stream
+  // as soon as the image is in, while this stream waits for uvw, bins the
+  // rows and builds the stream; degridding waits for both.
+  if (P->host_mm && P->main_ready && P->aux_stream && !P->plane_batch && !P->stop_stage &&
+      !P->timer.on && part == 0 && !reuse) {
+    CG_CUDA(cudaEventRecord(P->aux_ev0, st));  // the quarter tables
+    CG_CUDA(cudaStreamWaitEvent(P->aux_stream, P->aux_ev0, 0));
+    CG_CUDA(cudaStreamWaitEvent(P->aux_stream, P->main_ready, 0));  // the image
+    P->stream = P->aux_stream;  // the FFT helpers launch on P->stream
+    int rc = launch_plane_fill<T>(d_dirty, g, (const double*)P->K1.p, (const double*)P->K2.p,
+                                  (const double*)P->K3q.p, (const double*)P->zq.p, (T*)P->grid.p,
+                                  P->aux_stream);
+    if (rc == CG_OK) rc = fft_exec_pruned(P, P->grid.p, CUFFT_FORWARD);
+    P->stream = st;
+    CG_TRY(rc);
+    CG_CUDA(cudaEventRecord(P->aux_ev1, P->aux_stream));
+    CG_TRY(wait_uvw(P));
     CG_TRY(launch_bin(d_uvw, M, g, P->key_bytes, P->binws.p, P->binws.cap, (int*)P->perm.p,
                       P->skeys.p, (int*)P->hive_start.p, st,
                       (int*)P->hive_start.p + (nh_of(g) + 1)));
+    CG_TRY(wait_inputs(P));  // the weights
+    CG_TRY(launch_build_stream<T>((const int*)P->perm.p, M, d_uvw, (const T*)nullptr, d_wgt, g,
+                                  false, (Rec<T>*)P->recs_tmp.p, (Rec<T>*)P->recs.p, st));
+    CG_CUDA(cudaStreamWaitEvent(st, P->aux_ev1, 0));  // the transformed grid
+    CG_TRY(autotune_launch<T>(P, 1, d_vis));
+    CG_TRY(degrid_dispatch<T>(P, P->tune, d_vis));
+    return CG_OK;
+  }
+  if (!reuse) {
+    CG_TRY(wait_uvw(P));
+    CG_TRY(launch_bin(d_uvw, M, g, P->key_bytes, P->binws.p, P->binws.cap, (int*)P->perm.p,
+                      P->skeys.p, (int*)P->hive_start.p, st,
+                      (int*)P->hive_start.p + (nh_of(g) + 1)));
+  }
   timer_mark(P);  // 2: binning
   if (P->stop_stage == 1) return CG_OK;
   CG_TRY(wait_inputs(P, P->plane_batch == 0));  // the image (the weights before the stream)

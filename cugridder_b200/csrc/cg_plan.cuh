@@ -104,6 +104,16 @@ struct cg_plan_s {
   cudaStream_t io_stream = nullptr;
   cudaEvent_t io_event = nullptr, io_ev_uvw = nullptr, io_ev_main = nullptr;
   cudaEvent_t inputs_ready = nullptr, main_ready = nullptr;
+  // uvw_ready (when set): the plan's stream waits on it before the first
+  // stage that reads uvw.  host_mm (when set): the u/v/w range words and the
+  // non-finite flag, computed on the host from the caller's uvw (the layout
+  // of launch_wminmax's output), so prepare() needs no device pass and no
+  // synchronization.  With both, dirty2ms runs the plane fill and the FFT on
+  // aux_stream as soon as the image is in, concurrently with the binning.
+  cudaEvent_t uvw_ready = nullptr;
+  const unsigned long long* host_mm = nullptr;
+  cudaStream_t aux_stream = nullptr;
+  cudaEvent_t aux_ev0 = nullptr, aux_ev1 = nullptr;
   std::mutex mu;
 };
 
