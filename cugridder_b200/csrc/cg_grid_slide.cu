@@ -50,6 +50,7 @@ struct SlideTile {
   int nslots;          // (hive rows of a band's halo) x nw
   int nbands, nsegs, nitems;
   int warps;
+  size_t stage_off;  // byte offset of the candidate / kernel-value staging in a warp's region
   size_t warp_bytes, smem;
 };
 
@@ -97,6 +98,61 @@ __device__ __forceinline__ void zero_region(T* __restrict__ fw, const Geom& g, i
   }
 }
 
+// per-lane candidate slot of the staging area: float: (f0, f1, f2, c0),
+// (c1, ox, oy, oz) as two 16-byte words; double: four 16-byte words
+template <typename T>
+constexpr int kCandBytes = sizeof(T) == 4 ? 32 : 64;
+
+template <typename T>
+__device__ __forceinline__ void stage_cand(unsigned char* stg, int lane, T f0, T f1, T f2, T c0,
+                                           T c1, int ox, int oy, int oz) {
+  if constexpr (sizeof(T) == 4) {
+    float4* c = reinterpret_cast<float4*>(stg) + 2 * lane;
+    c[0] = make_float4(f0, f1, f2, c0);
+    c[1] = make_float4(c1, __int_as_float(ox), __int_as_float(oy), __int_as_float(oz));
+  } else {
+    double2* c = reinterpret_cast<double2*>(stg) + 4 * lane;
+    c[0] = make_double2(f0, f1);
+    c[1] = make_double2(f2, c0);
+    c[2] = make_double2(c1, 0.0);
+    reinterpret_cast<int4*>(c + 3)[0] = make_int4(ox, oy, oz, 0);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void read_cand(const unsigned char* stg, int src, T& f0, T& f1, T& f2,
+                                          T& c0, T& c1, int& ox, int& oy, int& oz) {
+  if constexpr (sizeof(T) == 4) {
+    const float4* c = reinterpret_cast<const float4*>(stg) + 2 * src;
+    const float4 a = c[0], b = c[1];
+    f0 = a.x; f1 = a.y; f2 = a.z; c0 = a.w; c1 = b.x;
+    ox = __float_as_int(b.y); oy = __float_as_int(b.z); oz = __float_as_int(b.w);
+  } else {
+    const double2* c = reinterpret_cast<const double2*>(stg) + 4 * src;
+    const double2 a = c[0], b = c[1], d = c[2];
+    const int4 o = reinterpret_cast<const int4*>(c + 3)[0];
+    f0 = a.x; f1 = a.y; f2 = b.x; c0 = b.y; c1 = d.x;
+    ox = o.x; oy = o.y; oz = o.z;
+  }
+}
+
+// the x kernel values kvs[0 .. 7] (W <= 8) with 16-byte broadcast loads
+template <typename T>
+__device__ __forceinline__ void read_kx(const T* kvs, T (&kx)[8]) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 a = reinterpret_cast<const float4*>(kvs)[0], b = reinterpret_cast<const float4*>(kvs)[1];
+    kx[0] = a.x; kx[1] = a.y; kx[2] = a.z; kx[3] = a.w;
+    kx[4] = b.x; kx[5] = b.y; kx[6] = b.z; kx[7] = b.w;
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const double2 v = reinterpret_cast<const double2*>(kvs)[q];
+      kx[2 * q] = v.x;
+      kx[2 * q + 1] = v.y;
+    }
+  }
+}
+
 template <typename T, int W, bool kPoly>
 __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
                                            const int* __restrict__ hive_start, const Geom& g,
@@ -111,6 +167,12 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
   int* t_start = reinterpret_cast<int*>(wsmem + (size_t)TY * RS * sizeof(C));
   int* t_pref = t_start + tc.nslots;      // nslots + 1
   int* t_shy = t_pref + tc.nslots + 1;
+  // staging of the current chunk's candidates (one 32- or 64-byte slot per
+  // lane) and of the current row's kernel values: every lane reads them with
+  // broadcast loads, where register shuffles took one crossbar operation per
+  // value
+  unsigned char* stg = wsmem + tc.stage_off;
+  T* kvs = reinterpret_cast<T*>(stg + 32 * kCandBytes<T>);
   const size_t plane = (size_t)nf1 * nf2;
   C* fwc = reinterpret_cast<C*>(fw);
   const T beta = (T)g.beta, ces = (T)g.es_c, halfw = (T)W * (T)0.5;
@@ -121,6 +183,7 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
   // light ones
   const int kb = item / tc.nsegs, ks = item - kb * tc.nsegs;
   const int band = tc.nbands / 2 + ((kb & 1) ? -((kb + 1) >> 1) : (kb >> 1));
+  const int lane_dq = lane / W, lane_dz = lane - lane_dq * W;  // pair offsets of round 0
   const int seg = tc.nsegs / 2 + ((ks & 1) ? -((ks + 1) >> 1) : (ks >> 1));
   const int y0 = band * TY, y1 = min(y0 + TY, nf2), wy = y1 - y0;
   const int hs = seg * tc.SEG, he = min(hs + tc.SEG, nhx);
@@ -198,42 +261,52 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
         oz = (int)r.bz + tap_offset<W>(f2);
         ok = oy < y1 && oy + W > y0;
       }
+      stage_cand<T>(stg, lane, f0, f1, f2, c0, c1, ox, oy, oz);
       unsigned mask = __ballot_sync(0xffffffffu, ok);
+      __syncwarp();
       while (mask) {
         const int src = __ffs(mask) - 1;
         mask &= mask - 1;
-        const T g0 = __shfl_sync(0xffffffffu, f0, src), g1 = __shfl_sync(0xffffffffu, f1, src);
-        const T g2 = __shfl_sync(0xffffffffu, f2, src);
-        const T vr0 = __shfl_sync(0xffffffffu, c0, src), vi0 = __shfl_sync(0xffffffffu, c1, src);
-        const int vx = __shfl_sync(0xffffffffu, ox, src);
-        const int vy = __shfl_sync(0xffffffffu, oy, src) - y0;
-        const int vz = __shfl_sync(0xffffffffu, oz, src);
-        // kernel values: lane l < 3W holds tap l % W of axis l / W
-        T kv = (T)0;
+        T g0, g1, g2, vr0, vi0;
+        int vx, vy, vz;
+        read_cand<T>(stg, src, g0, g1, g2, vr0, vi0, vx, vy, vz);
+        vy -= y0;
+        // kernel values: lane l < 3W computes tap l % W of axis l / W into kvs[l]
         if (lane < 3 * W) {
           const int axis = lane / W, i = lane - axis * W;
           const T f = axis == 0 ? g0 : (axis == 1 ? g1 : g2);
+          T kv;
           if constexpr (kPoly)
             kv = poly_eval(pc, poly_arg<W>(f));
           else
             kv = es_kernel<T>((T)(tap_offset<W>(f) + i) - f, beta, ces, halfw);
+          kvs[lane] = kv;
         }
-        T kx[W];
-#pragma unroll
-        for (int e = 0; e < W; e++) kx[e] = __shfl_sync(0xffffffffu, kv, e);
+        __syncwarp();
+        T kx[8];
+        read_kx<T>(kvs, kx);
         const int dya = max(0, -vy), dyb = min(W, wy - vy);
         const int np = (dyb - dya) * W;
         const int xs = vx & (kXW - 1);
-        {
-          const int p = lane, dq = p / W, dz = p - dq * W, dy = dya + dq;
-          const T ky = __shfl_sync(0xffffffffu, kv, (W + dy) & 31);
-          const T kz = __shfl_sync(0xffffffffu, kv, 2 * W + dz);
-          if (p < np) {
-            int z = vz + dz;
-            z += z < 0 ? nw : (z >= nw ? -nw : 0);
-            const T k = ky * kz;
-            const T vr = vr0 * k, vi = vi0 * k;
-            C* a = acc + (vy + dy) * RS + z * kPS;
+        if (lane < np) {  // pair (dya + lane / W, lane % W)
+          const int dy = dya + lane_dq;
+          const T ky = kvs[W + dy];
+          const T kz = kvs[2 * W + lane_dz];
+          int z = vz + lane_dz;
+          z += z < 0 ? nw : (z >= nw ? -nw : 0);
+          const T k = ky * kz;
+          const T vr = vr0 * k, vi = vi0 * k;
+          C* a = acc + (vy + dy) * RS + z * kPS;
+          if (xs + W <= kXW) {  // the row's taps do not wrap the window (same for all lanes)
+            C* b = a + xs;
+#pragma unroll
+            for (int e = 0; e < W; e++) {
+              C cur = b[e];
+              cur.x += vr * kx[e];
+              cur.y += vi * kx[e];
+              b[e] = cur;
+            }
+          } else {
 #pragma unroll
             for (int e = 0; e < W; e++) {
               C* cell = a + ((xs + e) & (kXW - 1));
@@ -250,10 +323,8 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
             const int t = t0 + lane;
             const int pq = t / W, e = t - pq * W, p = 32 + pq;
             const int dq = p / W, dz = p - dq * W, dy = dya + dq;
-            const T ky = __shfl_sync(0xffffffffu, kv, (W + dy) & 31);
-            const T kz = __shfl_sync(0xffffffffu, kv, (2 * W + dz) & 31);
-            const T kxe = __shfl_sync(0xffffffffu, kv, e & 31);
             if (t < nt) {
+              const T ky = kvs[W + dy], kz = kvs[2 * W + dz], kxe = kvs[e];
               int z = vz + dz;
               z += z < 0 ? nw : (z >= nw ? -nw : 0);
               const T k = ky * kz;
@@ -361,7 +432,9 @@ bool slide_tiling(const Geom& g, size_t tsz, const TileTune* tt, SlideTile& tc) 
   tc.nsegs = (g.nhx + SEG - 1) / SEG;
   if ((int64_t)tc.nbands * tc.nsegs > 2147483647LL) return false;
   tc.nitems = tc.nbands * tc.nsegs;
-  tc.warp_bytes = ((size_t)TY * rs * 2 * tsz + (size_t)(3 * tc.nslots + 1) * 4 + 15) & ~(size_t)15;
+  tc.stage_off = ((size_t)TY * rs * 2 * tsz + (size_t)(3 * tc.nslots + 1) * 4 + 15) & ~(size_t)15;
+  // candidate slots (32 per warp) and 32 kernel values
+  tc.warp_bytes = tc.stage_off + 32 * (tsz == 4 ? 32 : 64) + 32 * tsz;
   int warps = (tt && tt->warps > 0 && tt->wx < 0) ? tt->warps : env_or("CG_SLIDE_WARPS", 0);
   if (warps <= 0) warps = (int)std::max<size_t>(1, std::min<size_t>(16, kSlideSmemMax / tc.warp_bytes));
   warps = std::min(warps, 16);
