@@ -410,7 +410,7 @@ int env_or(const char* name, int dflt) {
 }
 
 // Band rows, hive columns per segment and warps per CTA: the tuned values,
-// else CG_SLIDE_TY / CG_SLIDE_SEG / CG_SLIDE_WARPS, else 8 / 8 / as many as
+// else CG_SLIDE_TY / CG_SLIDE_SEG / CG_SLIDE_WARPS, else 8 / 12 / as many as
 // fit.  Short segments keep the densest items (around the grid centre) well
 // below a warp's share of the work; each costs one warm-up hive column.
 bool slide_tiling(const Geom& g, size_t tsz, const TileTune* tt, SlideTile& tc) {
@@ -418,7 +418,7 @@ bool slide_tiling(const Geom& g, size_t tsz, const TileTune* tt, SlideTile& tc) 
   if (W < 4 || W > 8 || (g.nf1 % 8) != 0 || (g.nf2 % 8) != 0 || g.nf1 < kXW) return false;
   int TY = (tt && tt->wy > 0 && tt->wx < 0) ? tt->wy : env_or("CG_SLIDE_TY", 8);
   if (TY != 8 && TY != 16 && TY != 32) return false;
-  int SEG = (tt && tt->wpb > 0 && tt->wx < 0) ? tt->wpb : env_or("CG_SLIDE_SEG", 8);
+  int SEG = (tt && tt->wpb > 0 && tt->wx < 0) ? tt->wpb : env_or("CG_SLIDE_SEG", 12);
   SEG = std::max(1, std::min(SEG, g.nhx));
   tc.TY = TY;
   tc.logTY = TY == 8 ? 3 : (TY == 16 ? 4 : 5);

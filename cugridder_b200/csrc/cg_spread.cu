@@ -719,9 +719,9 @@ static const int kGridCand[][4] = {{16, 16, 0, 0},  {16, 8, 0, 0},   {16, 8, 64,
                                    {16, 8, 64, 12}, {16, 16, 64, 0}, {32, 8, 0, 0},
                                    {16, 16, 5, 16}, {16, 16, 0, 12}, {16, 8, 10, 16},
                                    {16, 8, 13, 12}, {16, 16, 8, 10}, {16, 8, 64, 13},
-                                   {16, 8, 64, 14}, {-1, 8, 8, 0},   {-1, 8, 16, 0},
-                                   {-1, 8, 6, 0},   {-1, 8, 12, 0},  {-1, 8, 8, 12},
-                                   {-1, 16, 8, 0}};
+                                   {16, 8, 64, 14}, {-1, 8, 8, 0},   {-1, 8, 12, 0},
+                                   {-1, 8, 16, 0},  {-1, 8, 10, 0},  {-1, 8, 12, 14},
+                                   {-1, 8, 16, 14}};
 // threads -1 .. -4: the TMA-staged kernel's variants (all planes; 32 x 16
 // tiles with 512 threads and two stages / 256 threads and one stage; 32 x 8
 // and 16 x 8 tiles with 128 threads and one stage) where they apply.
