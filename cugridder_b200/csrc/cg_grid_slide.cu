@@ -153,6 +153,23 @@ __device__ __forceinline__ void read_kx(const T* kvs, T (&kx)[8]) {
   }
 }
 
+// the 3W kernel values of staged candidate src: lane l < 3W evaluates tap
+// l % W of axis l / W (its fraction is word l / W of the candidate's slot)
+template <typename T, int W, bool kPoly>
+__device__ __forceinline__ void eval_kv(const unsigned char* stg, int src, T* kv, int lane,
+                                        int axis, int tap, const T (&pc)[kPolyCoef], T beta,
+                                        T ces, T halfw) {
+  if (lane < 3 * W) {
+    const T f = reinterpret_cast<const T*>(stg + src * kCandBytes<T>)[axis];
+    T v;
+    if constexpr (kPoly)
+      v = poly_eval(pc, poly_arg<W>(f));
+    else
+      v = es_kernel<T>((T)(tap_offset<W>(f) + tap) - f, beta, ces, halfw);
+    kv[lane] = v;
+  }
+}
+
 template <typename T, int W, bool kPoly>
 __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
                                            const int* __restrict__ hive_start, const Geom& g,
@@ -168,11 +185,13 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
   int* t_pref = t_start + tc.nslots;      // nslots + 1
   int* t_shy = t_pref + tc.nslots + 1;
   // staging of the current chunk's candidates (one 32- or 64-byte slot per
-  // lane) and of the current row's kernel values: every lane reads them with
+  // lane) and of two rows' kernel values (double-buffered: the next row's are
+  // evaluated while the current row is spread): every lane reads them with
   // broadcast loads, where register shuffles took one crossbar operation per
   // value
   unsigned char* stg = wsmem + tc.stage_off;
   T* kvs = reinterpret_cast<T*>(stg + 32 * kCandBytes<T>);
+  const int kv_axis = lane / W, kv_tap = lane - kv_axis * W;
   const size_t plane = (size_t)nf1 * nf2;
   C* fwc = reinterpret_cast<C*>(fw);
   const T beta = (T)g.beta, ces = (T)g.es_c, halfw = (T)W * (T)0.5;
@@ -264,34 +283,32 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
       stage_cand<T>(stg, lane, f0, f1, f2, c0, c1, ox, oy, oz);
       unsigned mask = __ballot_sync(0xffffffffu, ok);
       __syncwarp();
+      if (mask)
+        eval_kv<T, W, kPoly>(stg, __ffs(mask) - 1, kvs, lane, kv_axis, kv_tap, pc, beta, ces, halfw);
+      int buf = 0;
+      __syncwarp();
       while (mask) {
         const int src = __ffs(mask) - 1;
         mask &= mask - 1;
+        const T* kv = kvs + buf * 32;
+        // the next row's kernel values into the other buffer: independent of
+        // this row's taps, so their latency overlaps
+        if (mask)
+          eval_kv<T, W, kPoly>(stg, __ffs(mask) - 1, kvs + (buf ^ 1) * 32, lane, kv_axis, kv_tap,
+                               pc, beta, ces, halfw);
         T g0, g1, g2, vr0, vi0;
         int vx, vy, vz;
         read_cand<T>(stg, src, g0, g1, g2, vr0, vi0, vx, vy, vz);
         vy -= y0;
-        // kernel values: lane l < 3W computes tap l % W of axis l / W into kvs[l]
-        if (lane < 3 * W) {
-          const int axis = lane / W, i = lane - axis * W;
-          const T f = axis == 0 ? g0 : (axis == 1 ? g1 : g2);
-          T kv;
-          if constexpr (kPoly)
-            kv = poly_eval(pc, poly_arg<W>(f));
-          else
-            kv = es_kernel<T>((T)(tap_offset<W>(f) + i) - f, beta, ces, halfw);
-          kvs[lane] = kv;
-        }
-        __syncwarp();
         T kx[8];
-        read_kx<T>(kvs, kx);
+        read_kx<T>(kv, kx);
         const int dya = max(0, -vy), dyb = min(W, wy - vy);
         const int np = (dyb - dya) * W;
         const int xs = vx & (kXW - 1);
         if (lane < np) {  // pair (dya + lane / W, lane % W)
           const int dy = dya + lane_dq;
-          const T ky = kvs[W + dy];
-          const T kz = kvs[2 * W + lane_dz];
+          const T ky = kv[W + dy];
+          const T kz = kv[2 * W + lane_dz];
           int z = vz + lane_dz;
           z += z < 0 ? nw : (z >= nw ? -nw : 0);
           const T k = ky * kz;
@@ -324,7 +341,7 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
             const int pq = t / W, e = t - pq * W, p = 32 + pq;
             const int dq = p / W, dz = p - dq * W, dy = dya + dq;
             if (t < nt) {
-              const T ky = kvs[W + dy], kz = kvs[2 * W + dz], kxe = kvs[e];
+              const T ky = kv[W + dy], kz = kv[2 * W + dz], kxe = kv[e];
               int z = vz + dz;
               z += z < 0 ? nw : (z >= nw ? -nw : 0);
               const T k = ky * kz;
@@ -337,6 +354,7 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
           }
         }
         __syncwarp();
+        buf ^= 1;
       }
     }
 
@@ -433,8 +451,8 @@ bool slide_tiling(const Geom& g, size_t tsz, const TileTune* tt, SlideTile& tc) 
   if ((int64_t)tc.nbands * tc.nsegs > 2147483647LL) return false;
   tc.nitems = tc.nbands * tc.nsegs;
   tc.stage_off = ((size_t)TY * rs * 2 * tsz + (size_t)(3 * tc.nslots + 1) * 4 + 15) & ~(size_t)15;
-  // candidate slots (32 per warp) and 32 kernel values
-  tc.warp_bytes = tc.stage_off + 32 * (tsz == 4 ? 32 : 64) + 32 * tsz;
+  // candidate slots (32 per warp) and two buffers of 32 kernel values
+  tc.warp_bytes = tc.stage_off + 32 * (tsz == 4 ? 32 : 64) + 64 * tsz;
   int warps = (tt && tt->warps > 0 && tt->wx < 0) ? tt->warps : env_or("CG_SLIDE_WARPS", 0);
   if (warps <= 0) warps = (int)std::max<size_t>(1, std::min<size_t>(16, kSlideSmemMax / tc.warp_bytes));
   warps = std::min(warps, 16);
