@@ -153,6 +153,10 @@ cg_plan_s* cached_plan(int precision, int& status) {
     P = new cg_plan_s();
     P->device = dev;
     P->stream = nullptr;
+    // the reference-compatible calls cannot reach cg_plan_set_autotune, and
+    // their cached plan serves every later call of the same geometry: tune
+    // on the first call (CG_AUTOTUNE=0 turns it off)
+    P->autotune = 1;
     if (const char* m = getenv("CG_AUTOTUNE")) P->autotune = atoi(m) != 0;
     if (const char* m = getenv("CG_DEGRID_TMA")) P->tma_default = atoi(m);
   }

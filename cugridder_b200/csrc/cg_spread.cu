@@ -751,13 +751,18 @@ void set_tile_candidate(TileTune& tt, int dir, const int* c) {
 // offers 227 KB to one CTA)
 constexpr size_t kWarpSmemMax = 227 * 1024;
 
-// Warp tiles: 16 x 16 cells by default (CG_WTILE_X / CG_WTILE_Y); the plane
-// batch and warps per CTA are chosen so that two CTAs fit on an SM.
+// Warp tiles: shape from the tuned fields, CG_WTILE_X / CG_WTILE_Y /
+// CG_WTILE_PLANES / CG_WTILE_WARPS, else the defaults below.
 template <typename T>
 WarpTile warp_tiling(const Geom& g, const TileTune* tt) {
   WarpTile tc{};
   const int W = g.kw;
-  int tx = env_int("CG_WTILE_X", 16), ty = env_int("CG_WTILE_Y", 16);
+  // An untuned plan (no field set) gets the shape the autotuner picks for
+  // dense data: 16 x 8 cells, every plane, as many warps as fit up to 12.
+  // The fields a tuning candidate leaves at 0 keep their candidate-list
+  // meaning: 16 x 16 cells, 7 planes, warps up to 8 in 110 KB.
+  const bool cand = tt && (tt->wx || tt->wy || tt->wpb || tt->warps);
+  int tx = env_int("CG_WTILE_X", 16), ty = env_int("CG_WTILE_Y", cand ? 16 : 8);
   int PB = env_int("CG_WTILE_PLANES", 0);
   int warps = env_int("CG_WTILE_WARPS", 0);
   if (tt) {
@@ -769,7 +774,7 @@ WarpTile warp_tiling(const Geom& g, const TileTune* tt) {
   tc.TX = std::max(16, (tx / 16) * 16);
   tc.TY = std::max(8, (ty / 8) * 8);
   tc.PS = tc.TX + 1;  // = 1 (mod 16): consecutive dz of a lane group hit consecutive banks
-  if (PB <= 0) PB = std::min(g.nw, 7);
+  if (PB <= 0) PB = cand ? std::min(g.nw, 7) : g.nw;
   PB = std::min(PB, g.nw);
   tc.PB = PB;
   int rs = PB * tc.PS;
@@ -781,7 +786,9 @@ WarpTile warp_tiling(const Geom& g, const TileTune* tt) {
   tc.slots = ((tc.TY >> 3) + 2 + (g.nf2 % 8 != 0)) * (PB + (W - 1) / 2 + (W + 1) / 2) * 3;
   tc.warp_bytes =
       ((size_t)tc.TY * tc.RS * 2 * sizeof(T) + (size_t)(tc.slots + 1) * kSegInts * 4 + 15) & ~(size_t)15;
-  if (warps <= 0) warps = (int)std::max<size_t>(1, std::min<size_t>(8, (110 * 1024) / tc.warp_bytes));
+  if (warps <= 0)
+    warps = cand ? (int)std::max<size_t>(1, std::min<size_t>(8, (110 * 1024) / tc.warp_bytes))
+                 : (int)std::max<size_t>(1, std::min<size_t>(12, kWarpSmemMax / tc.warp_bytes));
   warps = std::min(warps, 16);
   while (warps > 1 && tc.warp_bytes * warps > kWarpSmemMax) warps--;
   tc.warps = warps;

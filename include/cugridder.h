@@ -214,9 +214,11 @@ int cg_plan_set_fixed_uvw(cg_plan *plan, int on);
  * direction for a grid geometry times a fixed list of candidate tilings of
  * its spreading / interpolation launch (tile size, plane batch, warps or
  * threads per CTA) on the call's own data and keeps the fastest for later
- * calls.  Off by default; the environment variable CG_AUTOTUNE=1 turns it on
- * for plans created afterwards, the host entry points' cached plans
- * included.  The tuning call synchronizes, so capture a plan's calls into a
+ * calls.  Off by default for plans made with cg_plan_create (the
+ * environment variable CG_AUTOTUNE=1 turns it on for plans created
+ * afterwards); on by default for the cached plans behind the host entry
+ * points (ms2dirty_1 ... cg_dirty2ms_mixed), which callers cannot reach with
+ * this call, unless CG_AUTOTUNE=0.  The tuning call synchronizes, so capture a plan's calls into a
  * CUDA graph only after it.  cg_plan_get_tiling reports the tiling in the
  * layout of cg_batch_get_tiling. */
 int cg_plan_set_autotune(cg_plan *plan, int on);
