@@ -139,11 +139,16 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_upsweep(const K* __restrict__
   hist[threadIdx.x] = 0;
   __syncthreads();
   int64_t base = (int64_t)blockIdx.x * kRsTile;
-#pragma unroll 4
+  // all loads first, so they are in flight together
+  int dg[kRsItems];
+#pragma unroll
   for (int i = 0; i < kRsItems; i++) {
     int64_t idx = base + i * kRsThreads + threadIdx.x;
-    if (idx < M) atomicAdd(&hist[(int)((keys[idx] >> shift) & 0xFF)], 1);
+    dg[i] = idx < M ? (int)((keys[idx] >> shift) & 0xFF) : -1;
   }
+#pragma unroll
+  for (int i = 0; i < kRsItems; i++)
+    if (dg[i] >= 0) atomicAdd(&hist[dg[i]], 1);
   __syncthreads();
   counts[(int64_t)threadIdx.x * ntiles + blockIdx.x] = hist[threadIdx.x];
 }
@@ -166,7 +171,10 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_downsweep(
   int (*wpref)[256] = whist + 8;                                  // [8][256]
   int* dstart = &wpref[8][0];                                     // [256]
   int* s_warp = dstart + 256;                                     // [33]
+  int* soff = s_warp + 36;                                        // [256]
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // this tile's output base of digit threadIdx.x, fetched while the tile ranks
+  const int my_off = offsets[(int64_t)threadIdx.x * ntiles + blockIdx.x];
   for (int d = threadIdx.x; d < 8 * 256; d += kRsThreads) (&whist[0][0])[d] = 0;
   __syncthreads();
   K k[kRsItems];
@@ -174,12 +182,19 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_downsweep(
   const int64_t tile0 = (int64_t)blockIdx.x * kRsTile;
   int64_t base = tile0 + warp * (kRsTile / 8);
   unsigned lt = (1u << lane) - 1u;
+  // all loads first, so they are in flight together (the ranking below
+  // synchronizes the warp per item)
 #pragma unroll
   for (int i = 0; i < kRsItems; i++) {
     int64_t idx = base + i * 32 + lane;
     bool valid = idx < M;
     k[i] = valid ? keys_in[idx] : (K)0;
     v[i] = valid ? vals_in[idx] : 0;
+  }
+#pragma unroll
+  for (int i = 0; i < kRsItems; i++) {
+    int64_t idx = base + i * 32 + lane;
+    bool valid = idx < M;
     int d = valid ? (int)((k[i] >> shift) & 0xFF) : 256;
     unsigned peers = __match_any_sync(0xffffffffu, d);
     int cur = (d < 256) ? whist[warp][d] : 0;
@@ -198,7 +213,9 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_downsweep(
       wpref[w][d] = run;
       run += whist[w][d];
     }
-    dstart[d] = block_excl_scan(run, s_warp, total);  // tile-local start of digit d
+    const int ds = block_excl_scan(run, s_warp, total);  // tile-local start of digit d
+    dstart[d] = ds;
+    soff[d] = my_off - ds;  // output position of tile slot p of digit d: soff[d] + p
   }
   __syncthreads();
 #pragma unroll
@@ -213,7 +230,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_downsweep(
   for (int p = threadIdx.x; p < total; p += kRsThreads) {
     const K key = skey[p];
     const int d = (int)((key >> shift) & 0xFF);
-    const int64_t pos = (int64_t)offsets[(int64_t)d * ntiles + blockIdx.x] + (p - dstart[d]);
+    const int64_t pos = (int64_t)soff[d] + p;
     keys_out[pos] = key;
     vals_out[pos] = sval[p];
   }
@@ -221,7 +238,7 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_downsweep(
 
 template <typename K>
 constexpr size_t rs_down_smem() {
-  return (size_t)kRsTile * (sizeof(K) + 4) + (8 * 256 * 2 + 256 + 33) * 4;
+  return (size_t)kRsTile * (sizeof(K) + 4) + (8 * 256 * 2 + 256 + 36 + 256) * 4;
 }
 
 // ---------------------------------------------------------------- scan
@@ -389,6 +406,10 @@ static int bin_impl(const double* d_uvw, int64_t M, const Geom& g, void* d_ws, i
     K* kin = ka; int* vin = va; K* kout = kb; int* vout = vb;
     for (int ps = 0; ps < passes; ps++) {
       int shift = 8 * ps;
+      if (ps == passes - 1) {  // the last pass writes the outputs in place of a copy
+        kout = d_sorted_keys;
+        if (vin != d_perm) vout = d_perm;
+      }
       k_rs_upsweep<K><<<(int)ntiles, kRsThreads, 0, st>>>(kin, M, shift, (int)ntiles, counts);
       count_launches(1);
       CG_TRY(scan_exclusive(counts, ncount, offs, sums, st));
@@ -400,7 +421,6 @@ static int bin_impl(const double* d_uvw, int64_t M, const Geom& g, void* d_ws, i
       int* tv = vin; vin = vout; vout = tv;
     }
     if (vin != d_perm) CG_CUDA(cudaMemcpyAsync(d_perm, vin, (size_t)M * 4, cudaMemcpyDeviceToDevice, st));
-    CG_CUDA(cudaMemcpyAsync(d_sorted_keys, kin, (size_t)M * sizeof(K), cudaMemcpyDeviceToDevice, st));
   }
   if (d_hs_sums) {
     // counts per hive, then an in-place exclusive scan: O(M + nh), no search
