@@ -276,6 +276,7 @@ int plan_configure(cg_plan_s* P, int nx, int ny, double fov, double eps, double 
   P->precision = precision;
   P->eps_status = st;
   P->bins_valid = false;
+  P->quarter_valid = false;
   P->kw = kw;
   P->beta = beta;
   P->es_c = c;
@@ -845,6 +846,19 @@ static int ms2dirty_tail(cg_plan_s* P, T* d_dirty) {
 }
 
 // part 0: the whole call; 1: the stages before gridding; 2: those after it
+// Quarter tables of the call's geometry; a call whose geometry equals the
+// last one's (same image, pixel sizes, w shift and scales, quadrature) finds
+// them already in place.
+static int quarter_tables(cg_plan_s* P, cudaStream_t st) {
+  const Geom& g = P->geom;
+  const double key[7] = {(double)g.N1, (double)g.N2, g.pixx, g.pixy, g.o_center, g.gamma, g.h};
+  if (P->quarter_valid && std::equal(key, key + 7, P->quarter_key)) return CG_OK;
+  CG_TRY(launch_quarter(g, P->quad, (double*)P->K3q.p, (double*)P->zq.p, st));
+  std::copy(key, key + 7, P->quarter_key);
+  P->quarter_valid = true;
+  return CG_OK;
+}
+
 template <typename T>
 static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T* d_wgt,
                       T* d_dirty, bool reuse, int part = 0) {
@@ -853,7 +867,7 @@ static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T
   cudaStream_t st = P->stream;
   int64_t M = P->nrow;
   timer_mark(P);  // stage 0: w range + geometry
-  if (!reuse) CG_TRY(launch_quarter(g, P->quad, (double*)P->K3q.p, (double*)P->zq.p, st));
+  if (!reuse) CG_TRY(quarter_tables(P, st));
   timer_mark(P);  // 1: quarter tables
   if (!reuse) {
     CG_TRY(wait_uvw(P));
@@ -891,7 +905,7 @@ static int dirty2ms_t(cg_plan_s* P, const double* d_uvw, const T* d_dirty, const
   cudaStream_t st = P->stream;
   int64_t M = P->nrow;
   timer_mark(P);  // stage 0: w range + geometry
-  if (!reuse) CG_TRY(launch_quarter(g, P->quad, (double*)P->K3q.p, (double*)P->zq.p, st));
+  if (!reuse) CG_TRY(quarter_tables(P, st));
   timer_mark(P);  // 1: quarter tables
   // Host entry points whose ranges came from the host: the plane fill and
   // the FFT need only the image and the geometry, so they run on aux_stream

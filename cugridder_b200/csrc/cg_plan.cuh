@@ -87,6 +87,11 @@ struct cg_plan_s {
   // synchronisation, so such calls can be captured in a CUDA graph)
   int fixed_uvw = 0;
   bool bins_valid = false;
+  // the quarter tables (K3q, zq) hold those of quarter_key: they depend only on
+  // the image geometry, the w-derived shift and scales and the kernel's
+  // quadrature (reset when the plan is reconfigured)
+  bool quarter_valid = false;
+  double quarter_key[7] = {};
   const double* last_uvw = nullptr;
   int64_t last_nrow = -1;
   double last_freq = 0;
