@@ -243,6 +243,20 @@ def make_data(cfg_name, seed, nrow, torch, fov=None):
     return d, img
 
 
+def fft_cells(d, info):
+    """Cells the band-pruned transform reads plus writes per w plane: the row
+    transforms over the grid rows that hold data (read and written whole,
+    batch rounded up to 64 rows as the plan does) and the column transforms
+    over the image columns, reading the band's rows and writing the image's
+    rows (ms2dirty; dirty2ms moves the same cells the other way)."""
+    nf1, nf2, W = info["nf1"], info["nf2"], info["kw"]
+    u = d["uvw"][:, 0] * (d["freq"] / 299792458.0)
+    pixx = np.deg2rad(d["fov"]) / d["nx"]
+    span = (float(u.max()) - float(u.min())) * pixx * nf2 + W + 1
+    nb = min(nf2, int(np.ceil(span / 64.0)) * 64)
+    return 2 * nb * nf1 + nb * d["ny"] + d["nx"] * d["ny"]
+
+
 def algorithmic_bytes(stage, d, info, prec):
     """Minimum HBM bytes of one launch of each stage (reads of its inputs plus
     writes of its outputs, each once)."""
@@ -262,7 +276,7 @@ def algorithmic_bytes(stage, d, info, prec):
         "degridding": G * s_c + M * rec + M * 4 + M * s_c,
         "plane_fill": fill_cells * s_c + npix * s_c + nq * 16,
         "wdft_deconv": info["nw"] * npix * s_c + npix * s_c + nq * 16,
-        "fft": 4 * G * s_c,
+        "fft": fft_cells(d, info) * info["nw"] * s_c,
         "sorted_stream": M * (4 + 24 + s_c + s_c // 2) + M * rec,
         "binning": M * 24 + 4 * 3 * M * 8,
     }.get(stage)
