@@ -127,10 +127,14 @@ int build_jobs(cg_batch_s* B, int dir, const cg::TileTune& tt, std::vector<cg::G
     order.push_back((int)i);
   }
   if (jobs.empty()) return CG_OK;
+  if (dir == 0 && tt.wx < 0)  // a sliding-window candidate needs every dataset's grid to take it
+    for (const auto& J : jobs)
+      if (J.st.TY == 0) return CG_ERR_ARG;
   std::vector<size_t> idx(jobs.size());
   std::iota(idx.begin(), idx.end(), 0);
   auto density = [&](size_t k) {
-    const int items = dir == 0 ? jobs[k].wt.nitems : jobs[k].dt.nitems;
+    const int items = dir == 0 ? (jobs[k].st.TY > 0 ? jobs[k].st.nitems : jobs[k].wt.nitems)
+                               : jobs[k].dt.nitems;
     return (double)jobs[k].M / std::max(1, items);
   };
   std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return density(a) > density(b); });
@@ -182,7 +186,11 @@ int prepare_phase2(cg_batch_s* B, int dir, cudaStream_t st) {
     cg::TileTune best_tt = B->tune;
     for (int c = 0; c < ncand; c++) {
       if (dir == 1 && cand[c][3] < 0) continue;  // the TMA-staged kernel is single-grid only
-      if (dir == 0 && cand[c][0] < 0) continue;  // so are the x-sliding gridding windows
+      // the x-sliding windows run in the batch only when CG_GRID_SLIDE=1 asks
+      // for them: on the 32-dataset workload (uv concentrated near each
+      // grid's centre, so a few items hold most rows) they measured 3.4x
+      // slower than the warp tiles, and each candidate costs two launches
+      if (dir == 0 && cand[c][0] < 0) continue;
       cg::TileTune tt = B->tune;
       cg::set_tile_candidate(tt, dir, cand[c]);
       if (build_jobs<T>(B, dir, tt, jobs, order, &sh) != CG_OK || jobs.empty()) continue;

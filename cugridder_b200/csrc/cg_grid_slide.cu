@@ -44,15 +44,6 @@ constexpr int kXW = 16;      // window columns (circular)
 constexpr int kPS = kXW + 1;  // plane stride (complex units)
 constexpr int kFlushL = 4;    // flushed cells of column c: [8c - 4, 8c + 4)
 
-struct SlideTile {
-  int TY, logTY, SEG;  // band rows (8, 16 or 32), hive columns per segment
-  int RS;              // row stride of the window (complex units)
-  int nslots;          // (hive rows of a band's halo) x nw
-  int nbands, nsegs, nitems;
-  int warps;
-  size_t stage_off;  // byte offset of the candidate / kernel-value staging in a warp's region
-  size_t warp_bytes, smem;
-};
 
 template <typename T>
 struct Cx;
@@ -420,12 +411,52 @@ __global__ void __launch_bounds__(512) k_grid_slide(const Rec<T>* __restrict__ r
   }
 }
 
+// Many grids in one persistent launch (batched solves): warps take (job,
+// item) pairs from one queue, every job with its own geometry and window
+// shape (jobs[j].st) in a per-warp region of warp_bytes, the largest of the
+// jobs'.  Every job shares W and the kernel.
+template <typename T, int W, bool kPoly>
+__global__ void __launch_bounds__(512) k_grid_slide_multi(const GridJob<T>* __restrict__ jobs,
+                                                          int njobs, int nitems,
+                                                          size_t warp_bytes,
+                                                          int* __restrict__ counter) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  T pc[kPolyCoef];
+#pragma unroll
+  for (int n = 0; n < kPolyCoef; n++) pc[n] = (T)0;
+  if constexpr (kPoly) {
+    const T* poly = geom_poly<T>(jobs[0].g);
+    if (lane < 3 * W) {
+      const int i = lane % W;
+#pragma unroll
+      for (int n = 0; n < kPolyCoef; n++) pc[n] = poly[i * kPolyCoef + n];
+    }
+  }
+  unsigned char* wsmem = smem + (size_t)wib * warp_bytes;
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(counter, 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= nitems) break;
+    int lo = 0, hi = njobs;  // jobs[lo].grid_item0 <= item < jobs[hi].grid_item0
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (jobs[mid].grid_item0 <= item) lo = mid; else hi = mid;
+    }
+    const GridJob<T>& J = jobs[lo];
+    slide_item<T, W, kPoly>(J.recs, J.hive_start, J.g, J.st, J.fw, item - J.grid_item0, wsmem, pc);
+  }
+}
+
 constexpr size_t kSlideSmemMax = 227 * 1024;
 
 int env_or(const char* name, int dflt) {
   const char* v = getenv(name);
   return v ? atoi(v) : dflt;
 }
+
+}  // namespace
 
 // Band rows, hive columns per segment and warps per CTA: the tuned values,
 // else CG_SLIDE_TY / CG_SLIDE_SEG / CG_SLIDE_WARPS, else 8 / 12 / as many as
@@ -462,6 +493,8 @@ bool slide_tiling(const Geom& g, size_t tsz, const TileTune* tt, SlideTile& tc) 
   tc.smem = tc.warp_bytes * warps;
   return true;
 }
+
+namespace {
 
 int sms_of_device() {
   int dev = 0, n = 0;
@@ -505,6 +538,46 @@ int launch_grid_slide(const Rec<T>* d_recs, const int* d_hive_start, const Geom&
   }
 }
 
+template <typename T, int W>
+static int slide_multi_w(const GridJob<T>* d_jobs, int njobs, const MultiShape& sh, int* d_counter,
+                         cudaStream_t st) {
+  auto* kern = sh.poly ? k_grid_slide_multi<T, W, true> : k_grid_slide_multi<T, W, false>;
+  const size_t smem = sh.warp_bytes * sh.warps;
+  int per_sm = 0;
+  CG_CUDA(kernel_occupancy((const void*)kern, sh.warps * 32, smem, &per_sm));
+  if (per_sm < 1) {
+    set_last_error("multi-grid sliding gridding does not fit on an SM");
+    return CG_ERR_ARG;
+  }
+  static int sms = 0;
+  if (!sms) sms = sms_of_device();
+  const int blocks = std::min((sh.grid_items + sh.warps - 1) / sh.warps, per_sm * sms);
+  CG_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(int), st));
+  kern<<<std::max(1, blocks), sh.warps * 32, smem, st>>>(d_jobs, njobs, sh.grid_items,
+                                                         sh.warp_bytes, d_counter);
+  count_launches(1);
+  CG_CUDA(cudaGetLastError());
+  return CG_OK;
+}
+
+template <typename T>
+int launch_grid_slide_multi(const GridJob<T>* d_jobs, int njobs, const MultiShape& sh,
+                            int* d_counter, cudaStream_t st) {
+  if (njobs < 1 || sh.grid_items < 1) return CG_OK;
+  switch (sh.kw) {
+    case 4: return slide_multi_w<T, 4>(d_jobs, njobs, sh, d_counter, st);
+    case 5: return slide_multi_w<T, 5>(d_jobs, njobs, sh, d_counter, st);
+    case 6: return slide_multi_w<T, 6>(d_jobs, njobs, sh, d_counter, st);
+    case 7: return slide_multi_w<T, 7>(d_jobs, njobs, sh, d_counter, st);
+    case 8: return slide_multi_w<T, 8>(d_jobs, njobs, sh, d_counter, st);
+    default: return CG_ERR_ARG;
+  }
+}
+
+template int launch_grid_slide_multi<float>(const GridJob<float>*, int, const MultiShape&, int*,
+                                            cudaStream_t);
+template int launch_grid_slide_multi<double>(const GridJob<double>*, int, const MultiShape&, int*,
+                                             cudaStream_t);
 template int launch_grid_slide<float>(const Rec<float>*, const int*, const Geom&, float*, int*,
                                       cudaStream_t, const TileTune*);
 template int launch_grid_slide<double>(const Rec<double>*, const int*, const Geom&, double*, int*,

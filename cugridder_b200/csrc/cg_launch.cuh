@@ -52,6 +52,24 @@ int degrid_slots(const TileCfg& tc, int W);
 int tile_candidates(int dir, const int (**cand)[4]);
 void set_tile_candidate(TileTune& tt, int dir, const int* c);
 
+// Shape of the x-sliding gridding (cg_grid_slide.cu) for one grid: bands of
+// TY rows, segments of SEG hive columns, the circular window's row stride RS
+// (complex elements), nslots segment slots per column, the items, warps per
+// CTA and the per-warp shared-memory layout.
+struct SlideTile {
+  int TY, logTY, SEG;
+  int RS;
+  int nslots;
+  int nbands, nsegs, nitems;
+  int warps;
+  size_t stage_off;
+  size_t warp_bytes, smem;
+};
+// Shape for grid g in working precision tsz from the tuned fields of tt
+// (wx < 0 selects the sliding kernel; wy band rows, wpb segment columns,
+// warps) or the defaults; false where the sliding kernel does not apply.
+bool slide_tiling(const Geom& g, size_t tsz, const TileTune* tt, SlideTile& tc);
+
 // One grid of a multi-grid launch (batched solves): the plan's sorted stream,
 // hive offsets and grid, its tilings and its first work item in the launch.
 template <typename T>
@@ -64,6 +82,7 @@ struct GridJob {
   int64_t M;
   Geom g;
   WarpTile wt;
+  SlideTile st;     // sliding-window gridding shape (st.TY = 0: warp tiles)
   TileCfg dt;
   int nslots;       // segment slots of the degridding tiles
   int grid_item0;   // first gridding item of this job (prefix over jobs)
@@ -79,6 +98,7 @@ struct MultiShape {
   size_t dsmem;       // degridding bytes per CTA (largest of the jobs)
   int grid_items, degrid_items;
   bool partial_hives;  // some job's grid has an axis that is not a multiple of 8 cells
+  bool slide;          // gridding by x-sliding windows (every job's st set)
 };
 // Fill the item prefixes and the shared shape of jobs (host array).
 template <typename T>
@@ -86,6 +106,10 @@ int multi_shape(GridJob<T>* jobs, int njobs, MultiShape* shape);
 template <typename T>
 int launch_grid_multi(const GridJob<T>* d_jobs, int njobs, const MultiShape& sh, int* d_counter,
                       cudaStream_t st);
+// the same launch for jobs gridded by x-sliding windows (sh.slide)
+template <typename T>
+int launch_grid_slide_multi(const GridJob<T>* d_jobs, int njobs, const MultiShape& sh,
+                            int* d_counter, cudaStream_t st);
 // the multi-grid job of a plan whose last call was split at its spreading
 // step (cg_plan.cuh's cg_plan_s; tilings from tt)
 template <typename T>

@@ -1100,6 +1100,12 @@ int plan_grid_job(const cg_plan_s* P, const TileTune& tt, T* d_vis, GridJob<T>* 
   J.M = P->nrow;
   J.g = g;
   J.wt = warp_tiling<T>(g, &tt);
+  // x-sliding windows for a tuning candidate with wx < 0, or CG_GRID_SLIDE=1
+  // (as for a single plan); st.TY = 0 where they do not apply
+  J.st = SlideTile{};
+  const char* sl = getenv("CG_GRID_SLIDE");
+  if ((tt.wx < 0 || (sl && atoi(sl) != 0)) && !slide_tiling(g, sizeof(T), &tt, J.st))
+    J.st = SlideTile{};
   J.dt = grid_tiling<T>(g, true, &tt);
   J.nslots = degrid_slots(J.dt, g.kw);
   *job = J;

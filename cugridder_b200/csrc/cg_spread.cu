@@ -924,6 +924,9 @@ int multi_shape(GridJob<T>* jobs, int njobs, MultiShape* sh) {
   sh->threads = jobs[0].dt.threads;
   int64_t gi = 0, di = 0;
   int warps = 16;
+  // sliding-window gridding when every job has its window shape
+  sh->slide = true;
+  for (int j = 0; j < njobs; j++) sh->slide = sh->slide && jobs[j].st.TY > 0;
   for (int j = 0; j < njobs; j++) {
     GridJob<T>& J = jobs[j];
     if (J.g.kw != sh->kw || (geom_poly_host<T>(J.g) != nullptr) != sh->poly ||
@@ -933,12 +936,12 @@ int multi_shape(GridJob<T>* jobs, int njobs, MultiShape* sh) {
     }
     J.grid_item0 = (int)gi;
     J.degrid_item0 = (int)di;
-    gi += J.wt.nitems;
+    gi += sh->slide ? J.st.nitems : J.wt.nitems;
     di += J.dt.nitems;
-    sh->warp_bytes = std::max(sh->warp_bytes, J.wt.warp_bytes);
+    sh->warp_bytes = std::max(sh->warp_bytes, sh->slide ? J.st.warp_bytes : J.wt.warp_bytes);
     if ((J.g.nf1 % 8) != 0 || (J.g.nf2 % 8) != 0) sh->partial_hives = true;
     sh->dsmem = std::max(sh->dsmem, J.dt.smem);
-    warps = std::min(warps, J.wt.warps);
+    warps = std::min(warps, sh->slide ? J.st.warps : J.wt.warps);
   }
   if (gi > 2147483647LL || di > 2147483647LL) return CG_ERR_SIZE;
   sh->grid_items = (int)gi;
@@ -991,6 +994,7 @@ template <typename T>
 int launch_grid_multi(const GridJob<T>* d_jobs, int njobs, const MultiShape& sh, int* d_counter,
                       cudaStream_t st) {
   if (njobs < 1 || sh.grid_items < 1) return CG_OK;
+  if (sh.slide) return launch_grid_slide_multi<T>(d_jobs, njobs, sh, d_counter, st);
 #define CG_GRID_MULTI_CALL(w) grid_multi_w<T, w>(d_jobs, njobs, sh, d_counter, st)
   CG_W_SWITCH(sh.kw, CG_GRID_MULTI_CALL)
 #undef CG_GRID_MULTI_CALL

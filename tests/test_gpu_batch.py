@@ -137,6 +137,27 @@ def test_batch_learned_kernel(torch_cuda):
     b.close()
 
 
+@pytest.mark.parametrize("learned", [False, True])
+def test_batch_sliding_windows(torch_cuda, monkeypatch, learned):
+    """Every dataset gridded by x-sliding windows in the one launch
+    (k_grid_slide_multi: per-dataset band and segment items, window shapes
+    and geometry), through the eager, captured and replayed calls, against
+    one plan per dataset and the oracle.  Only the datasets whose grids the
+    sliding kernel takes (both axes multiples of 8 cells)."""
+    from cugridder_b200.learn import load_kernel
+
+    torch = torch_cuda
+    monkeypatch.setenv("CG_GRID_SLIDE", "1")
+    monkeypatch.setenv("CG_BATCH_AUTOTUNE", "0")
+    ds = [d for d, spec in zip(_datasets(torch), SPECS) if spec[0] == spec[1]]
+    k = load_kernel(5) if learned else None
+    b = Batch(ds, epsilon=1e-4, precision="fp32")
+    if k is not None:
+        b.set_kernel("poly", k.W, k.horner)
+    _check_batch(torch, ds, b, 3, kernel=k)
+    b.close()
+
+
 def test_batch_untuned_eager(torch_cuda, monkeypatch):
     torch = torch_cuda
     monkeypatch.setenv("CG_BATCH_AUTOTUNE", "0")
