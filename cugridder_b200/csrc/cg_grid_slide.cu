@@ -194,6 +194,7 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
   const int kb = item / tc.nsegs, ks = item - kb * tc.nsegs;
   const int band = tc.nbands / 2 + ((kb & 1) ? -((kb + 1) >> 1) : (kb >> 1));
   const int lane_dq = lane / W, lane_dz = lane - lane_dq * W;  // pair offsets of round 0
+  const int lane_dq2 = (lane + 32) / W, lane_dz2 = lane + 32 - lane_dq2 * W;  // of round 1
   const int seg = tc.nsegs / 2 + ((ks & 1) ? -((ks + 1) >> 1) : (ks >> 1));
   const int y0 = band * TY, y1 = min(y0 + TY, nf2), wy = y1 - y0;
   const int hs = seg * tc.SEG, he = min(hs + tc.SEG, nhx);
@@ -296,11 +297,12 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
         const int dya = max(0, -vy), dyb = min(W, wy - vy);
         const int np = (dyb - dya) * W;
         const int xs = vx & (kXW - 1);
-        if (lane < np) {  // pair (dya + lane / W, lane % W)
-          const int dy = dya + lane_dq;
+        // pair (dya + dq, dz): its W taps along x
+        auto spread = [&](int dq, int dz) {
+          const int dy = dya + dq;
           const T ky = kv[W + dy];
-          const T kz = kv[2 * W + lane_dz];
-          int z = vz + lane_dz;
+          const T kz = kv[2 * W + dz];
+          int z = vz + dz;
           z += z < 0 ? nw : (z >= nw ? -nw : 0);
           const T k = ky * kz;
           const T vr = vr0 * k, vi = vi0 * k;
@@ -324,8 +326,13 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
               *cell = cur;
             }
           }
-        }
-        if (np > 32) {  // pairs 32 .. np - 1, one tap per lane (warp-uniform loop)
+        };
+        if (lane < np) spread(lane_dq, lane_dz);  // pair lane: (dya + lane / W, lane % W)
+        if constexpr (W >= 7) {
+          // W = 7, 8: up to 49 / 64 pairs; pairs 32 .. np - 1 take a second
+          // round of the same form, pair lane + 32 per lane
+          if (np > 32 && lane < np - 32) spread(lane_dq2, lane_dz2);
+        } else if (np > 32) {  // W <= 6: at most 4 more pairs, one tap per lane
           const int nt = (np - 32) * W;
           for (int t0 = 0; t0 < nt; t0 += 32) {
             const int t = t0 + lane;
