@@ -50,6 +50,15 @@ struct Geom {
   int rowperm;
 };
 
+// Grid rows [r0, r0 + n) that the band-pruned transform's row pass covers:
+// the data band, its row count rounded up to 64 (the row plan's batch).
+__host__ __device__ inline void fft_row_band(const Geom& g, int& r0, int& n) {
+  const int nrows = g.band_r1 - g.band_r0 + 1;
+  n = ((nrows + 63) / 64) * 64;
+  if (n > g.nf2) n = g.nf2;
+  r0 = g.band_r0 < g.nf2 - n ? g.band_r0 : g.nf2 - n;
+}
+
 // storage row of grid index g along dim 1 (identity unless rowperm)
 __host__ __device__ __forceinline__ int row_of(const Geom& g, int g1) {
   return g.rowperm ? g1 / 64 + g.rowperm * (g1 % 64) : g1;

@@ -592,10 +592,10 @@ static int exec_c2c(cg_plan_s* P, cufftHandle h, void* data, int direction) {
 // Falls back to the full 2-D transform when the band saves little.
 static int fft_exec_pruned(cg_plan_s* P, void* d_grid, int direction) {
   const Geom& g = P->geom;
-  const int nrows = g.band_r1 - g.band_r0 + 1;
   if (!fft_is_pruned(P, g)) return fft_exec(P, d_grid, direction);
   // rows plan: batch rounded up to 64 rows (extra rows are zero or unused)
-  int batch = std::min(g.nf2, ((nrows + 63) / 64) * 64);
+  int r0, batch;
+  fft_row_band(g, r0, batch);
   if (!P->rows_valid || P->rows_n != g.nf1 || P->rows_batch != batch) {
     CG_TRY(make_1d_plan(P, P->fft_rows, P->rows_valid, g.nf1, 1, batch));
     P->rows_n = g.nf1;
@@ -612,7 +612,6 @@ static int fft_exec_pruned(cg_plan_s* P, void* d_grid, int direction) {
   }
   const size_t esz = (P->precision == CG_PREC_FP64) ? 16 : 8;
   const size_t plane = (size_t)g.nf1 * g.nf2;
-  const int r0 = std::min(g.band_r0, g.nf2 - batch);
   char* base = (char*)d_grid;
   auto rows = [&](int p) { return exec_c2c(P, P->fft_rows, base + esz * (p * plane + (size_t)r0 * g.nf1), direction); };
   auto cols = [&](int p) {

@@ -148,8 +148,15 @@ __global__ void k_plane_fill(const T* __restrict__ dirty, Geom g, const double* 
   const int col = inv_cmcl(g0, g.N1, g.nf1), row = inv_cmcl(g1, g.N2, g.nf2);
   if (col < 0 || row < 0) {
     // cells in the image's columns but outside its rows are neither loaded
-    // nor kept by the one-pass forward column transform: no zeros needed
-    if (g.fill_skip && col >= 0) return;
+    // nor kept by the one-pass forward column transform, and cells outside
+    // the image's columns are read only by the row pass, in its rows: no
+    // zeros needed elsewhere
+    if (g.fill_skip) {
+      if (col >= 0) return;
+      int r0, n;
+      fft_row_band(g, r0, n);
+      if (g1 < r0 || g1 >= r0 + n) return;
+    }
     V zero;
     zero.x = (T)0;
     zero.y = (T)0;
