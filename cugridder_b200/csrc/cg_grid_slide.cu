@@ -197,6 +197,11 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
   const int lane_dq2 = (lane + 32) / W, lane_dz2 = lane + 32 - lane_dq2 * W;  // of round 1
   const int seg = tc.nsegs / 2 + ((ks & 1) ? -((ks + 1) >> 1) : (ks >> 1));
   const int y0 = band * TY, y1 = min(y0 + TY, nf2), wy = y1 - y0;
+  if (g.grid_skip) {  // a band wholly outside the rows the transform reads holds no rows
+    int r0, n;
+    fft_row_band(g, r0, n);
+    if (y1 <= r0 || y0 >= r0 + n) return;
+  }
   const int hs = seg * tc.SEG, he = min(hs + tc.SEG, nhx);
   const int hya = floordiv8(y0 - hi), hyb = floordiv8(y1 - 1 + lo);
   const int nyr = hyb - hya + 1;

@@ -44,6 +44,10 @@ struct Geom {
   // the forward column transform does not load the rows outside the image in
   // the image's columns (one-pass column kernel): the plane fill leaves them
   int fill_skip;
+  // the same skips for ms2dirty: the row pass reads only the rows of
+  // fft_row_band and the column kernel loads no other row, so gridding may
+  // leave the rows outside it unwritten (tiles and bands wholly outside)
+  int grid_skip;
   // four-step column transform active (its L2 = nf2 / 64; 0 = off): grid
   // index g along dim 1 sits at row g / 64 + rowperm * (g % 64) between the
   // column transform and the w stage (see row_of)

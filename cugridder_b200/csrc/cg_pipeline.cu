@@ -476,6 +476,7 @@ static int prepare(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw)
   CG_TRY(ensure(P->recs_tmp, (size_t)nrow * (tsz == 8 ? sizeof(Rec<double>) : sizeof(Rec<float>))));
   P->geom.rowperm = four_step_rows(P, P->geom);
   P->geom.fill_skip = fill_skip_ok(P, P->geom, P->geom.rowperm) ? 1 : 0;
+  P->geom.grid_skip = P->geom.fill_skip;
   return CG_OK;
 }
 
@@ -889,7 +890,9 @@ static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T
   }
   if (part == 1) return CG_OK;
   CG_TRY(autotune_launch<T>(P, 0, (T*)nullptr));
-  CG_TRY(launch_grid<T>((const Rec<T>*)P->recs.p, (const int*)P->hive_start.p, M, g,
+  Geom gg = g;
+  if (P->stop_stage != 0) gg.grid_skip = 0;  // the grid is inspected: every row written
+  CG_TRY(launch_grid<T>((const Rec<T>*)P->recs.p, (const int*)P->hive_start.p, M, gg,
                         (T*)P->grid.p, P->grid_method, queue_counter(P), st, &P->tune));
   timer_mark(P);  // 4: gridding
   if (P->stop_stage == 2) return CG_OK;

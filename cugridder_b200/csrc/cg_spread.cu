@@ -270,6 +270,11 @@ __device__ __forceinline__ void grid_warp_tile(
     const int tx0 = tix * TX, ty0 = tiy * TY, p0 = tib * PB;
     const int tx1 = min(tx0 + TX, nf1), ty1 = min(ty0 + TY, nf2), p1 = min(p0 + PB, nw);
     const int wx = tx1 - tx0, wy = ty1 - ty0, wz = p1 - p0;
+    if (g.grid_skip) {  // a tile wholly outside the rows the transform reads holds no rows
+      int r0, n;
+      fft_row_band(g, r0, n);
+      if (ty1 <= r0 || ty0 >= r0 + n) return;
+    }
     // FP32 cells are written two at a time (16 bytes) when every pair is aligned:
     // an even tile width and grid row length and a 16-byte aligned grid
     const bool flush_pairs = sizeof(T) == 4 && ((wx | nf1) & 1) == 0 &&
