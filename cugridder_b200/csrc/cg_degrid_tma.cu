@@ -37,7 +37,9 @@ constexpr int kWaitTries = 1 << 20;  // bounded barrier wait (well under a secon
 struct TmaTile {
   int TX, TY;        // tile cells (multiples of 8)
   int SX, SY, SZ;    // staged box: SX even >= TX + W + 1, SY = TY + W, SZ = nw
-  int ntx, nty, nitems;
+  int ntx, nty;      // tiles of the grid
+  int bx0, by0, nbx; // the tiles of the data band: nbx per band row, from tile (bx0, by0)
+  int nitems;        // tiles of the data band (the queue's items)
   int nslots;        // segment slots of a tile's own hives
   size_t stage_bytes;  // one stage, rounded up to 1024 bytes
 };
@@ -121,7 +123,7 @@ __global__ void __launch_bounds__(NT, NS == 1 ? (NT <= 128 ? 3 : 2) : 1) k_degri
       if (lane == 0) item = atomicAdd(counter, 1);
       item = __shfl_sync(0xffffffffu, item, 0);
       if (item >= tc.nitems) return tc.nitems;
-      const int tix = item % tc.ntx, tiy = item / tc.ntx;
+      const int tix = tc.bx0 + item % tc.nbx, tiy = tc.by0 + item / tc.nbx;
       const int tx0 = tix * tc.TX, ty0 = tiy * tc.TY;
       const int hx0 = tx0 >> 3, hx1 = (min(tx0 + tc.TX, nf1) - 1) >> 3;
       const int hy0 = ty0 >> 3, nhyr = ((min(ty0 + tc.TY, nf2) - 1) >> 3) - hy0 + 1;
@@ -136,7 +138,7 @@ __global__ void __launch_bounds__(NT, NS == 1 ? (NT <= 128 ? 3 : 2) : 1) k_degri
   };
   // box origin of a tile (x rounded down to even) and whether it lies inside the grid
   auto origin = [&](int item, int& gx0, int& gy0) {
-    const int tix = item % tc.ntx, tiy = item / tc.ntx;
+    const int tix = tc.bx0 + item % tc.nbx, tiy = tc.by0 + item / tc.nbx;
     gx0 = (tix * tc.TX - lo) & ~1;
     gy0 = tiy * tc.TY - lo;
     return gx0 >= 0 && gy0 >= 0 && gx0 + SX <= nf1 && gy0 + SY <= nf2;
@@ -208,7 +210,7 @@ __global__ void __launch_bounds__(NT, NS == 1 ? (NT <= 128 ? 3 : 2) : 1) k_degri
       break;
     }
     // runs of the tile's own hives, all planes
-    const int tix = cur % tc.ntx, tiy = cur / tc.ntx;
+    const int tix = tc.bx0 + cur % tc.nbx, tiy = tc.by0 + cur / tc.nbx;
     const int tx0 = tix * tc.TX, ty0 = tiy * tc.TY;
     const int tx1 = min(tx0 + tc.TX, nf1), ty1 = min(ty0 + tc.TY, nf2);
     int gx0, gy0;
@@ -317,7 +319,21 @@ bool tma_tiling(const Geom& g, TmaTile& tc, int variant) {
   tc.SZ = g.nw;
   tc.ntx = (g.nf1 + tx - 1) / tx;
   tc.nty = (g.nf2 + ty - 1) / ty;
-  tc.nitems = tc.ntx * tc.nty;
+  // only the tiles of the cells the data can reach (the full grid when the
+  // data wraps around an edge): the others hold no rows
+  int bx0 = 0, bx1 = tc.ntx - 1, by0 = 0, by1 = tc.nty - 1;
+  if (0 <= g.band_c0 && g.band_c0 <= g.band_c1 && g.band_c1 < g.nf1) {
+    bx0 = g.band_c0 / tx;
+    bx1 = g.band_c1 / tx;
+  }
+  if (0 <= g.band_r0 && g.band_r0 <= g.band_r1 && g.band_r1 < g.nf2) {
+    by0 = g.band_r0 / ty;
+    by1 = g.band_r1 / ty;
+  }
+  tc.bx0 = bx0;
+  tc.by0 = by0;
+  tc.nbx = bx1 - bx0 + 1;
+  tc.nitems = tc.nbx * (by1 - by0 + 1);
   tc.nslots = ((ty >> 3) + 1) * g.nw * 3;
   tc.stage_bytes = ((size_t)tc.SX * tc.SY * tc.SZ * sizeof(float2) + 1023) & ~(size_t)1023;
   // box dimensions <= 256, grid rows 16-byte multiples; two stages on one
