@@ -93,7 +93,8 @@ struct alignas(16) Rec {
 // TX x TY cells (multiples of the 8x8 hive) times batches of PB planes.
 struct TileCfg {
   int TX, TY, PB;
-  int ntx, nty, npb, nitems;
+  int ntx, nty, npb, nitems;  // tiles per queue row, queue rows, plane batches, items
+  int bx0, by0;               // grid tile of queue item 0 (the data band's first tile)
   int threads;
   size_t smem;
 };

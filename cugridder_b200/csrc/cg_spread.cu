@@ -560,7 +560,8 @@ __device__ __forceinline__ void degrid_tile(const Rec<T>* __restrict__ recs,
   const T* __restrict__ poly = geom_poly<T>(g);
   const size_t plane = (size_t)nf1 * nf2;
   {
-    const int tix = item % tc.ntx, tiy = (item / tc.ntx) % tc.nty, tib = item / (tc.ntx * tc.nty);
+    const int tix = tc.bx0 + item % tc.ntx, tiy = tc.by0 + (item / tc.ntx) % tc.nty,
+              tib = item / (tc.ntx * tc.nty);
     const int tx0 = tix * TX, ty0 = tiy * TY, p0 = all_planes ? 0 : tib * PB;
     const int tx1 = min(tx0 + TX, nf1), ty1 = min(ty0 + TY, nf2);
     const int p1 = all_planes ? nw : min(p0 + PB, nw);
@@ -706,6 +707,16 @@ TileCfg grid_tiling(const Geom& g, bool degrid, const TileTune* tt) {
   tc.PB = PB;
   tc.ntx = (g.nf1 + TX - 1) / TX;
   tc.nty = (g.nf2 + TY - 1) / TY;
+  // degridding: only the tiles of the cells the data can reach (the full grid
+  // when the data wraps around an edge); the others hold no rows
+  if (degrid && 0 <= g.band_c0 && g.band_c0 <= g.band_c1 && g.band_c1 < g.nf1) {
+    tc.bx0 = g.band_c0 / TX;
+    tc.ntx = g.band_c1 / TX - tc.bx0 + 1;
+  }
+  if (degrid && 0 <= g.band_r0 && g.band_r0 <= g.band_r1 && g.band_r1 < g.nf2) {
+    tc.by0 = g.band_r0 / TY;
+    tc.nty = g.band_r1 / TY - tc.by0 + 1;
+  }
   tc.npb = (g.nw + PB - 1) / PB;
   tc.nitems = tc.ntx * tc.nty * tc.npb;
   tc.threads = threads;
