@@ -193,8 +193,8 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
   // light ones
   const int kb = item / tc.nsegs, ks = item - kb * tc.nsegs;
   const int band = tc.nbands / 2 + ((kb & 1) ? -((kb + 1) >> 1) : (kb >> 1));
-  const int lane_dq = lane / W, lane_dz = lane - lane_dq * W;  // pair offsets of round 0
-  const int lane_dq2 = (lane + 32) / W, lane_dz2 = lane + 32 - lane_dq2 * W;  // of round 1
+  const int lane_dq = lane / W, lane_dz = lane - lane_dq * W;  // pair offsets, first pass of pairs
+  const int lane_dq2 = (lane + 32) / W, lane_dz2 = lane + 32 - lane_dq2 * W;  // second pass of pairs
   const int seg = tc.nsegs / 2 + ((ks & 1) ? -((ks + 1) >> 1) : (ks >> 1));
   const int y0 = band * TY, y1 = min(y0 + TY, nf2), wy = y1 - y0;
   if (g.grid_skip) {  // a band wholly outside the rows the transform reads holds no rows
@@ -335,7 +335,7 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
         if (lane < np) spread(lane_dq, lane_dz);  // pair lane: (dya + lane / W, lane % W)
         if constexpr (W >= 7) {
           // W = 7, 8: up to 49 / 64 pairs; pairs 32 .. np - 1 take a second
-          // round of the same form, pair lane + 32 per lane
+          // pass of the same form, pair lane + 32 per lane
           if (np > 32 && lane < np - 32) spread(lane_dq2, lane_dz2);
         } else if (np > 32) {  // W <= 6: at most 4 more pairs, one tap per lane
           const int nt = (np - 32) * W;
