@@ -12,10 +12,13 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <limits>
 #include <sched.h>
 #include <string>
+#include <condition_variable>
+#include <functional>
 #include <thread>
 #include <vector>
 
@@ -287,6 +290,180 @@ void scan_uvw_host(const F* uvw, int64_t nrow, unsigned long long out[7]) {
   out[6] = (unsigned long long)(r.bad ? 1 : 0);
 }
 
+// ---------------------------------------------------------------- pageable host buffers
+// The reference's callers (its Python binding passes numpy arrays) hand the
+// host entry points ordinary pageable memory, which the DMA engine cannot
+// read directly: a plain cudaMemcpyAsync then copies through the driver's
+// own staging at about 10 GB/s.  Here worker threads copy each chunk into
+// one of a few pinned staging buffers while the DMA engine moves the
+// previous chunk, so both run at once.
+
+// A fixed team of worker threads running one job over all of them at a time.
+class CopyTeam {
+ public:
+  explicit CopyTeam(int n) : n_(n) {
+    for (int i = 1; i < n_; i++) th_.emplace_back([this, i] { work(i); });
+  }
+  ~CopyTeam() {
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : th_) t.join();
+  }
+  int size() const { return n_; }
+  // fn(i) for i in [0, n), the caller running i = 0; returns when all are done
+  void run(const std::function<void(int)>& fn) {
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      job_ = &fn;
+      pending_ = n_ - 1;
+      gen_++;
+    }
+    cv_.notify_all();
+    fn(0);
+    std::unique_lock<std::mutex> lk(m_);
+    done_.wait(lk, [this] { return pending_ == 0; });
+    job_ = nullptr;
+  }
+
+ private:
+  void work(int i) {
+    long seen = 0;
+    for (;;) {
+      const std::function<void(int)>* job;
+      {
+        std::unique_lock<std::mutex> lk(m_);
+        cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+        job = job_;
+      }
+      (*job)(i);
+      std::lock_guard<std::mutex> lk(m_);
+      if (--pending_ == 0) done_.notify_one();
+    }
+  }
+  int n_;
+  std::vector<std::thread> th_;
+  std::mutex m_;
+  std::condition_variable cv_, done_;
+  const std::function<void(int)>* job_ = nullptr;
+  long gen_ = 0;
+  int pending_ = 0;
+  bool stop_ = false;
+};
+
+int host_threads() {
+  cpu_set_t cs;
+  int ncpu = 1;
+  if (sched_getaffinity(0, sizeof(cs), &cs) == 0) ncpu = std::max(1, CPU_COUNT(&cs));
+  return std::min(16, ncpu);
+}
+
+// Pinned staging: kBufs buffers of kChunk bytes, each with the event of the
+// last copy that used it.  Used by one call at a time (the caller holds
+// g_cache_mu); allocated on the first pageable copy.
+struct Staging {
+  static constexpr size_t kChunk = 8u << 20;
+  static constexpr int kBufs = 4;
+  void* buf[kBufs] = {};
+  cudaEvent_t ev[kBufs] = {};
+  int dev = -1;
+  std::unique_ptr<CopyTeam> team;
+};
+Staging g_staging;
+
+int staging_ready() {
+  int dev = 0;
+  CG_CUDA(cudaGetDevice(&dev));
+  Staging& S = g_staging;
+  if (S.buf[0] && S.dev == dev) return CG_OK;
+  for (int b = 0; b < Staging::kBufs; b++) {
+    if (!S.buf[b]) CG_CUDA(cudaHostAlloc(&S.buf[b], Staging::kChunk, cudaHostAllocPortable));
+    if (S.ev[b]) cudaEventDestroy(S.ev[b]);  // events belong to the device current at creation
+    CG_CUDA(cudaEventCreateWithFlags(&S.ev[b], cudaEventDisableTiming));
+  }
+  S.dev = dev;
+  if (!S.team) S.team.reset(new CopyTeam(host_threads()));
+  return CG_OK;
+}
+
+// whole-team memcpy of n bytes
+void team_copy(void* dst, const void* src, size_t n) {
+  CopyTeam& T = *g_staging.team;
+  const int k = T.size();
+  T.run([&](int i) {
+    const size_t a = n * i / k, b = n * (i + 1) / k;
+    if (b > a) std::memcpy((char*)dst + a, (const char*)src + a, b - a);
+  });
+}
+
+// pageable: memory the DMA engine cannot read directly (not pinned or
+// registered, not device or managed memory); small copies go direct
+bool staged(const void* host, size_t bytes) {
+  if (bytes < (2u << 20)) return false;
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, host) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeUnregistered;
+}
+
+// host -> device on stream st; returns when the last chunk is handed to the
+// DMA engine (the copies complete in stream order)
+int copy_h2d(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (!staged(src, bytes)) {
+    CG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+    return CG_OK;
+  }
+  CG_TRY(staging_ready());
+  Staging& S = g_staging;
+  int k = 0;
+  for (size_t off = 0; off < bytes; off += Staging::kChunk, k++) {
+    const int b = k % Staging::kBufs;
+    const size_t n = std::min(Staging::kChunk, bytes - off);
+    CG_CUDA(cudaEventSynchronize(S.ev[b]));  // the copy that last read buffer b is done
+    team_copy(S.buf[b], (const char*)src + off, n);
+    CG_CUDA(cudaMemcpyAsync((char*)dst + off, S.buf[b], n, cudaMemcpyHostToDevice, st));
+    CG_CUDA(cudaEventRecord(S.ev[b], st));
+  }
+  return CG_OK;
+}
+
+// device -> host on stream st (after the work queued on it); returns when
+// every byte is in dst
+int copy_d2h(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  if (!staged(dst, bytes)) {
+    CG_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+    CG_CUDA(cudaStreamSynchronize(st));
+    return CG_OK;
+  }
+  CG_TRY(staging_ready());
+  Staging& S = g_staging;
+  const size_t nchunks = (bytes + Staging::kChunk - 1) / Staging::kChunk;
+  auto issue = [&](size_t k) -> int {
+    const int b = (int)(k % Staging::kBufs);
+    const size_t off = k * Staging::kChunk, n = std::min(Staging::kChunk, bytes - off);
+    CG_CUDA(cudaMemcpyAsync(S.buf[b], (const char*)src + off, n, cudaMemcpyDeviceToHost, st));
+    CG_CUDA(cudaEventRecord(S.ev[b], st));
+    return CG_OK;
+  };
+  // keep kBufs - 1 chunks in flight ahead of the one being drained
+  const size_t ahead = std::min<size_t>(nchunks, Staging::kBufs - 1);
+  for (size_t k = 0; k < ahead; k++) CG_TRY(issue(k));
+  for (size_t k = 0; k < nchunks; k++) {
+    const int b = (int)(k % Staging::kBufs);
+    const size_t off = k * Staging::kChunk, n = std::min(Staging::kChunk, bytes - off);
+    if (k + ahead < nchunks) CG_TRY(issue(k + ahead));  // buffer (k + ahead) % kBufs was drained
+    CG_CUDA(cudaEventSynchronize(S.ev[b]));
+    team_copy((char*)dst + off, S.buf[b], n);
+  }
+  return CG_OK;
+}
+
 // Host-pointer driver shared by every host entry point.
 // uvw_is_float: uvw given in float (reference -DSINGLE API), widened on device.
 int host_call(bool to_dirty, int precision, int64_t nrow, int nx, int ny, double fov,
@@ -345,12 +522,12 @@ int host_call(bool to_dirty, int precision, int64_t nrow, int nx, int ny, double
     if (nrow <= 0) return CG_OK;
     if (uvw_is_float) {
       float* d_f = (float*)(d_uvw + n_uvw);
-      CG_CUDA(cudaMemcpyAsync(d_f, uvw, n_uvw * 4, cudaMemcpyHostToDevice, s2));
+      CG_TRY(copy_h2d(d_f, uvw, n_uvw * 4, s2));
       k_widen_uvw<<<592, 256, 0, s2>>>(d_f, d_uvw, (int64_t)n_uvw);
       cg::count_launches(1);
       CG_CUDA(cudaGetLastError());
     } else {
-      CG_CUDA(cudaMemcpyAsync(d_uvw, uvw, n_uvw * 8, cudaMemcpyHostToDevice, s2));
+      CG_TRY(copy_h2d(d_uvw, uvw, n_uvw * 8, s2));
     }
     CG_CUDA(cudaEventRecord(P->io_ev_uvw, s2));
     return CG_OK;
@@ -358,15 +535,15 @@ int host_call(bool to_dirty, int precision, int64_t nrow, int nx, int ny, double
   if (to_dirty) {
     CG_TRY(copy_uvw());
     if (nrow > 0)
-      CG_CUDA(cudaMemcpyAsync(P->io_vis.p, vis, (size_t)nrow * 2 * tsz, cudaMemcpyHostToDevice, s2));
+      CG_TRY(copy_h2d(P->io_vis.p, vis, (size_t)nrow * 2 * tsz, s2));
     CG_CUDA(cudaEventRecord(P->io_ev_main, s2));
   } else {
-    CG_CUDA(cudaMemcpyAsync(P->io_dirty.p, dirty, (size_t)nx * ny * 2 * tsz, cudaMemcpyHostToDevice, s2));
+    CG_TRY(copy_h2d(P->io_dirty.p, dirty, (size_t)nx * ny * 2 * tsz, s2));
     CG_CUDA(cudaEventRecord(P->io_ev_main, s2));
     CG_TRY(copy_uvw());
   }
   if (nrow > 0 && wgt)
-    CG_CUDA(cudaMemcpyAsync(P->io_wgt.p, wgt, (size_t)nrow * tsz, cudaMemcpyHostToDevice, s2));
+    CG_TRY(copy_h2d(P->io_wgt.p, wgt, (size_t)nrow * tsz, s2));
   CG_CUDA(cudaEventRecord(P->io_event, s2));
   P->main_ready = P->io_ev_main;
   P->inputs_ready = P->io_event;
@@ -377,7 +554,10 @@ int host_call(bool to_dirty, int precision, int64_t nrow, int nx, int ny, double
   // binning waits for uvw anyway and is done before the visibilities are in)
   unsigned long long host_mm[7];
   const char* hr = getenv("CG_HOST_RANGES");  // 0: the device range pass instead (A/B timing)
-  if (!to_dirty && !(hr && atoi(hr) == 0)) {
+  // a pageable uvw was staged before this point, so the device pass on it
+  // is already possible and the host scan would only add its own time
+  const bool uvw_staged = nrow > 0 && staged(uvw, n_uvw * (uvw_is_float ? 4 : 8));
+  if (!to_dirty && !(hr && atoi(hr) == 0) && !uvw_staged) {
     if (uvw_is_float)
       scan_uvw_host((const float*)uvw, nrow, host_mm);
     else
@@ -389,12 +569,12 @@ int host_call(bool to_dirty, int precision, int64_t nrow, int nx, int ny, double
     rs = cg::ms2dirty_device(P, nrow, freq, d_uvw, P->io_vis.p, wgt ? P->io_wgt.p : nullptr,
                              P->io_dirty.p);
     if (rs > 1) return rs;
-    CG_CUDA(cudaMemcpyAsync(dirty, P->io_dirty.p, (size_t)nx * ny * 2 * tsz, cudaMemcpyDeviceToHost, s));
+    CG_TRY(copy_d2h(dirty, P->io_dirty.p, (size_t)nx * ny * 2 * tsz, s));
   } else {
     rs = cg::dirty2ms_device(P, nrow, freq, d_uvw, P->io_dirty.p, wgt ? P->io_wgt.p : nullptr,
                              P->io_vis.p);
     if (rs > 1) return rs;
-    if (nrow > 0) CG_CUDA(cudaMemcpyAsync(vis, P->io_vis.p, (size_t)nrow * 2 * tsz, cudaMemcpyDeviceToHost, s));
+    if (nrow > 0) CG_TRY(copy_d2h(vis, P->io_vis.p, (size_t)nrow * 2 * tsz, s));
   }
   CG_CUDA(cudaStreamSynchronize(s));
   return rs;
