@@ -506,6 +506,8 @@ int host_call(bool to_dirty, int precision, int64_t nrow, int nx, int ny, double
       P->main_ready = nullptr;
       P->uvw_ready = nullptr;
       P->host_mm = nullptr;
+      P->spec_pending = false;
+      P->spec_hit = false;
       cudaStreamSynchronize(P->io_stream);
       cudaStreamSynchronize(P->aux_stream);
       cudaStreamSynchronize(P->stream);
@@ -557,7 +559,12 @@ int host_call(bool to_dirty, int precision, int64_t nrow, int nx, int ny, double
   // a pageable uvw was staged before this point, so the device pass on it
   // is already possible and the host scan would only add its own time
   const bool uvw_staged = nrow > 0 && staged(uvw, n_uvw * (uvw_is_float ? 4 : 8));
-  if (!to_dirty && !(hr && atoi(hr) == 0) && !uvw_staged) {
+  // dirty2ms with the last call's rows and frequency: the plane fill and FFT
+  // start on its geometry now, and the device range pass confirms it
+  const char* sp = getenv("CG_SPECULATE");  // 0: never (A/B timing)
+  if (!to_dirty && !(sp && atoi(sp) == 0))
+    CG_TRY(cg::dirty2ms_speculate(P, nrow, freq, P->io_dirty.p));
+  if (!to_dirty && !(hr && atoi(hr) == 0) && !uvw_staged && !P->spec_pending) {
     if (uvw_is_float)
       scan_uvw_host((const float*)uvw, nrow, host_mm);
     else

@@ -127,6 +127,12 @@ int ms2dirty_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw
                     const void* d_vis, const void* d_wgt, void* d_dirty);
 int dirty2ms_device(cg_plan_s* P, int64_t nrow, double freq, const double* d_uvw,
                     const void* d_dirty, const void* d_wgt, void* d_vis);
+// Host entry points: when the plan's last call had this call's row count and
+// frequency, start dirty2ms's plane fill and FFT on aux_stream with that
+// call's geometry as soon as the image (P->main_ready) is in, before uvw.  The
+// call's own range pass then confirms the geometry (same u, v, w ranges) or
+// discards the work and redoes it.
+int dirty2ms_speculate(cg_plan_s* P, int64_t nrow, double freq, const void* d_dirty);
 // Calls split at the spreading step (batched solves): ms2dirty part 1 runs
 // the stages before gridding, part 2 those after it; dirty2ms_split runs the
 // stages before degridding.  *split = false when the call ran whole (no

@@ -92,6 +92,14 @@ struct cg_plan_s {
   // quadrature (reset when the plan is reconfigured)
   bool quarter_valid = false;
   double quarter_key[7] = {};
+  // the u, v, w ranges (range words 0-5), row count and frequency the current
+  // geometry was built from (spec_valid), for dirty2ms_speculate: a plane fill
+  // and FFT started on that geometry (spec_pending) and confirmed by the
+  // call's range pass (spec_hit)
+  bool spec_valid = false, spec_pending = false, spec_hit = false;
+  unsigned long long spec_mm[6] = {};
+  int64_t spec_nrow = -1;
+  double spec_freq = 0;
   const double* last_uvw = nullptr;
   int64_t last_nrow = -1;
   double last_freq = 0;
