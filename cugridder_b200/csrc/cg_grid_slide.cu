@@ -150,15 +150,15 @@ template <typename T, int W, bool kPoly>
 __device__ __forceinline__ void eval_kv(const unsigned char* stg, int src, T* kv, int lane,
                                         int axis, int tap, const T (&pc)[kPolyCoef], T beta,
                                         T ces, T halfw) {
-  if (lane < 3 * W) {
-    const T f = reinterpret_cast<const T*>(stg + src * kCandBytes<T>)[axis];
-    T v;
-    if constexpr (kPoly)
-      v = poly_eval(pc, poly_arg<W>(f));
-    else
-      v = es_kernel<T>((T)(tap_offset<W>(f) + tap) - f, beta, ces, halfw);
-    kv[lane] = v;
-  }
+  // every lane evaluates (lanes from 3W on repeat axis 2), only 3W store:
+  // straight-line code that can interleave with the taps around it
+  const T f = reinterpret_cast<const T*>(stg + src * kCandBytes<T>)[axis < 3 ? axis : 2];
+  T v;
+  if constexpr (kPoly)
+    v = poly_eval(pc, poly_arg<W>(f));
+  else
+    v = es_kernel<T>((T)(tap_offset<W>(f) + tap) - f, beta, ces, halfw);
+  if (lane < 3 * W) kv[lane] = v;
 }
 
 template <typename T, int W, bool kPoly>
@@ -312,24 +312,30 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
           const T k = ky * kz;
           const T vr = vr0 * k, vi = vi0 * k;
           C* a = acc + (vy + dy) * RS + z * kPS;
+          // all W loads first, then the FMAs, then the stores: the loads are
+          // in flight together
+          C cur[W];
           if (xs + W <= kXW) {  // the row's taps do not wrap the window (same for all lanes)
             C* b = a + xs;
 #pragma unroll
-            for (int e = 0; e < W; e++) {
-              C cur = b[e];
-              cur.x += vr * kx[e];
-              cur.y += vi * kx[e];
-              b[e] = cur;
-            }
-          } else {
+            for (int e = 0; e < W; e++) cur[e] = b[e];
 #pragma unroll
             for (int e = 0; e < W; e++) {
-              C* cell = a + ((xs + e) & (kXW - 1));
-              C cur = *cell;
-              cur.x += vr * kx[e];
-              cur.y += vi * kx[e];
-              *cell = cur;
+              cur[e].x += vr * kx[e];
+              cur[e].y += vi * kx[e];
             }
+#pragma unroll
+            for (int e = 0; e < W; e++) b[e] = cur[e];
+          } else {
+#pragma unroll
+            for (int e = 0; e < W; e++) cur[e] = a[(xs + e) & (kXW - 1)];
+#pragma unroll
+            for (int e = 0; e < W; e++) {
+              cur[e].x += vr * kx[e];
+              cur[e].y += vi * kx[e];
+            }
+#pragma unroll
+            for (int e = 0; e < W; e++) a[(xs + e) & (kXW - 1)] = cur[e];
           }
         };
         if (lane < np) spread(lane_dq, lane_dz);  // pair lane: (dya + lane / W, lane % W)

@@ -398,15 +398,19 @@ __device__ __forceinline__ void grid_warp_tile(
             const T k = ky * kz;
             const T vr = vr0 * k, vi = vi0 * k;
             C* a = acc + z * PS + y * RS + vx;
+            // the taps' loads first, then the FMAs, then the stores
+            C cur[W];
+#pragma unroll
+            for (int e = 0; e < W; e++)
+              if (xmask & (1u << e)) cur[e] = a[e];
 #pragma unroll
             for (int e = 0; e < W; e++) {
-              if (xmask & (1u << e)) {
-                C cur = a[e];
-                cur.x += vr * kx[e];
-                cur.y += vi * kx[e];
-                a[e] = cur;
-              }
+              cur[e].x += vr * kx[e];
+              cur[e].y += vi * kx[e];
             }
+#pragma unroll
+            for (int e = 0; e < W; e++)
+              if (xmask & (1u << e)) a[e] = cur[e];
           }
         }
         if constexpr (kTail) {
