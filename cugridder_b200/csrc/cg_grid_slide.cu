@@ -195,6 +195,9 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
   const int band = tc.nbands / 2 + ((kb & 1) ? -((kb + 1) >> 1) : (kb >> 1));
   const int lane_dq = lane / W, lane_dz = lane - lane_dq * W;  // pair offsets, first pass of pairs
   const int lane_dq2 = (lane + 32) / W, lane_dz2 = lane + 32 - lane_dq2 * W;  // second pass of pairs
+  // W <= 6: tap lane of the pairs beyond 32, pair 32 + lane / W, x tap lane % W
+  const int tail_e = lane % W, tail_p = 32 + lane / W;
+  const int tail_dq = tail_p / W, tail_dz = tail_p - tail_dq * W;
   const int seg = tc.nsegs / 2 + ((ks & 1) ? -((ks + 1) >> 1) : (ks >> 1));
   const int y0 = band * TY, y1 = min(y0 + TY, nf2), wy = y1 - y0;
   if (g.grid_skip) {  // a band wholly outside the rows the transform reads holds no rows
@@ -313,7 +316,30 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
           const T vr = vr0 * k, vi = vi0 * k;
           C* a = acc + (vy + dy) * RS + z * kPS;
           // all W loads first, then the FMAs, then the stores: the loads are
-          // in flight together
+          // in flight together (FP32, and FP64 up to W = 6; FP64 W = 7, 8 take
+          // a load, FMA and store per tap, at half the registers)
+          if constexpr (sizeof(T) == 8 && W > 6) {
+            if (xs + W <= kXW) {
+              C* b = a + xs;
+#pragma unroll
+              for (int e = 0; e < W; e++) {
+                C cv = b[e];
+                cv.x += vr * kx[e];
+                cv.y += vi * kx[e];
+                b[e] = cv;
+              }
+            } else {
+#pragma unroll
+              for (int e = 0; e < W; e++) {
+                C* c = a + ((xs + e) & (kXW - 1));
+                C cv = *c;
+                cv.x += vr * kx[e];
+                cv.y += vi * kx[e];
+                *c = cv;
+              }
+            }
+            return;
+          }
           C cur[W];
           if (xs + W <= kXW) {  // the row's taps do not wrap the window (same for all lanes)
             C* b = a + xs;
@@ -343,13 +369,10 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
           // W = 7, 8: up to 49 / 64 pairs; pairs 32 .. np - 1 take a second
           // pass of the same form, pair lane + 32 per lane
           if (np > 32 && lane < np - 32) spread(lane_dq2, lane_dz2);
-        } else if (np > 32) {  // W <= 6: at most 4 more pairs, one tap per lane
-          const int nt = (np - 32) * W;
-          for (int t0 = 0; t0 < nt; t0 += 32) {
-            const int t = t0 + lane;
-            const int pq = t / W, e = t - pq * W, p = 32 + pq;
-            const int dq = p / W, dz = p - dq * W, dy = dya + dq;
-            if (t < nt) {
+        } else if (np > 32) {  // W <= 6: at most 4 more pairs (24 taps), one tap per lane
+          if (lane < (np - 32) * W) {
+            const int e = tail_e, dz = tail_dz, dy = dya + tail_dq;
+            {
               const T ky = kv[W + dy], kz = kv[2 * W + dz], kxe = kv[e];
               int z = vz + dz;
               z += z < 0 ? nw : (z >= nw ? -nw : 0);
