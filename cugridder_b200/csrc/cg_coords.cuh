@@ -113,6 +113,22 @@ __device__ __forceinline__ int taps(T f, T beta, T c, const T* __restrict__ poly
   return o;
 }
 
+// Tap update c + (vr, vi) * k of a complex cell: for FP32 one packed
+// fma.rn.f32x2 (sm_100), which rounds each half as fma.rn.f32 does, so the
+// result is the same as two scalar FMAs.
+__device__ __forceinline__ float2 tap_fma(float2 c, float vr, float vi, float k) {
+  float2 r;
+  asm("{\n.reg .b64 pv, pk, pc, pr;\n"
+      "mov.b64 pv, {%2, %3};\nmov.b64 pk, {%4, %4};\nmov.b64 pc, {%5, %6};\n"
+      "fma.rn.f32x2 pr, pv, pk, pc;\nmov.b64 {%0, %1}, pr;\n}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(vr), "f"(vi), "f"(k), "f"(c.x), "f"(c.y));
+  return r;
+}
+__device__ __forceinline__ double2 tap_fma(double2 c, double vr, double vi, double k) {
+  return make_double2(fma(vr, k, c.x), fma(vi, k, c.y));
+}
+
 // true modulo (any number of periods)
 __device__ __forceinline__ int modi(int i, int n) {
   i %= n;

@@ -229,27 +229,26 @@ __global__ void __launch_bounds__(NT, NS == 1 ? (NT <= 128 ? 3 : 2) : 1) k_degri
       const int ly = by + taps<float, W>(r.f[1], beta, c, poly, ky) - gy0;
       const int lz = bz + taps<float, W>(r.f[2], beta, c, poly, kz);
       if (lx < 0 || ly < 0 || lx + W > SX || ly + W > SY) continue;  // cannot happen: tile rows only
-      float sr = 0.f, si = 0.f;
+      // complex sums of cells times real kernel values, one packed FMA each
+      float2 s2 = make_float2(0.f, 0.f);
 #pragma unroll
       for (int a = 0; a < W; a++) {
         const int zz = wrapi(lz + a, nw);
-        float pr = 0.f, pi = 0.f;
+        float2 p2 = make_float2(0.f, 0.f);
 #pragma unroll
         for (int b = 0; b < W; b++) {
           const float2* row = st + ((size_t)zz * SY + (ly + b)) * SX + lx;
-          float qr = 0.f, qi = 0.f;
+          float2 q2 = make_float2(0.f, 0.f);
 #pragma unroll
           for (int e = 0; e < W; e++) {
             const float2 v = row[e];
-            qr += v.x * kx[e];
-            qi += v.y * kx[e];
+            q2 = tap_fma(q2, v.x, v.y, kx[e]);
           }
-          pr += qr * ky[b];
-          pi += qi * ky[b];
+          p2 = tap_fma(p2, q2.x, q2.y, ky[b]);
         }
-        sr += pr * kz[a];
-        si += pi * kz[a];
+        s2 = tap_fma(s2, p2.x, p2.y, kz[a]);
       }
+      const float sr = s2.x, si = s2.y;
       const int64_t i = perm[sidx];
       if (i < 0 || i >= M) continue;
       vis[2 * i] = sr * r.c[0] - si * r.c[1];

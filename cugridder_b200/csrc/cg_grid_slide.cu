@@ -347,8 +347,7 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
             for (int e = 0; e < W; e++) cur[e] = b[e];
 #pragma unroll
             for (int e = 0; e < W; e++) {
-              cur[e].x += vr * kx[e];
-              cur[e].y += vi * kx[e];
+              cur[e] = tap_fma(cur[e], vr, vi, kx[e]);
             }
 #pragma unroll
             for (int e = 0; e < W; e++) b[e] = cur[e];
@@ -357,8 +356,7 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
             for (int e = 0; e < W; e++) cur[e] = a[(xs + e) & (kXW - 1)];
 #pragma unroll
             for (int e = 0; e < W; e++) {
-              cur[e].x += vr * kx[e];
-              cur[e].y += vi * kx[e];
+              cur[e] = tap_fma(cur[e], vr, vi, kx[e]);
             }
 #pragma unroll
             for (int e = 0; e < W; e++) a[(xs + e) & (kXW - 1)] = cur[e];
@@ -379,8 +377,7 @@ __device__ __forceinline__ void slide_item(const Rec<T>* __restrict__ recs,
               const T k = ky * kz;
               C* cell = acc + (vy + dy) * RS + z * kPS + ((xs + e) & (kXW - 1));
               C cur = *cell;
-              cur.x += vr0 * k * kxe;
-              cur.y += vi0 * k * kxe;
+              cur = tap_fma(cur, vr0 * k, vi0 * k, kxe);
               *cell = cur;
             }
           }

@@ -411,8 +411,7 @@ __device__ __forceinline__ void grid_warp_tile(
                 if (xmask & (1u << e)) cur[e] = a[e];
 #pragma unroll
               for (int e = 0; e < W; e++) {
-                cur[e].x += vr * kx[e];
-                cur[e].y += vi * kx[e];
+                cur[e] = tap_fma(cur[e], vr, vi, kx[e]);
               }
 #pragma unroll
               for (int e = 0; e < W; e++)
@@ -422,8 +421,7 @@ __device__ __forceinline__ void grid_warp_tile(
               for (int e = 0; e < W; e++) {
                 if (xmask & (1u << e)) {
                   C cur = a[e];
-                  cur.x += vr * kx[e];
-                  cur.y += vi * kx[e];
+                  cur = tap_fma(cur, vr, vi, kx[e]);
                   a[e] = cur;
                 }
               }
@@ -451,8 +449,7 @@ __device__ __forceinline__ void grid_warp_tile(
               const T vr = vr0 * k, vi = vi0 * k;
               C* a = acc + z * PS + y * RS + x;
               C cur = *a;
-              cur.x += vr * kxe;
-              cur.y += vi * kxe;
+              cur = tap_fma(cur, vr, vi, kxe);
               *a = cur;
             }
           }
