@@ -18,7 +18,9 @@
 // captured into a CUDA graph and every later call replays it.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <numeric>
 #include <vector>
 
@@ -70,6 +72,13 @@ struct cg_batch_s {
   bool jobs_ready[2] = {false, false};
   cg::TileTune tune{};
   float tuned_ms[2] = {0.f, 0.f};
+  // row-split heavy gridding tiles: host copies of the datasets' hive offsets
+  // (read back once: the uvw are fixed), the split tables and their device
+  // copies, the partial tiles' scratch
+  std::vector<std::vector<int>> hs_host;
+  std::vector<cg::SplitItem> split_host;  // chunk items, then one entry per split tile
+  std::vector<int> split_flags;
+  cg_dev_buf split_dev, flags_dev, parts_dev;
 };
 
 namespace {
@@ -82,6 +91,9 @@ void destroy_batch(cg_batch_s* B) {
     cg::release(B->jobs[d]);
     cg::release(B->counter[d]);
   }
+  cg::release(B->split_dev);
+  cg::release(B->flags_dev);
+  cg::release(B->parts_dev);
   for (auto P : B->plans) cg_plan_destroy(P);
   for (auto& b : B->uvw_chan) cg::release(b);
   for (auto& b : B->scales) cg::release(b);
@@ -112,11 +124,168 @@ int join_streams(cg_batch_s* B, cudaStream_t origin) {
   return CG_OK;
 }
 
+int floordiv8_host(int a) { return a >= 0 ? a >> 3 : -((7 - a) >> 3); }
+
+// Rows of the hive slots of every warp tile of job J (the rows its segment
+// table walks: the hives of the tile and its kernel halo) from the hive
+// offsets hs, exclusive prefix sums in (plane, hive row, hive column) order.
+void tile_rows(const cg::Geom& g, const cg::WarpTile& wt, const std::vector<int>& hs,
+               std::vector<int64_t>& rows) {
+  const int nhx = g.nhx, nhy = g.nhy, nhz = g.nhz;
+  const int lo = (g.kw - 1) / 2, hi = (g.kw + 1) / 2;
+  // [a, b] of a periodic axis of n as at most two intervals inside [0, n)
+  auto wrap = [](int a, int b, int n, int (&iv)[2][2]) {
+    if (b - a + 1 >= n) {
+      iv[0][0] = 0; iv[0][1] = n - 1;
+      return 1;
+    }
+    a = ((a % n) + n) % n;
+    b = ((b % n) + n) % n;
+    if (a <= b) {
+      iv[0][0] = a; iv[0][1] = b;
+      return 1;
+    }
+    iv[0][0] = a; iv[0][1] = n - 1;
+    iv[1][0] = 0; iv[1][1] = b;
+    return 2;
+  };
+  rows.assign((size_t)wt.nitems, 0);
+  for (int item = 0; item < wt.nitems; item++) {
+    const int tix = item % wt.ntx, tiy = (item / wt.ntx) % wt.nty, tib = item / (wt.ntx * wt.nty);
+    const int tx0 = tix * wt.TX, ty0 = tiy * wt.TY, p0 = tib * wt.PB;
+    const int tx1 = std::min(tx0 + wt.TX, g.nf1), ty1 = std::min(ty0 + wt.TY, g.nf2);
+    const int p1 = std::min(p0 + wt.PB, g.nw);
+    int ix[2][2], iy[2][2], iz[2][2];
+    const int nx = wrap(floordiv8_host(tx0 - hi), floordiv8_host(tx1 - 1 + lo), nhx, ix);
+    const int ny = wrap(floordiv8_host(ty0 - hi), floordiv8_host(ty1 - 1 + lo), nhy, iy);
+    const int nz = wrap(p0 - hi, p1 - 1 + lo, nhz, iz);
+    int64_t n = 0;
+    for (int a = 0; a < nz; a++)
+      for (int z = iz[a][0]; z <= iz[a][1]; z++)
+        for (int b = 0; b < ny; b++)
+          for (int y = iy[b][0]; y <= iy[b][1]; y++) {
+            const int64_t r = ((int64_t)z * nhy + y) * nhx;
+            for (int c = 0; c < nx; c++) n += hs[r + ix[c][1] + 1] - hs[r + ix[c][0]];
+          }
+    rows[item] = n;
+  }
+}
+
+// Row-split plan of the gridding launch's warp tiles.  A warp grids one tile's
+// rows alone, so a tile holding far more than a warp's share of the launch
+// (the centre of a dense small grid: 3% of a 19M-visibility dataset in one
+// 16 x 8 tile) sets the launch's length.  Tiles with more than R rows, R about
+// a quarter of a warp's share, become ceil(rows / R) chunk items at the head
+// of the queue, each into a partial tile that k_split_reduce sums in chunk
+// order.  Rows per tile come from the hive offsets, read back once (the
+// batch's uvw are fixed); a chunk takes its share of the rows the kernel
+// itself counts, so the estimate only sets the number of chunks.
+// CG_BATCH_SPLIT=0 turns this off, CG_BATCH_SPLIT_ROWS sets R.
+template <typename T>
+int plan_splits(cg_batch_s* B, std::vector<cg::GridJob<T>>& jobs, const std::vector<int>& order,
+                cg::MultiShape* sh, cudaStream_t st) {
+  using C = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
+  B->split_host.clear();
+  B->split_flags.clear();
+  const char* off = std::getenv("CG_BATCH_SPLIT");
+  if (off && std::atoi(off) == 0) return CG_OK;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CG_CUDA(cudaStreamIsCapturing(st, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return CG_OK;  // planned by the eager first call only
+  if (B->hs_host.size() != B->ds.size()) B->hs_host.assign(B->ds.size(), {});
+  bool copied = false;
+  for (size_t j = 0; j < jobs.size(); j++) {
+    const cg::Geom& g = jobs[j].g;
+    const size_t nh1 = (size_t)g.nhx * g.nhy * g.nhz + 1;
+    std::vector<int>& hs = B->hs_host[order[j]];
+    if (hs.size() == nh1) continue;
+    hs.resize(nh1);
+    CG_CUDA(cudaMemcpyAsync(hs.data(), jobs[j].hive_start, nh1 * sizeof(int),
+                            cudaMemcpyDeviceToHost, st));
+    copied = true;
+  }
+  if (copied) CG_CUDA(cudaStreamSynchronize(st));
+  std::vector<std::vector<int64_t>> rows(jobs.size());
+  int64_t V = 0;
+  for (size_t j = 0; j < jobs.size(); j++) {
+    tile_rows(jobs[j].g, jobs[j].wt, B->hs_host[order[j]], rows[j]);
+    for (int64_t r : rows[j]) V += r;
+  }
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int64_t warps = (int64_t)sms * std::max(1, sh->warps);
+  int64_t R = std::max<int64_t>(2048, (V + 4 * warps - 1) / (4 * warps));
+  if (const char* e = std::getenv("CG_BATCH_SPLIT_ROWS")) R = std::max<int64_t>(1, std::atoll(e));
+  constexpr int kMaxChunks = 1024;
+  constexpr size_t kMaxParts = (size_t)1 << 30;  // scratch bytes at most
+  struct Heavy {
+    int job, tile, nchunks;
+    int64_t rows;
+  };
+  std::vector<Heavy> heavy;
+  size_t parts = 0;
+  for (;;) {  // R doubles until the partial tiles fit the scratch bound
+    heavy.clear();
+    parts = 0;
+    for (size_t j = 0; j < jobs.size(); j++) {
+      const cg::WarpTile& wt = jobs[j].wt;
+      for (int t = 0; t < wt.nitems; t++) {
+        const int64_t r = rows[j][t];
+        if (r <= R) continue;
+        const int k = (int)std::min<int64_t>(kMaxChunks, (r + R - 1) / R);
+        heavy.push_back({(int)j, t, k, r});
+        parts += (size_t)k * wt.TX * wt.TY * wt.PB * sizeof(C);
+      }
+    }
+    if (parts <= kMaxParts) break;
+    R *= 2;
+  }
+  if (heavy.empty()) return CG_OK;
+  std::stable_sort(heavy.begin(), heavy.end(), [](const Heavy& a, const Heavy& b) { return a.rows > b.rows; });
+  // flags of the jobs that have split tiles, one device array
+  std::vector<int64_t> flag0(jobs.size(), -1);
+  for (const Heavy& h : heavy)
+    if (flag0[h.job] < 0) {
+      flag0[h.job] = (int64_t)B->split_flags.size();
+      B->split_flags.resize(B->split_flags.size() + jobs[h.job].wt.nitems, 0);
+    }
+  for (const Heavy& h : heavy) B->split_flags[flag0[h.job] + h.tile] = 1;
+  std::vector<cg::SplitItem> tiles;
+  long long offc = 0;  // complex cells
+  for (const Heavy& h : heavy) {
+    const cg::WarpTile& wt = jobs[h.job].wt;
+    const long long slot = (long long)wt.TX * wt.TY * wt.PB;
+    tiles.push_back({h.job, h.tile, 0, h.nchunks, offc});
+    for (int c = 0; c < h.nchunks; c++)
+      B->split_host.push_back({h.job, h.tile, c, h.nchunks, offc + c * slot});
+    offc += (long long)h.nchunks * slot;
+  }
+  const size_t nsplit = B->split_host.size();
+  if (nsplit + (size_t)sh->grid_items > 2147483647u) return CG_ERR_SIZE;
+  B->split_host.insert(B->split_host.end(), tiles.begin(), tiles.end());
+  CG_TRY(cg::ensure(B->split_dev, B->split_host.size() * sizeof(cg::SplitItem)));
+  CG_TRY(cg::ensure(B->flags_dev, B->split_flags.size() * sizeof(int)));
+  CG_TRY(cg::ensure(B->parts_dev, std::max<size_t>(parts, 256)));
+  CG_CUDA(cudaMemcpyAsync(B->split_dev.p, B->split_host.data(),
+                          B->split_host.size() * sizeof(cg::SplitItem), cudaMemcpyHostToDevice, st));
+  CG_CUDA(cudaMemcpyAsync(B->flags_dev.p, B->split_flags.data(), B->split_flags.size() * sizeof(int),
+                          cudaMemcpyHostToDevice, st));
+  for (size_t j = 0; j < jobs.size(); j++)
+    jobs[j].tile_split = flag0[j] < 0 ? nullptr : (const int*)B->flags_dev.p + flag0[j];
+  sh->nsplit = (int)nsplit;
+  sh->nsplit_tiles = (int)tiles.size();
+  sh->d_split = (const cg::SplitItem*)B->split_dev.p;
+  sh->d_split_tiles = (const cg::SplitItem*)B->split_dev.p + nsplit;
+  sh->d_parts = B->parts_dev.p;
+  return CG_OK;
+}
+
 // Jobs of the split datasets for tiling tt, heaviest rows-per-item first so
 // that the queue ends on light items; fills the shape.
 template <typename T>
 int build_jobs(cg_batch_s* B, int dir, const cg::TileTune& tt, std::vector<cg::GridJob<T>>& jobs,
-               std::vector<int>& order, cg::MultiShape* shape) {
+               std::vector<int>& order, cg::MultiShape* shape, cudaStream_t st) {
   jobs.clear();
   order.clear();
   for (size_t i = 0; i < B->ds.size(); i++) {
@@ -146,7 +315,9 @@ int build_jobs(cg_batch_s* B, int dir, const cg::TileTune& tt, std::vector<cg::G
   }
   jobs.swap(sorted);
   order.swap(sorted_order);
-  return cg::multi_shape<T>(jobs.data(), (int)jobs.size(), shape);
+  CG_TRY(cg::multi_shape<T>(jobs.data(), (int)jobs.size(), shape));
+  if (dir == 0 && !shape->slide) CG_TRY(plan_splits<T>(B, jobs, order, shape, st));
+  return CG_OK;
 }
 
 template <typename T>
@@ -193,7 +364,7 @@ int prepare_phase2(cg_batch_s* B, int dir, cudaStream_t st) {
       if (dir == 0 && cand[c][0] < 0) continue;
       cg::TileTune tt = B->tune;
       cg::set_tile_candidate(tt, dir, cand[c]);
-      if (build_jobs<T>(B, dir, tt, jobs, order, &sh) != CG_OK || jobs.empty()) continue;
+      if (build_jobs<T>(B, dir, tt, jobs, order, &sh, st) != CG_OK || jobs.empty()) continue;
       CG_TRY(upload_jobs<T>(B, dir, jobs, st));
       float ms = 0.f;
       bool ok = true;
@@ -213,7 +384,7 @@ int prepare_phase2(cg_batch_s* B, int dir, cudaStream_t st) {
     B->tune = best_tt;
     B->tuned_ms[dir] = std::max(best, 0.f);
   }
-  CG_TRY(build_jobs<T>(B, dir, B->tune, jobs, order, &sh));
+  CG_TRY(build_jobs<T>(B, dir, B->tune, jobs, order, &sh, st));
   CG_TRY(upload_jobs<T>(B, dir, jobs, st));
   B->job_of[dir] = order;
   B->shape[dir] = sh;

@@ -70,6 +70,17 @@ struct SlideTile {
 // warps) or the defaults; false where the sliding kernel does not apply.
 bool slide_tiling(const Geom& g, size_t tsz, const TileTune* tt, SlideTile& tc);
 
+// Row chunk of a heavy warp tile in a multi-grid gridding launch: chunk
+// `chunk` of `nchunks` of tile `tile` of job `job` spreads its share of the
+// tile's rows into a partial tile (TX x TY x PB complex cells of the job's
+// tiling) at complex offset `off` of the launch's scratch.  Chunks of one tile
+// are consecutive slots; the reduce pass sums them in chunk order into the
+// grid, so results do not depend on which warp ran which chunk.
+struct SplitItem {
+  int job, tile, chunk, nchunks;
+  long long off;
+};
+
 // One grid of a multi-grid launch (batched solves): the plan's sorted stream,
 // hive offsets and grid, its tilings and its first work item in the launch.
 template <typename T>
@@ -86,6 +97,7 @@ struct GridJob {
   TileCfg dt;
   int nslots;       // segment slots of the degridding tiles
   int grid_item0;   // first gridding item of this job (prefix over jobs)
+  const int* tile_split;  // per warp tile: nonzero = gridded by split items (nullptr: none)
   int degrid_item0; // first degridding item of this job
 };
 // Launch shape shared by all jobs of a multi-grid launch.
@@ -99,6 +111,13 @@ struct MultiShape {
   int grid_items, degrid_items;
   bool partial_hives;  // some job's grid has an axis that is not a multiple of 8 cells
   bool slide;          // gridding by x-sliding windows (every job's st set)
+  // row-split heavy warp tiles: nsplit chunk items (first in the queue),
+  // nsplit_tiles reduce entries (chunk 0 of each split tile), the partial
+  // tiles' scratch (complex cells of the working precision)
+  int nsplit, nsplit_tiles;
+  const SplitItem* d_split;
+  const SplitItem* d_split_tiles;
+  void* d_parts;
 };
 // Fill the item prefixes and the shared shape of jobs (host array).
 template <typename T>

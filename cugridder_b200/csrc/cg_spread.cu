@@ -243,11 +243,16 @@ __device__ __forceinline__ void load_lane_poly(const T* __restrict__ poly,
 // warp's shared-memory region `wsmem` and write every cell of it to fw.
 // kExactWrap: halo hive bounds from the wrapped cells (raw_hive_lo/hi), needed
 // when an axis of the grid is not a multiple of 8 cells; otherwise floordiv8.
+// part != nullptr: row chunk `chunk` of `nchunks` of the tile -- rows
+// [total * chunk / nchunks, total * (chunk + 1) / nchunks) of its `total` --
+// into a partial tile at part (cell (x, y, z) at (z * TY + y) * TX + x),
+// written whole (zeros where no row reaches) instead of the grid cells.
 template <typename T, int W, bool kPoly, bool kExactWrap>
 __device__ __forceinline__ void grid_warp_tile(
     const Rec<T>* __restrict__ recs, const int* __restrict__ hive_start, const Geom& g,
     const WarpTile& tc, T* __restrict__ fw, int item, unsigned char* wsmem,
-    const T (&pc)[kPoly ? WarpSpread<W>::NKV : 1][kPolyCoef]) {
+    const T (&pc)[kPoly ? WarpSpread<W>::NKV : 1][kPolyCoef], int chunk = 0, int nchunks = 1,
+    typename Cplx<T>::type* __restrict__ part = nullptr) {
   using C = typename Cplx<T>::type;
   using WS = WarpSpread<W>;
   constexpr int lo = Halo<W>::lo, hi = Halo<W>::hi;
@@ -270,10 +275,16 @@ __device__ __forceinline__ void grid_warp_tile(
     const int tx0 = tix * TX, ty0 = tiy * TY, p0 = tib * PB;
     const int tx1 = min(tx0 + TX, nf1), ty1 = min(ty0 + TY, nf2), p1 = min(p0 + PB, nw);
     const int wx = tx1 - tx0, wy = ty1 - ty0, wz = p1 - p0;
+    auto zero_part = [&]() {
+      for (int i = lane; i < TX * TY * PB; i += 32) part[i] = zero;
+    };
     if (g.grid_skip) {  // a tile wholly outside the rows the transform reads holds no rows
       int r0, n;
       fft_row_band(g, r0, n);
-      if (ty1 <= r0 || ty0 >= r0 + n) return;
+      if (ty1 <= r0 || ty0 >= r0 + n) {
+        if (part) zero_part();
+        return;
+      }
     }
     // FP32 cells are written two at a time (16 bytes) when every pair is aligned:
     // an even tile width and grid row length and a 16-byte aligned grid
@@ -291,6 +302,15 @@ __device__ __forceinline__ void grid_warp_tile(
                                    p1 - 1 + lo, t);
     const int total = t.pref[nslots];
     __syncwarp();  // every lane has read the table head before it can be rebuilt
+    int qb = 0, qe = total;  // the rows of this item
+    if (part) {
+      qb = (int)((int64_t)total * chunk / nchunks);
+      qe = (int)((int64_t)total * (chunk + 1) / nchunks);
+      if (qb == qe) {
+        zero_part();
+        return;
+      }
+    }
     if (total == 0) {
       if (flush_pairs) {
         const int hx = wx >> 1;
@@ -322,7 +342,7 @@ __device__ __forceinline__ void grid_warp_tile(
     };
     auto load_cand = [&](int q) {
       Cand cd{};
-      cd.ok = q < total;
+      cd.ok = q < qe;
       if (cd.ok) {
         const int sgi = find_segment(t.pref, nslots, q);
         const Rec<T> r = recs[t.start[sgi] + (q - t.pref[sgi])];
@@ -339,10 +359,10 @@ __device__ __forceinline__ void grid_warp_tile(
       T vr0, vi0;
       int vx, vy, vz;
     };
-    Cand nextc = load_cand(lane);
-    for (int q0 = 0; q0 < total; q0 += 32) {
+    Cand nextc = load_cand(qb + lane);
+    for (int q0 = qb; q0 < qe; q0 += 32) {
       const Cand cc = nextc;
-      if (q0 + 32 < total) nextc = load_cand(q0 + 32 + lane);
+      if (q0 + 32 < qe) nextc = load_cand(q0 + 32 + lane);
       const int ox = cc.bx + tap_offset<W>(cc.f0);
       const int oy = cc.by + tap_offset<W>(cc.f1);
       const int oz = cc.bz + tap_offset<W>(cc.f2);
@@ -483,7 +503,13 @@ __device__ __forceinline__ void grid_warp_tile(
       }
     }
     // flush the tile, coalesced along x
-    if (flush_pairs) {
+    if (part) {
+      const TileDiv div_x(TX), div_xy(TX * TY);
+      for (int i = lane; i < TX * TY * PB; i += 32) {
+        const int z = div_xy(i), r = i - z * TX * TY, y = div_x(r), x = r - y * TX;
+        part[i] = acc[z * PS + y * RS + x];
+      }
+    } else if (flush_pairs) {
       const int hx = wx >> 1;
       const TileDiv div_x(hx), div_xy(hx * wy);
       for (int i = lane; i < hx * wy * wz; i += 32) {
@@ -532,10 +558,16 @@ __device__ __forceinline__ int find_job(const J* __restrict__ jobs, int njobs, i
 // Many grids in one persistent launch: warps take (job, tile) items from a
 // global queue; every job shares W and the kernel.  warp_bytes is the largest
 // per-warp footprint of the jobs' tilings.
+// Items [0, nsplit) are the row chunks of the heavy tiles (splits), the
+// others the jobs' tiles in job order; a tile with split chunks is skipped
+// there.
 template <typename T, int W, bool kPoly, bool kExactWrap>
 __global__ void __launch_bounds__(512) k_grid_warp_multi(const GridJob<T>* __restrict__ jobs,
                                                          int njobs, int nitems, size_t warp_bytes,
-                                                         int* __restrict__ counter) {
+                                                         int* __restrict__ counter,
+                                                         const SplitItem* __restrict__ splits,
+                                                         int nsplit,
+                                                         typename Cplx<T>::type* __restrict__ parts) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   T pc[kPoly ? WarpSpread<W>::NKV : 1][kPolyCoef];
@@ -545,11 +577,53 @@ __global__ void __launch_bounds__(512) k_grid_warp_multi(const GridJob<T>* __res
     int item = 0;
     if (lane == 0) item = atomicAdd(counter, 1);
     item = __shfl_sync(0xffffffffu, item, 0);
-    if (item >= nitems) break;
+    if (item >= nsplit + nitems) break;
+    if (item < nsplit) {
+      const SplitItem si = splits[item];
+      const GridJob<T>& J = jobs[si.job];
+      grid_warp_tile<T, W, kPoly, kExactWrap>(J.recs, J.hive_start, J.g, J.wt, J.fw, si.tile, wsmem,
+                                              pc, si.chunk, si.nchunks, parts + si.off);
+      continue;
+    }
+    item -= nsplit;
     const int j = find_job(jobs, njobs, item, [](const GridJob<T>& x) { return x.grid_item0; });
     const GridJob<T>& J = jobs[j];
-    grid_warp_tile<T, W, kPoly, kExactWrap>(J.recs, J.hive_start, J.g, J.wt, J.fw, item - J.grid_item0, wsmem,
-                                pc);
+    const int tile = item - J.grid_item0;
+    if (J.tile_split && J.tile_split[tile]) continue;  // gridded by its split items
+    grid_warp_tile<T, W, kPoly, kExactWrap>(J.recs, J.hive_start, J.g, J.wt, J.fw, tile, wsmem, pc);
+  }
+}
+
+// Sum of the partial tiles of each split tile (tiles[blockIdx.x]: chunk 0 of
+// its nchunks, chunks at consecutive slots) in chunk order, into its cells.
+template <typename T>
+__global__ void __launch_bounds__(256) k_split_reduce(const GridJob<T>* __restrict__ jobs,
+                                                      const SplitItem* __restrict__ tiles,
+                                                      const typename Cplx<T>::type* __restrict__ parts) {
+  using C = typename Cplx<T>::type;
+  const SplitItem si = tiles[blockIdx.x];
+  const GridJob<T>& J = jobs[si.job];
+  const WarpTile& tc = J.wt;
+  const Geom& g = J.g;
+  const int item = si.tile;
+  const int tix = item % tc.ntx, tiy = (item / tc.ntx) % tc.nty, tib = item / (tc.ntx * tc.nty);
+  const int tx0 = tix * tc.TX, ty0 = tiy * tc.TY, p0 = tib * tc.PB;
+  const int wx = min(tx0 + tc.TX, g.nf1) - tx0, wy = min(ty0 + tc.TY, g.nf2) - ty0;
+  const int wz = min(p0 + tc.PB, g.nw) - p0;
+  const size_t slot = (size_t)tc.TX * tc.TY * tc.PB;
+  const size_t plane = (size_t)g.nf1 * g.nf2;
+  C* fwc = reinterpret_cast<C*>(J.fw);
+  const C* base = parts + si.off;
+  for (int i = threadIdx.x; i < wx * wy * wz; i += blockDim.x) {
+    const int z = i / (wx * wy), r = i - z * wx * wy, y = r / wx, x = r - y * wx;
+    const size_t cell = ((size_t)z * tc.TY + y) * tc.TX + x;
+    C s = base[cell];
+    for (int k = 1; k < si.nchunks; k++) {
+      const C v = base[(size_t)k * slot + cell];
+      s.x += v.x;
+      s.y += v.y;
+    }
+    fwc[(size_t)(p0 + z) * plane + (size_t)(ty0 + y) * g.nf1 + tx0 + x] = s;
   }
 }
 
@@ -997,12 +1071,20 @@ static int grid_multi_w(const GridJob<T>* d_jobs, int njobs, const MultiShape& s
     set_last_error("multi-grid gridding does not fit on an SM");
     return CG_ERR_ARG;
   }
-  const int blocks = std::min((sh.grid_items + sh.warps - 1) / sh.warps, per_sm * num_sms());
+  const int items = sh.grid_items + sh.nsplit;
+  const int blocks = std::min((items + sh.warps - 1) / sh.warps, per_sm * num_sms());
+  using C = typename Cplx<T>::type;
   CG_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(int), st));
   kern<<<std::max(1, blocks), sh.warps * 32, smem, st>>>(d_jobs, njobs, sh.grid_items, sh.warp_bytes,
-                                                         d_counter);
+                                                         d_counter, sh.d_split, sh.nsplit,
+                                                         (C*)sh.d_parts);
   count_launches(1);
   CG_CUDA(cudaGetLastError());
+  if (sh.nsplit_tiles > 0) {
+    k_split_reduce<T><<<sh.nsplit_tiles, 256, 0, st>>>(d_jobs, sh.d_split_tiles, (const C*)sh.d_parts);
+    count_launches(1);
+    CG_CUDA(cudaGetLastError());
+  }
   return CG_OK;
 }
 

@@ -279,3 +279,70 @@ def test_batch_channel_flattening_vs_direct_sums(torch_cuda):
                                      d["freqs"][c], pixels=pix) for c in range(nchan))
         assert rel_l2(images[i].reshape(-1)[pix], truth_d) < 2e-4, i
     b.close()
+
+
+def _split_datasets(torch, prec):
+    """Square datasets of SPECS plus one whose rows sit near its grid centre
+    (u, v scaled by 0.05: most rows in a few tiles), in precision prec."""
+    cdt, rdt = (np.complex64, np.float32) if prec == "fp32" else (np.complex128, np.float64)
+    tdt = torch.complex64 if prec == "fp32" else torch.complex128
+    specs = [s for s in SPECS if s[0] == s[1] and s[3] > 0] + [(64, 64, 2.0, 40000, 2)]
+    out = []
+    for i, (n, _, fov, nrow, nchan) in enumerate(specs):
+        d = synth.make("ms2dirty_256_fp64", seed=600 + i, nrow=nrow, nx=n, ny=n, fov=fov)
+        uvw = d["uvw"].copy()
+        if i == len(specs) - 1:
+            uvw[:, :2] *= 0.05
+        freqs = np.linspace(1.0e8, 2.0e8, nchan) if nchan > 1 else np.array([1.0e8])
+        rng = np.random.Generator(np.random.PCG64(700 + i))
+        vis = (rng.standard_normal((nrow, nchan)) + 1j * rng.standard_normal((nrow, nchan))).astype(cdt)
+        wgt = rng.uniform(0.5, 1.5, (nrow, nchan)).astype(rdt)
+        out.append(dict(uvw=to_dev(torch, uvw), freqs=freqs, vis=to_dev(torch, vis),
+                        wgt=to_dev(torch, wgt), fov=fov, h_uvw=uvw, h_wgt=wgt, h_vis=vis,
+                        dirty=torch.zeros((n, n), dtype=tdt, device="cuda")))
+    return out
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_batch_split_tiles(torch_cuda, monkeypatch, prec):
+    """Heavy warp tiles gridded as row chunks into partial tiles summed in
+    chunk order (CG_BATCH_SPLIT_ROWS=300: chunks of at most 300 rows, so the
+    dense dataset's central tiles split many ways) against the same batch
+    unsplit (CG_BATCH_SPLIT=0), one plan per dataset and the oracle, through
+    the eager, captured and replayed calls.  The captured call launches one
+    kernel more than the unsplit one: the reduce pass."""
+    from cugridder_b200 import _lib
+
+    torch = torch_cuda
+    lib = _lib.load()
+    eps, tol_split, tol_oracle = (1e-4, 2e-6, 2e-5) if prec == "fp32" else (1e-9, 1e-13, 1e-10)
+    ds = _split_datasets(torch, prec)
+
+    def run(env, ncalls):
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
+        b = Batch(ds, epsilon=eps, precision=prec)
+        outs, launches = [], []
+        for call in range(ncalls):  # eager (autotuned, split plan), captured, replayed
+            l0 = lib.cg_kernel_launches()
+            b.ms2dirty()
+            torch.cuda.synchronize()
+            launches.append(lib.cg_kernel_launches() - l0)
+            outs.append([d["dirty"].cpu().numpy().copy() for d in ds])
+        tiling = b.tiling()
+        b.close()
+        for k in env:
+            monkeypatch.delenv(k)
+        return outs, launches, tiling
+
+    ref, ref_launches, ref_tiling = run({"CG_BATCH_SPLIT": "0", "CG_BATCH_AUTOTUNE": "0"}, 2)
+    outs, launches, tiling = run({"CG_BATCH_SPLIT_ROWS": "300", "CG_BATCH_AUTOTUNE": "0"}, 3)
+    assert tiling[0] == ref_tiling[0]
+    assert launches[1] == ref_launches[1] + 1, (launches, ref_launches)
+    for call in range(3):
+        for i, d in enumerate(ds):
+            assert rel_l2(outs[call][i], ref[0][i]) < tol_split, (call, i)
+    for i, d in enumerate(ds):
+        assert _close_oracle(outs[2][i], d, 0, eps, tol=tol_oracle), i
+        if prec == "fp32":
+            assert _close(outs[2][i], _plan_ref(torch, d, 0)), i
