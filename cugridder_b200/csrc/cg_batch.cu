@@ -26,6 +26,7 @@
 
 #include "cg_launch.cuh"
 #include "cg_plan.cuh"
+#include "cg_tiles.cuh"
 
 namespace {
 
@@ -124,53 +125,6 @@ int join_streams(cg_batch_s* B, cudaStream_t origin) {
   return CG_OK;
 }
 
-int floordiv8_host(int a) { return a >= 0 ? a >> 3 : -((7 - a) >> 3); }
-
-// Rows of the hive slots of every warp tile of job J (the rows its segment
-// table walks: the hives of the tile and its kernel halo) from the hive
-// offsets hs, exclusive prefix sums in (plane, hive row, hive column) order.
-void tile_rows(const cg::Geom& g, const cg::WarpTile& wt, const std::vector<int>& hs,
-               std::vector<int64_t>& rows) {
-  const int nhx = g.nhx, nhy = g.nhy, nhz = g.nhz;
-  const int lo = (g.kw - 1) / 2, hi = (g.kw + 1) / 2;
-  // [a, b] of a periodic axis of n as at most two intervals inside [0, n)
-  auto wrap = [](int a, int b, int n, int (&iv)[2][2]) {
-    if (b - a + 1 >= n) {
-      iv[0][0] = 0; iv[0][1] = n - 1;
-      return 1;
-    }
-    a = ((a % n) + n) % n;
-    b = ((b % n) + n) % n;
-    if (a <= b) {
-      iv[0][0] = a; iv[0][1] = b;
-      return 1;
-    }
-    iv[0][0] = a; iv[0][1] = n - 1;
-    iv[1][0] = 0; iv[1][1] = b;
-    return 2;
-  };
-  rows.assign((size_t)wt.nitems, 0);
-  for (int item = 0; item < wt.nitems; item++) {
-    const int tix = item % wt.ntx, tiy = (item / wt.ntx) % wt.nty, tib = item / (wt.ntx * wt.nty);
-    const int tx0 = tix * wt.TX, ty0 = tiy * wt.TY, p0 = tib * wt.PB;
-    const int tx1 = std::min(tx0 + wt.TX, g.nf1), ty1 = std::min(ty0 + wt.TY, g.nf2);
-    const int p1 = std::min(p0 + wt.PB, g.nw);
-    int ix[2][2], iy[2][2], iz[2][2];
-    const int nx = wrap(floordiv8_host(tx0 - hi), floordiv8_host(tx1 - 1 + lo), nhx, ix);
-    const int ny = wrap(floordiv8_host(ty0 - hi), floordiv8_host(ty1 - 1 + lo), nhy, iy);
-    const int nz = wrap(p0 - hi, p1 - 1 + lo, nhz, iz);
-    int64_t n = 0;
-    for (int a = 0; a < nz; a++)
-      for (int z = iz[a][0]; z <= iz[a][1]; z++)
-        for (int b = 0; b < ny; b++)
-          for (int y = iy[b][0]; y <= iy[b][1]; y++) {
-            const int64_t r = ((int64_t)z * nhy + y) * nhx;
-            for (int c = 0; c < nx; c++) n += hs[r + ix[c][1] + 1] - hs[r + ix[c][0]];
-          }
-    rows[item] = n;
-  }
-}
-
 // Row-split plan of the gridding launch's warp tiles.  A warp grids one tile's
 // rows alone, so a tile holding far more than a warp's share of the launch
 // (the centre of a dense small grid: 3% of a 19M-visibility dataset in one
@@ -208,8 +162,12 @@ int plan_splits(cg_batch_s* B, std::vector<cg::GridJob<T>>& jobs, const std::vec
   std::vector<std::vector<int64_t>> rows(jobs.size());
   int64_t V = 0;
   for (size_t j = 0; j < jobs.size(); j++) {
-    tile_rows(jobs[j].g, jobs[j].wt, B->hs_host[order[j]], rows[j]);
-    for (int64_t r : rows[j]) V += r;
+    const cg::WarpTile& wt = jobs[j].wt;
+    rows[j].resize((size_t)wt.nitems);
+    for (int t = 0; t < wt.nitems; t++) {
+      rows[j][t] = cg::tile_slot_rows(B->hs_host[order[j]].data(), jobs[j].g, wt, t);
+      V += rows[j][t];
+    }
   }
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess)

@@ -375,6 +375,10 @@ size_t bin_workspace_bytes(int64_t M, int key_bytes) {
          align256((size_t)nsums * 4);
 }
 
+int launch_scan_exclusive(const int* d_in, int64_t n, int* d_out, int* d_sums, cudaStream_t st) {
+  return scan_exclusive(d_in, n, d_out, d_sums, st);
+}
+
 template <typename K>
 static int bin_impl(const double* d_uvw, int64_t M, const Geom& g, void* d_ws, int* d_perm,
                     K* d_sorted_keys, int* d_hive_start, cudaStream_t st, int* d_hs_sums) {

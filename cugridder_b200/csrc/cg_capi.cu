@@ -126,7 +126,8 @@ void destroy_plan(cg_plan_s* P) {
   cg_dev_buf* bs[] = {&P->mm,   &P->K1,    &P->K2,     &P->K3q,    &P->zq,     &P->grid,
                       &P->recs, &P->perm,  &P->skeys,  &P->hive_start, &P->binws, &P->fftwork,
                       &P->io_uvw, &P->io_vis, &P->io_wgt, &P->io_dirty, &P->polyf, &P->polyd, &P->recs_tmp,
-                      &P->chan_uvw, &P->chan_scale, &P->coltw, &P->acc, &P->roots};
+                      &P->chan_uvw, &P->chan_scale, &P->coltw, &P->acc, &P->roots,
+                      &P->split_chunks, &P->split_sums, &P->split_parts};
   for (auto b : bs) cg::release(*b);
   if (P->h_mm) cudaFreeHost(P->h_mm);
   if (P->io_stream) cudaStreamDestroy(P->io_stream);

@@ -3,6 +3,8 @@
 #pragma once
 #include "cg_internal.cuh"
 
+struct cg_dev_buf;
+
 namespace cg {
 
 // ---- binning (cg_bin.cu) ----
@@ -19,6 +21,9 @@ int launch_bin(const double* d_uvw, int64_t M, const Geom& g, int key_bytes, voi
                size_t ws_bytes, int* d_perm, void* d_sorted_keys, int* d_hive_start,
                cudaStream_t st, int* d_hs_sums = nullptr);
 inline int64_t hive_sums_ints(int64_t nh) { return (nh + 1 + 4095) / 4096; }
+// Exclusive scan of n int32 counters (in place allowed); d_sums holds
+// hive_sums_ints(n - 1) ints.
+int launch_scan_exclusive(const int* d_in, int64_t n, int* d_out, int* d_sums, cudaStream_t st);
 int launch_sort_u32(uint32_t* d_keys, int64_t M, int bits, void* d_ws, size_t ws_bytes,
                     int* d_perm, uint32_t* d_sorted, cudaStream_t st);
 
@@ -28,6 +33,13 @@ int launch_build_stream(const int* d_perm, int64_t M, const double* d_uvw, const
                         Rec<T>* d_recs, cudaStream_t st);
 
 // ---- spreading / interpolation (cg_spread.cu) ----
+// Device scratch of a plan's row-split warp tiles (see launch_grid): the
+// buffers grow on first use and are kept by the plan.
+struct SplitScratch {
+  cg_dev_buf* chunks;  // per tile: chunks, then their exclusive scan (int)
+  cg_dev_buf* sums;    // the scan's workspace
+  cg_dev_buf* parts;   // partial tiles
+};
 // method 0: direct (global atomics / global gathers); 1: tiled (shared memory).
 // d_counter: one device int used as the work-queue head of the tiled kernels.
 constexpr int kGridDirect = 0;
@@ -136,10 +148,12 @@ int plan_grid_job(const cg_plan_s* P, const TileTune& tt, T* d_vis, GridJob<T>* 
 template <typename T>
 int launch_degrid_multi(const GridJob<T>* d_jobs, int njobs, const MultiShape& sh, int* d_counter,
                         cudaStream_t st);
-// tt: tiling choices (nullptr = defaults)
+// tt: tiling choices (nullptr = defaults); sp: scratch for the row split of
+// heavy warp tiles (nullptr: no split)
 template <typename T>
 int launch_grid(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, const Geom& g, T* d_fw,
-                int method, int* d_counter, cudaStream_t st, const TileTune* tt = nullptr);
+                int method, int* d_counter, cudaStream_t st, const TileTune* tt = nullptr,
+                const SplitScratch* sp = nullptr);
 template <typename T>
 int launch_degrid(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_start, int64_t M,
                   const Geom& g, const T* d_fw, T* d_vis, int method, int* d_counter,

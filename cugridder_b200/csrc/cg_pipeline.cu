@@ -186,7 +186,7 @@ size_t workspace_bytes(const cg_plan_s* P) {
   const cg_dev_buf* bs[] = {&P->mm,   &P->K1,    &P->K2,         &P->K3q,   &P->zq,
                             &P->grid, &P->recs,  &P->recs_tmp, &P->perm,       &P->skeys, &P->hive_start,
                             &P->binws, &P->fftwork, &P->io_uvw, &P->io_vis, &P->io_wgt,
-                            &P->io_dirty};
+                            &P->io_dirty, &P->split_chunks, &P->split_sums, &P->split_parts};
   size_t s = 0;
   for (auto b : bs) s += b->cap;
   return s;
@@ -784,10 +784,11 @@ static int autotune_launch(cg_plan_s* P, int dir, T* d_vis) {
       std::equal(key, key + 4, P->tuned_key[dir]))
     return CG_OK;
   cudaStream_t st = P->stream;
+  const SplitScratch split{&P->split_chunks, &P->split_sums, &P->split_parts};
   auto launch = [&](const TileTune& tt) {
     return dir == 0 ? launch_grid<T>((const Rec<T>*)P->recs.p, (const int*)P->hive_start.p,
                                      P->nrow, g, (T*)P->grid.p, P->grid_method,
-                                     queue_counter(P), st, &tt)
+                                     queue_counter(P), st, &tt, &split)
                     : degrid_dispatch<T>(P, tt, d_vis);
   };
   cudaEvent_t e0, e1;
@@ -905,8 +906,9 @@ static int ms2dirty_t(cg_plan_s* P, const double* d_uvw, const T* d_vis, const T
   CG_TRY(autotune_launch<T>(P, 0, (T*)nullptr));
   Geom gg = g;
   if (P->stop_stage != 0) gg.grid_skip = 0;  // the grid is inspected: every row written
+  const SplitScratch split{&P->split_chunks, &P->split_sums, &P->split_parts};
   CG_TRY(launch_grid<T>((const Rec<T>*)P->recs.p, (const int*)P->hive_start.p, M, gg,
-                        (T*)P->grid.p, P->grid_method, queue_counter(P), st, &P->tune));
+                        (T*)P->grid.p, P->grid_method, queue_counter(P), st, &P->tune, &split));
   timer_mark(P);  // 4: gridding
   if (P->stop_stage == 2) return CG_OK;
   return ms2dirty_tail<T>(P, d_dirty);

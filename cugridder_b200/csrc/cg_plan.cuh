@@ -64,6 +64,9 @@ struct cg_plan_s {
   // device buffers
   cg_dev_buf mm, K1, K2, K3q, zq, grid, recs, perm, skeys, hive_start, binws, fftwork, io_uvw,
       io_vis, io_wgt, io_dirty, polyf, polyd, recs_tmp, chan_uvw, chan_scale, coltw, acc, roots;
+  // row split of heavy warp tiles in gridding (chunks per tile and their
+  // scan, the scan's workspace, the partial tiles)
+  cg_dev_buf split_chunks, split_sums, split_parts;
   unsigned long long* h_mm = nullptr;  // pinned, 2 words + flag
   // cuFFT: full 2-D batched plan, and the 1-D plans of the band-pruned path
   cufftHandle fft = 0;

@@ -25,6 +25,7 @@
 
 #include "cg_coords.cuh"
 #include "cg_launch.cuh"
+#include "cg_plan.cuh"
 #include "cg_tiles.cuh"
 
 namespace cg {
@@ -530,18 +531,117 @@ __device__ __forceinline__ void grid_warp_tile(
   }
 }
 
+// Tile t of chunk slot `slot` (chunk_off: exclusive scan of the tiles'
+// chunks, entry nitems = their total, slot below it): the last t with
+// chunk_off[t] <= slot.
+__device__ __forceinline__ int chunk_tile(const int* __restrict__ chunk_off, int nitems, int slot) {
+  int lo = 0, hi = nitems;  // chunk_off[lo] <= slot < chunk_off[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (chunk_off[mid] <= slot) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Warps take items from an atomic queue.  With row splitting (chunk_off set)
+// items [0, cap) are chunk slots: slot s below the chunks' total is chunk
+// s - chunk_off[t] of tile t, into partial tile s, when all of t's chunks fit
+// below cap; items from cap on are the tiles, a tile whose chunks ran is
+// skipped there and one whose chunks did not fit is gridded whole.
 template <typename T, int W, bool kPoly, bool kExactWrap>
 __global__ void __launch_bounds__(512) k_grid_warp(const Rec<T>* __restrict__ recs,
                                                    const int* __restrict__ hive_start, Geom g,
-                                                   WarpTile tc, T* __restrict__ fw) {
+                                                   WarpTile tc, T* __restrict__ fw,
+                                                   int* __restrict__ counter,
+                                                   const int* __restrict__ chunk_off, int cap,
+                                                   typename Cplx<T>::type* __restrict__ parts) {
   extern __shared__ __align__(16) unsigned char smem[];
-  const int wib = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   T pc[kPoly ? WarpSpread<W>::NKV : 1][kPolyCoef];
   load_lane_poly<T, W, kPoly>(geom_poly<T>(g), pc);
   unsigned char* wsmem = smem + (size_t)wib * tc.warp_bytes;
-  const int gwarp = blockIdx.x * tc.warps + wib, nwarps = gridDim.x * tc.warps;
-  for (int item = gwarp; item < tc.nitems; item += nwarps)
-    grid_warp_tile<T, W, kPoly, kExactWrap>(recs, hive_start, g, tc, fw, item, wsmem, pc);
+  const int nslot = chunk_off ? cap : 0;
+  const int total = chunk_off ? chunk_off[tc.nitems] : 0;
+  const size_t slot_cells = (size_t)tc.TX * tc.TY * tc.PB;
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(counter, 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= nslot + tc.nitems) break;
+    if (item < nslot) {
+      if (item >= total) continue;
+      const int t = chunk_tile(chunk_off, tc.nitems, item);
+      const int k0 = chunk_off[t], k1 = chunk_off[t + 1];
+      if (k1 > cap) continue;  // the tile's chunks do not fit: gridded whole below
+      grid_warp_tile<T, W, kPoly, kExactWrap>(recs, hive_start, g, tc, fw, t, wsmem, pc, item - k0,
+                                              k1 - k0, parts + (size_t)item * slot_cells);
+      continue;
+    }
+    const int t = item - nslot;
+    if (chunk_off) {
+      const int k0 = chunk_off[t], k1 = chunk_off[t + 1];
+      if (k1 > k0 && k1 <= cap) continue;  // gridded by its chunks
+    }
+    grid_warp_tile<T, W, kPoly, kExactWrap>(recs, hive_start, g, tc, fw, t, wsmem, pc);
+  }
+}
+
+// Chunks of each warp tile: 0 for a tile with at most R rows in its hive
+// slots, else ceil(rows / R), at most kMaxTileChunks; entry nitems is 0 (the
+// scan then leaves the chunks' total there).
+constexpr int kMaxTileChunks = 1024;
+__global__ void k_tile_chunks(const int* __restrict__ hive_start, Geom g, WarpTile tc, int R,
+                              int* __restrict__ chunks) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t > tc.nitems) return;
+  if (t == tc.nitems) {
+    chunks[t] = 0;
+    return;
+  }
+  const int64_t rows = tile_slot_rows(hive_start, g, tc, t);
+  chunks[t] = rows > R ? (int)min((rows + R - 1) / R, (int64_t)kMaxTileChunks) : 0;
+}
+
+// Sum of a split tile's nchunks partial tiles (base: chunk 0; chunks
+// slot_cells apart) in chunk order, into the tile's grid cells.
+template <typename T>
+__device__ __forceinline__ void split_reduce_tile(const WarpTile& tc, const Geom& g, int item,
+                                                  const typename Cplx<T>::type* __restrict__ base,
+                                                  int nchunks, T* __restrict__ fw) {
+  using C = typename Cplx<T>::type;
+  const int tix = item % tc.ntx, tiy = (item / tc.ntx) % tc.nty, tib = item / (tc.ntx * tc.nty);
+  const int tx0 = tix * tc.TX, ty0 = tiy * tc.TY, p0 = tib * tc.PB;
+  const int wx = min(tx0 + tc.TX, g.nf1) - tx0, wy = min(ty0 + tc.TY, g.nf2) - ty0;
+  const int wz = min(p0 + tc.PB, g.nw) - p0;
+  const size_t slot = (size_t)tc.TX * tc.TY * tc.PB;
+  const size_t plane = (size_t)g.nf1 * g.nf2;
+  C* fwc = reinterpret_cast<C*>(fw);
+  for (int i = threadIdx.x; i < wx * wy * wz; i += blockDim.x) {
+    const int z = i / (wx * wy), r = i - z * wx * wy, y = r / wx, x = r - y * wx;
+    const size_t cell = ((size_t)z * tc.TY + y) * tc.TX + x;
+    C s = base[cell];
+    for (int k = 1; k < nchunks; k++) {
+      const C v = base[(size_t)k * slot + cell];
+      s.x += v.x;
+      s.y += v.y;
+    }
+    fwc[(size_t)(p0 + z) * plane + (size_t)(ty0 + y) * g.nf1 + tx0 + x] = s;
+  }
+}
+
+// One block per chunk slot below cap; the block of a split tile's chunk 0
+// reduces the tile.
+template <typename T>
+__global__ void __launch_bounds__(256) k_split_reduce_plan(const int* __restrict__ chunk_off,
+                                                           WarpTile tc, Geom g, int cap,
+                                                           const typename Cplx<T>::type* __restrict__ parts,
+                                                           T* __restrict__ fw) {
+  const int s = blockIdx.x;
+  if (s >= chunk_off[tc.nitems]) return;
+  const int t = chunk_tile(chunk_off, tc.nitems, s);
+  const int k0 = chunk_off[t], k1 = chunk_off[t + 1];
+  if (s != k0 || k1 > cap) return;
+  split_reduce_tile<T>(tc, g, t, parts + (size_t)k0 * tc.TX * tc.TY * tc.PB, k1 - k0, fw);
 }
 
 // index of the job holding global work item `item` (item0 ascending, item0[0] = 0)
@@ -600,31 +700,9 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_split_reduce(const GridJob<T>* __restrict__ jobs,
                                                       const SplitItem* __restrict__ tiles,
                                                       const typename Cplx<T>::type* __restrict__ parts) {
-  using C = typename Cplx<T>::type;
   const SplitItem si = tiles[blockIdx.x];
   const GridJob<T>& J = jobs[si.job];
-  const WarpTile& tc = J.wt;
-  const Geom& g = J.g;
-  const int item = si.tile;
-  const int tix = item % tc.ntx, tiy = (item / tc.ntx) % tc.nty, tib = item / (tc.ntx * tc.nty);
-  const int tx0 = tix * tc.TX, ty0 = tiy * tc.TY, p0 = tib * tc.PB;
-  const int wx = min(tx0 + tc.TX, g.nf1) - tx0, wy = min(ty0 + tc.TY, g.nf2) - ty0;
-  const int wz = min(p0 + tc.PB, g.nw) - p0;
-  const size_t slot = (size_t)tc.TX * tc.TY * tc.PB;
-  const size_t plane = (size_t)g.nf1 * g.nf2;
-  C* fwc = reinterpret_cast<C*>(J.fw);
-  const C* base = parts + si.off;
-  for (int i = threadIdx.x; i < wx * wy * wz; i += blockDim.x) {
-    const int z = i / (wx * wy), r = i - z * wx * wy, y = r / wx, x = r - y * wx;
-    const size_t cell = ((size_t)z * tc.TY + y) * tc.TX + x;
-    C s = base[cell];
-    for (int k = 1; k < si.nchunks; k++) {
-      const C v = base[(size_t)k * slot + cell];
-      s.x += v.x;
-      s.y += v.y;
-    }
-    fwc[(size_t)(p0 + z) * plane + (size_t)(ty0 + y) * g.nf1 + tx0 + x] = s;
-  }
+  split_reduce_tile<T>(J.wt, J.g, si.tile, parts + si.off, si.nchunks, J.fw);
 }
 
 // ---------------------------------------------------------------- degridding
@@ -910,8 +988,8 @@ WarpTile warp_tiling(const Geom& g, const TileTune* tt) {
 
 template <typename T, int W>
 static int grid_w(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, const Geom& g, T* d_fw,
-                  int method, int* d_counter, cudaStream_t st, const TileTune* tt) {
-  (void)d_counter;
+                  int method, int* d_counter, cudaStream_t st, const TileTune* tt,
+                  const SplitScratch* sp) {
   if (method == kGridDirect) {
     size_t G = (size_t)g.nf1 * g.nf2 * g.nw;
     CG_CUDA(cudaMemsetAsync(d_fw, 0, G * 2 * sizeof(T), st));
@@ -938,10 +1016,45 @@ static int grid_w(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, cons
     set_last_error("warp-tiled gridding does not fit on an SM");
     return CG_ERR_ARG;
   }
-  int blocks = per_sm * num_sms();
-  kern<<<blocks, tc.warps * 32, tc.smem, st>>>(d_recs, d_hive_start, g, tc, d_fw);
+  const int blocks = per_sm * num_sms();
+  // Row split: a warp grids one tile's rows alone, so a tile holding far more
+  // than a warp's share of the launch (the centre of a dense small grid) sets
+  // its length.  A tile with more than R rows in its hive slots, R about a
+  // quarter of a warp's share (each row sits in about 8 tiles' slots), runs
+  // as ceil(rows / R) chunks into partial tiles that k_split_reduce_plan sums
+  // in chunk order.  CG_SPLIT=0 turns it off, CG_SPLIT_ROWS sets R.
+  using C = typename Cplx<T>::type;
+  const int* chunk_off = nullptr;
+  int cap = 0;
+  C* parts = nullptr;
+  if (sp && env_int("CG_SPLIT", 1) && tc.nitems > 0 && M > 0) {
+    const int64_t warps = (int64_t)blocks * tc.warps;
+    int64_t R = std::max<int64_t>(2048, (2 * M + warps - 1) / warps);
+    if (const char* e = getenv("CG_SPLIT_ROWS")) R = std::max<int64_t>(1, atoll(e));
+    R = std::min<int64_t>(R, 2147483647);
+    const size_t slot_bytes = (size_t)tc.TX * tc.TY * tc.PB * sizeof(C);
+    cap = (int)std::max<size_t>(64, ((size_t)64 << 20) / slot_bytes);  // 64 MB of partial tiles
+    CG_TRY(ensure(*sp->chunks, (size_t)(tc.nitems + 1) * sizeof(int)));
+    CG_TRY(ensure(*sp->sums, (size_t)hive_sums_ints(tc.nitems) * sizeof(int)));
+    CG_TRY(ensure(*sp->parts, (size_t)cap * slot_bytes));
+    int* chunks = (int*)sp->chunks->p;
+    k_tile_chunks<<<(tc.nitems + 1 + 255) / 256, 256, 0, st>>>(d_hive_start, g, tc, (int)R, chunks);
+    count_launches(1);
+    CG_CUDA(cudaGetLastError());
+    CG_TRY(launch_scan_exclusive(chunks, (int64_t)tc.nitems + 1, chunks, (int*)sp->sums->p, st));
+    chunk_off = chunks;
+    parts = (C*)sp->parts->p;
+  }
+  CG_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(int), st));
+  kern<<<blocks, tc.warps * 32, tc.smem, st>>>(d_recs, d_hive_start, g, tc, d_fw, d_counter, chunk_off,
+                                               cap, parts);
   count_launches(1);
   CG_CUDA(cudaGetLastError());
+  if (chunk_off) {
+    k_split_reduce_plan<T><<<cap, 256, 0, st>>>(chunk_off, tc, g, cap, parts, d_fw);
+    count_launches(1);
+    CG_CUDA(cudaGetLastError());
+  }
   return CG_OK;
 }
 
@@ -997,7 +1110,8 @@ static int degrid_w(const Rec<T>* d_recs, const int* d_perm, const int* d_hive_s
 
 template <typename T>
 int launch_grid(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, const Geom& g, T* d_fw,
-                int method, int* d_counter, cudaStream_t st, const TileTune* tt) {
+                int method, int* d_counter, cudaStream_t st, const TileTune* tt,
+                const SplitScratch* sp) {
   if (method == kGridMma) {
     // tensor-core path: FP32, ES kernel and W <= 8; everything else on the SIMT kernels
     if (sizeof(T) == 4 && !g.polyf) {
@@ -1006,7 +1120,7 @@ int launch_grid(const Rec<T>* d_recs, const int* d_hive_start, int64_t M, const 
     }
     method = kGridTiled;
   }
-#define CG_GRID_CALL(w) grid_w<T, w>(d_recs, d_hive_start, M, g, d_fw, method, d_counter, st, tt)
+#define CG_GRID_CALL(w) grid_w<T, w>(d_recs, d_hive_start, M, g, d_fw, method, d_counter, st, tt, sp)
   CG_W_SWITCH(g.kw, CG_GRID_CALL)
 #undef CG_GRID_CALL
 }
@@ -1277,9 +1391,9 @@ template int launch_degrid_multi<float>(const GridJob<float>*, int, const MultiS
 template int launch_degrid_multi<double>(const GridJob<double>*, int, const MultiShape&, int*,
                                          cudaStream_t);
 template int launch_grid<float>(const Rec<float>*, const int*, int64_t, const Geom&, float*, int,
-                                int*, cudaStream_t, const TileTune*);
+                                int*, cudaStream_t, const TileTune*, const SplitScratch*);
 template int launch_grid<double>(const Rec<double>*, const int*, int64_t, const Geom&, double*, int,
-                                 int*, cudaStream_t, const TileTune*);
+                                 int*, cudaStream_t, const TileTune*, const SplitScratch*);
 template int launch_degrid<float>(const Rec<float>*, const int*, const int*, int64_t, const Geom&,
                                   const float*, float*, int, int*, cudaStream_t, const TileTune*);
 template int launch_degrid<double>(const Rec<double>*, const int*, const int*, int64_t,

@@ -33,6 +33,51 @@ __device__ __forceinline__ int raw_hive_hi(int b, int nf, int nh) {
   return b >= nf ? nh + ((b - nf) >> 3) : b >> 3;
 }
 
+// Rows in the hive slots of warp tile `item` of tiling wt (the hives of the
+// tile and of its kernel halo, each counted once per periodic axis), from the
+// exclusive hive offsets hs in (plane, hive row, hive column) order: the
+// number of rows the tile's segment table lists, up to the partial-hive edge
+// cases (it sets how many chunks a heavy tile is split into, nothing else).
+__host__ __device__ inline int64_t tile_slot_rows(const int* hs, const Geom& g, const WarpTile& wt,
+                                                  int item) {
+  const int nhx = g.nhx, nhy = g.nhy, nhz = g.nhz;
+  const int lo = (g.kw - 1) / 2, hi = (g.kw + 1) / 2;
+  auto fdiv8 = [](int a) { return a >= 0 ? a >> 3 : -((7 - a) >> 3); };
+  // [a, b] of a periodic axis of n as at most two intervals inside [0, n)
+  auto wrap = [](int a, int b, int n, int* iv) {
+    if (b - a + 1 >= n) {
+      iv[0] = 0; iv[1] = n - 1;
+      return 1;
+    }
+    a = ((a % n) + n) % n;
+    b = ((b % n) + n) % n;
+    if (a <= b) {
+      iv[0] = a; iv[1] = b;
+      return 1;
+    }
+    iv[0] = a; iv[1] = n - 1; iv[2] = 0; iv[3] = b;
+    return 2;
+  };
+  const int tix = item % wt.ntx, tiy = (item / wt.ntx) % wt.nty, tib = item / (wt.ntx * wt.nty);
+  const int tx0 = tix * wt.TX, ty0 = tiy * wt.TY, p0 = tib * wt.PB;
+  const int tx1 = tx0 + wt.TX < g.nf1 ? tx0 + wt.TX : g.nf1;
+  const int ty1 = ty0 + wt.TY < g.nf2 ? ty0 + wt.TY : g.nf2;
+  const int p1 = p0 + wt.PB < g.nw ? p0 + wt.PB : g.nw;
+  int ix[4], iy[4], iz[4];
+  const int nx = wrap(fdiv8(tx0 - hi), fdiv8(tx1 - 1 + lo), nhx, ix);
+  const int ny = wrap(fdiv8(ty0 - hi), fdiv8(ty1 - 1 + lo), nhy, iy);
+  const int nz = wrap(p0 - hi, p1 - 1 + lo, nhz, iz);
+  int64_t n = 0;
+  for (int a = 0; a < nz; a++)
+    for (int z = iz[2 * a]; z <= iz[2 * a + 1]; z++)
+      for (int b = 0; b < ny; b++)
+        for (int y = iy[2 * b]; y <= iy[2 * b + 1]; y++) {
+          const int64_t r = ((int64_t)z * nhy + y) * nhx;
+          for (int c = 0; c < nx; c++) n += hs[r + ix[2 * c + 1] + 1] - hs[r + ix[2 * c]];
+        }
+  return n;
+}
+
 // n / d for a tile index: 0 <= n, 0 < d, n * d < 2^32.  m = floor((2^32 - 1) / d) + 1
 // exceeds 2^32 / d by e = m - 2^32 / d < 1, so n * m / 2^32 = n / d + n * e / 2^32 and
 // the excess n * e / 2^32 < n / 2^32 < 1 / d never carries floor(n / d) over: the
