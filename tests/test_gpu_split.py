@@ -80,3 +80,40 @@ def test_plan_split_tiles(torch_cuda, monkeypatch, prec, learned, nchan):
         assert not np.array_equal(split, whole)  # the chunked sums ran (they round differently)
     assert rel_l2(split, whole) < tol_split
     assert rel_l2(split, _oracle(d, eps, kernel)) < tol_oracle
+
+
+@pytest.mark.parametrize("prec", ["fp32", "fp64"])
+def test_plan_split_tiles_partial_hives(torch_cuda, monkeypatch, prec):
+    """Split tiles on a grid whose axes are not multiples of 8 cells (a 42 x 74
+    image on a 90 x 150 grid: partial last hives, the exact-wrap kernels), with
+    rows over the whole band and aliased past its edge, so that the chunks of
+    edge tiles walk wrapped halo hives."""
+    from oracle import oracle as O
+
+    torch = torch_cuda
+    eps = 1e-4 if prec == "fp32" else 1e-9
+    tol_split, tol_oracle = (2e-6, 2e-5) if prec == "fp32" else (1e-13, 1e-10)
+    cdt, rdt = (np.complex64, np.float32) if prec == "fp32" else (np.complex128, np.float64)
+    tdt = torch.complex64 if prec == "fp32" else torch.complex128
+    d = synth.wrap_case(60000, 42, 74, 3.0, freq=1.0e8, seed=950)
+
+    def grid():
+        p = Plan(42, 74, 3.0, eps, precision=prec)
+        out = torch.zeros((42, 74), dtype=tdt, device="cuda")
+        p.ms2dirty(to_dev(torch, d["uvw"]), d["freq"], to_dev(torch, d["vis"].astype(cdt)),
+                   to_dev(torch, d["wgt"].astype(rdt)), out)
+        torch.cuda.synchronize()
+        p.close()
+        return out.cpu().numpy()
+
+    monkeypatch.setenv("CG_SPLIT", "0")
+    whole = grid()
+    monkeypatch.delenv("CG_SPLIT")
+    monkeypatch.setenv("CG_SPLIT_ROWS", "300")
+    split = grid()
+    if prec == "fp32":
+        assert not np.array_equal(split, whole)  # the chunked sums ran
+    assert rel_l2(split, whole) < tol_split
+    ref, _ = O.ms2dirty(d["uvw"], d["vis"].astype(cdt).astype(np.complex128),
+                        d["wgt"].astype(rdt).astype(np.float64), 42, 74, 3.0, d["freq"], eps)
+    assert rel_l2(split, ref) < tol_oracle
